@@ -1,0 +1,131 @@
+"""GPU parity of the accumulation kernel (ocs_chan_profile_*) against the oracle.
+
+Bar: float64 kernel within 1e-10 relative L2 of the oracle's serial numba-equivalent sum
+(only the summation order differs); single-precision kernel within 1e-5.
+"""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import range_profile as orp
+
+pytestmark = pytest.mark.gpu
+G = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _built():
+    from oceansar_b200 import build
+    build.build()
+
+
+@pytest.mark.parametrize("case", ["smoke", "edges", "ties"])
+def test_golden_cases(case):
+    from oceansar_b200.radarsim import range_profile as rp
+    d = np.load(os.path.join(G, "range_profile.npz"))
+    g = {k.split("__", 1)[1]: d[k] for k in d.files if k.startswith(case + "__")}
+    out = g["out0"].astype(np.complex128).copy()
+    rp.chan_profile_numba(g["srg"], g["scene"], float(g["binsize"]), float(g["min_sr"]), g["sinc"],
+                          int(g["n"]), int(g["ovs"]), out)
+    assert rel(out, g["out"]) < 1e-12
+
+
+@pytest.mark.parametrize("name", ["c1small", "c2small", "c3small"])
+def test_captured_sar_raw_calls(name):
+    from oceansar_b200.radarsim import range_profile as rp
+    d = np.load(os.path.join(G, "sar_raw_%s.npz" % name))
+    sinc = rp.calc_sinc_vec(8, 20, Fs=1.1)
+    for i in range(3):
+        out = d["call%d_out0" % i].copy()
+        rp.chan_profile_numba(d["call%d_srg" % i], d["call%d_scene" % i], float(d["call%d_binsize" % i]),
+                              float(d["call%d_min_sr" % i]), sinc, 8, 20, out)
+        assert rel(out, d["call%d_out" % i]) < 1e-10
+
+
+def _synthetic(ny, nx, nbins, seed, binsize=2.725):
+    rs = np.random.RandomState(seed)
+    col = np.arange(nx) * 0.57 + 5.0
+    row = ((np.arange(ny) - ny / 2) ** 2) / 4e5
+    srg = col[None, :] + row[:, None] + 0.8 * rs.randn(ny, nx)
+    scene = rs.randn(ny, nx) + 1j * rs.randn(ny, nx)
+    return srg.ravel(), scene.ravel()
+
+
+@pytest.mark.parametrize("shape", [(64, 64, 32), (512, 512, 160), (1024, 2048, 512)])
+def test_large_against_oracle(shape):
+    from oceansar_b200.radarsim import range_profile as rp
+    ny, nx, nbins = shape
+    srg, scene = _synthetic(ny, nx, nbins, 3)
+    sinc = rp.calc_sinc_vec(8, 20, Fs=1.1)
+    ref = np.zeros(nbins, complex)
+    orp.chan_profile(srg, scene, 2.725, 0.0, sinc, 8, 20, ref)
+    out = np.zeros(nbins, complex)
+    rp.chan_profile_numba(srg, scene, 2.725, 0.0, sinc, 8, 20, out)
+    assert rel(out, ref) < 1e-10
+    # in-place accumulation: a second call doubles the result
+    rp.chan_profile_numba(srg, scene, 2.725, 0.0, sinc, 8, 20, out)
+    assert rel(out, 2 * ref) < 1e-10
+
+
+def test_rows_variant():
+    from oceansar_b200.radarsim import range_profile as rp
+    srg, scene = _synthetic(96, 300, 80, 4)
+    srg = srg.reshape(96, 300)
+    scene = scene.reshape(96, 300)
+    sinc = rp.calc_sinc_vec(8, 20, Fs=1.1)
+    ref = np.zeros((96, 80), complex)
+    orp.chan_profile(srg, scene, 2.725, 0.0, sinc, 8, 20, ref, rg_only=True)
+    out = np.zeros((96, 80), complex)
+    rp.chan_profile_numba(srg, scene, 2.725, 0.0, sinc, 8, 20, out, rg_only=True)
+    assert rel(out, ref) < 1e-10
+
+
+def test_empty_and_tensor_inplace():
+    from oceansar_b200.radarsim import range_profile as rp
+    sinc = rp.calc_sinc_vec(8, 20, Fs=1.1)
+    out = np.ones(8, complex)
+    rp.chan_profile_numba(np.zeros(0), np.zeros(0, complex), 1.0, 0.0, sinc, 8, 20, out)
+    assert np.all(out == 1)
+    srg, scene = _synthetic(32, 128, 64, 5)
+    t = torch.zeros(64, dtype=torch.complex128, device="cuda")
+    rp.chan_profile_numba(torch.from_numpy(srg).cuda(), torch.from_numpy(scene).cuda(), 2.725, 0.0,
+                          sinc, 8, 20, t)
+    ref = np.zeros(64, complex)
+    orp.chan_profile(srg, scene, 2.725, 0.0, sinc, 8, 20, ref)
+    assert rel(t.cpu().numpy(), ref) < 1e-10
+
+
+def test_nonfinite_scene_touches_only_its_taps():
+    from oceansar_b200.radarsim import range_profile as rp
+    sinc = rp.calc_sinc_vec(8, 20, Fs=1.0)
+    srg = np.array([10.3, 30.7, 31.2])
+    scene = np.array([1 + 1j, np.nan + 0j, 2 - 1j])
+    ref = np.zeros(48, complex)
+    orp.chan_profile(srg, scene, 1.0, 0.0, sinc, 8, 20, ref)
+    out = np.zeros(48, complex)
+    rp.chan_profile_numba(srg, scene, 1.0, 0.0, sinc, 8, 20, out)
+    np.testing.assert_array_equal(np.isnan(out), np.isnan(ref))
+    fin = ~np.isnan(ref)
+    assert rel(out[fin], ref[fin]) < 1e-12
+
+
+def test_single_precision_kernel():
+    from oceansar_b200 import _capi, _device
+    from oceansar_b200.radarsim import range_profile as rp
+    srg, scene = _synthetic(512, 512, 160, 6)
+    sinc = rp.calc_sinc_vec(8, 20, Fs=1.1)
+    ref = np.zeros(160, complex)
+    orp.chan_profile(srg, scene, 2.725, 0.0, sinc, 8, 20, ref)
+    srg_d = _device.to_device(srg, np.float64)
+    sc_d = _device.to_device(scene.astype(np.complex64), np.complex64)
+    out_d = _device.zeros(160, np.complex64)
+    sinc_d = _device.to_device(sinc, np.float32)
+    _capi.call("ocs_chan_profile_c64", _device.ptr(srg_d), _device.ptr(sc_d), srg.size, 2.725, 0.0,
+               _device.ptr(sinc_d), 8, 20, _device.ptr(out_d), 160, _device.stream_ptr())
+    assert rel(out_d.cpu().numpy(), ref) < 1e-5
