@@ -63,6 +63,70 @@ int ocs_chan_profile_c64(const double *srg_d, const float *scene_d, int64_t npts
                          int n_sinc_samples, int sinc_ovs, float *output_d, int64_t nbins,
                          void *stream);
 
+
+/* ------------------------------------------------------------------------------------
+ * Per-pulse surface synthesis.
+ *
+ * Replaces the OceanSurface.t setter (oceansar/surfaces/ocean.py:418-526): propagation
+ * c(t) = wave_coefs * exp(-i omega t) (:424-427) and one inverse 2-D FFT per field, here
+ * two real fields per complex transform.  Field codes name the reference's attributes;
+ * the OCS_FIELD_AUX_* codes are the intermediate choppy-wave transforms (:452-482).
+ */
+enum {
+    OCS_FIELD_DZ = 0, OCS_FIELD_DX = 1, OCS_FIELD_DY = 2,
+    OCS_FIELD_DIFFX = 3, OCS_FIELD_DIFFY = 4,
+    OCS_FIELD_DIFFXX = 5, OCS_FIELD_DIFFYY = 6, OCS_FIELD_DIFFXY = 7,
+    OCS_FIELD_VX = 8, OCS_FIELD_VY = 9, OCS_FIELD_VZ = 10,
+    OCS_FIELD_AX = 11, OCS_FIELD_AY = 12, OCS_FIELD_AZ = 13,
+    OCS_FIELD_HMTF = 14,
+    OCS_FIELD_AUX_XX = 15, OCS_FIELD_AUX_YY = 16,
+    OCS_FIELD_AUX_XXX = 17, OCS_FIELD_AUX_YYY = 18, OCS_FIELD_AUX_XXY = 19,
+    OCS_FIELD_COUNT = 20
+};
+
+typedef struct {
+    int32_t nx, ny;            /* grid (Nx, Ny); every prime factor in {2, 3, 5, 7}      */
+    const void *coefs_d;       /* complex64 [ny][nx] wave_coefs (ocean.py:236)          */
+    const float *omega_d;      /* float32 [ny][nx] dispersion relation (ocean.py:155-158) */
+    const float *kx_d;         /* float32 [nx] 2*pi*fftfreq(nx, dx) (ocean.py:131)      */
+    const float *ky_d;         /* float32 [ny] 2*pi*fftfreq(ny, dy) (ocean.py:133)      */
+    float kmin_half;           /* min(kx_res, ky_res)/2, the |k| cut of kxn/kyn/kinv (:142) */
+    int32_t nfields;           /* 1 .. 24                                               */
+    const int32_t *codes;      /* host [nfields] OCS_FIELD_* codes                      */
+    float *const *dst_d;       /* host [nfields] device pointers, float32 [ny][nx]      */
+    const float *add;          /* host [nfields] constant term (current*t, current) or NULL */
+    const float *swell_mult;   /* host [2*nfields] complex factor of the swell term or NULL */
+    const void *swell_exp_d;   /* complex64 [ny][nx] monochromatic swell (:231-233) or NULL */
+    float swell_rot_re;        /* exp(-i swell_omega t), complex64                      */
+    float swell_rot_im;
+    void *workspace_d;         /* ocs_surface_workspace_bytes() bytes, ocs_surface_prepare()d */
+} ocs_surface_desc;
+
+/* Workspace for a grid and field count: twiddle tables + packed scratch planes; < 0 on
+ * invalid sizes. */
+int64_t ocs_surface_workspace_bytes(int32_t nx, int32_t ny, int32_t nfields);
+
+/* Fill the twiddle tables of a workspace (once per grid). */
+int ocs_surface_prepare(int32_t nx, int32_t ny, void *workspace_d, void *stream);
+
+/* Synthesize the requested fields at time t (float32, as ocean.py:424 casts it). */
+int ocs_surface_update(const ocs_surface_desc *desc, float t, void *stream);
+
+typedef struct {
+    int64_t n;                                       /* ny*nx                               */
+    const float *ax_d, *ay_d, *axx_d, *ayy_d;        /* Re ifft2 of i kx c, i ky c, -kx^2/k c, -ky^2/k c */
+    const float *axxx_d, *ayyy_d, *axxy_d;           /* -i kx^3/k c, -i ky^3/k c, -i kx^2 ky/k c (Diff2 only) */
+    const float *fxx_d, *fyy_d, *fxy_d;              /* -kx^2 c, -ky^2 c, -kx ky c (Diff2 only) */
+    float *diffx_d, *diffy_d;                        /* outputs (NULL: skip the slopes)    */
+    float *diffxx_d, *diffyy_d, *diffxy_d;           /* outputs (NULL: skip the curvatures) */
+    const void *swell_exp_d;                         /* complex64 swell or NULL            */
+    float swell_rot_re, swell_rot_im;
+    const float *swell_mult;                         /* host [10]: Diffx, Diffy, Diffxx, Diffyy, Diffxy */
+} ocs_choppy_desc;
+
+/* Choppy-wave slopes / curvatures from the auxiliary fields (ocean.py:451-456, 468-482). */
+int ocs_surface_choppy(const ocs_choppy_desc *desc, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

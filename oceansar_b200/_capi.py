@@ -31,8 +31,12 @@ SIGNATURES = {
     "ocs_chan_profile_rows_f64": [c_ptr, c_ptr, c_i64, c_i64, c_dbl, c_dbl, c_ptr, c_int, c_int, c_ptr,
                                   c_i64, c_ptr],
     "ocs_chan_profile_c64": [c_ptr, c_ptr, c_i64, c_dbl, c_dbl, c_ptr, c_int, c_int, c_ptr, c_i64, c_ptr],
+    "ocs_surface_workspace_bytes": [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32],
+    "ocs_surface_prepare": [ctypes.c_int32, ctypes.c_int32, c_ptr, c_ptr],
+    "ocs_surface_update": [c_ptr, c_flt, c_ptr],
+    "ocs_surface_choppy": [c_ptr, c_ptr],
 }
-_RESTYPE = {"ocs_version": ctypes.c_char_p}
+_RESTYPE = {"ocs_version": ctypes.c_char_p, "ocs_surface_workspace_bytes": ctypes.c_int64}
 
 _lib = None
 

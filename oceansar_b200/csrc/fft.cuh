@@ -1,0 +1,218 @@
+// Shared-memory mixed-radix (2, 3, 4, 5, 7, 8) inverse FFT used by the surface kernels.
+//
+// A CTA transforms `nvec` vectors of length n held in shared memory with the
+// self-sorting Stockham formulation: at a stage of radix R after radices of product Ns,
+// butterfly j reads x[j + r*n/R] (r < R), multiplies by w^(r*(j mod Ns)*n/(Ns*R)),
+// takes an R-point DFT and writes x[(j/Ns)*Ns*R + j mod Ns + r*Ns].  Power-of-two lengths
+// are compiled per length (radix 8, then one 4 or 2): each thread keeps its butterflies in
+// registers between a read phase and a write phase separated by a barrier, so one buffer
+// suffices.  Other lengths (primes 3, 5, 7) run a runtime plan out of place between two
+// buffers.  Element i of a vector lives at smem index
+// i + (i >> 3) (one pad slot per 8) to break the power-of-two strides of the first stage.
+// Twiddles w^m = exp(+2*pi*i*m/n) come from a float64-accurate table in global memory.
+#pragma once
+#include "common.cuh"
+
+namespace ocs {
+
+constexpr int kMaxStages = 16;
+
+struct FftPlan {
+    int n;
+    int nstages;
+    int radix[kMaxStages];
+    const float2 *tw;       // [n] twiddles exp(+2 pi i m / n)
+};
+
+OCS_HD int pad_idx(int i) { return i + (i >> 3); }
+OCS_HD int padded_len(int n) { return n + (n >> 3) + 1; }
+
+OCS_D float2 c_mul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+OCS_D float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+OCS_D float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+OCS_D float2 c_ipos(float2 a) { return make_float2(-a.y, a.x); }     // +i * a
+
+// In-place R-point inverse DFT (positive exponent) of v[0..R).
+template <int R> OCS_D void dft_inv(float2 *v);
+
+template <> OCS_D void dft_inv<2>(float2 *v) {
+    float2 a = v[0], b = v[1];
+    v[0] = c_add(a, b);
+    v[1] = c_sub(a, b);
+}
+template <> OCS_D void dft_inv<4>(float2 *v) {
+    float2 a0 = c_add(v[0], v[2]), a1 = c_sub(v[0], v[2]);
+    float2 b0 = c_add(v[1], v[3]), b1 = c_ipos(c_sub(v[1], v[3]));
+    v[0] = c_add(a0, b0);
+    v[2] = c_sub(a0, b0);
+    v[1] = c_add(a1, b1);
+    v[3] = c_sub(a1, b1);
+}
+template <> OCS_D void dft_inv<8>(float2 *v) {
+    const float h = 0.70710678118654752f;
+    float2 e[4] = {v[0], v[2], v[4], v[6]};
+    float2 o[4] = {v[1], v[3], v[5], v[7]};
+    dft_inv<4>(e);
+    dft_inv<4>(o);
+    // o[k] *= exp(+2 pi i k / 8)
+    o[1] = make_float2(h * (o[1].x - o[1].y), h * (o[1].x + o[1].y));
+    o[2] = c_ipos(o[2]);
+    o[3] = make_float2(-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y));
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        v[k] = c_add(e[k], o[k]);
+        v[k + 4] = c_sub(e[k], o[k]);
+    }
+}
+template <> OCS_D void dft_inv<3>(float2 *v) {
+    const float c1 = -0.5f, s1 = 0.86602540378443865f;
+    float2 a = v[0], b = v[1], c = v[2];
+    float2 t = c_add(b, c);
+    float2 d = c_sub(b, c);
+    float2 m = make_float2(a.x + c1 * t.x, a.y + c1 * t.y);
+    v[0] = c_add(a, t);
+    v[1] = make_float2(m.x - s1 * d.y, m.y + s1 * d.x);
+    v[2] = make_float2(m.x + s1 * d.y, m.y - s1 * d.x);
+}
+template <> OCS_D void dft_inv<5>(float2 *v) {
+    const float c1 = 0.30901699437494742f, c2 = -0.80901699437494742f;
+    const float s1 = 0.95105651629515357f, s2 = 0.58778525229247313f;
+    float2 a = v[0];
+    float2 t1 = c_add(v[1], v[4]), d1 = c_sub(v[1], v[4]);
+    float2 t2 = c_add(v[2], v[3]), d2 = c_sub(v[2], v[3]);
+    v[0] = c_add(a, c_add(t1, t2));
+    float2 m1 = make_float2(a.x + c1 * t1.x + c2 * t2.x, a.y + c1 * t1.y + c2 * t2.y);
+    float2 m2 = make_float2(a.x + c2 * t1.x + c1 * t2.x, a.y + c2 * t1.y + c1 * t2.y);
+    float2 n1 = make_float2(s1 * d1.x + s2 * d2.x, s1 * d1.y + s2 * d2.y);
+    float2 n2 = make_float2(s2 * d1.x - s1 * d2.x, s2 * d1.y - s1 * d2.y);
+    v[1] = make_float2(m1.x - n1.y, m1.y + n1.x);
+    v[4] = make_float2(m1.x + n1.y, m1.y - n1.x);
+    v[2] = make_float2(m2.x - n2.y, m2.y + n2.x);
+    v[3] = make_float2(m2.x + n2.y, m2.y - n2.x);
+}
+template <> OCS_D void dft_inv<7>(float2 *v) {
+    // X[j] = a + sum_k (t_k cos(2 pi jk/7) + i d_k sin(2 pi jk/7)), k = 1..3, with
+    // t_k = v[k] + v[7-k] and d_k = v[k] - v[7-k]; X[7-j] takes the conjugate sine part.
+    const float C7[7] = {1.f, 0.62348980185873353f, -0.22252093395631440f, -0.90096886790241913f,
+                         -0.90096886790241913f, -0.22252093395631440f, 0.62348980185873353f};
+    const float S7[7] = {0.f, 0.78183148246802981f, 0.97492791218182361f, 0.43388373911755812f,
+                         -0.43388373911755812f, -0.97492791218182361f, -0.78183148246802981f};
+    float2 a = v[0];
+    float2 t[3], d[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { t[k] = c_add(v[k + 1], v[6 - k]); d[k] = c_sub(v[k + 1], v[6 - k]); }
+    v[0] = c_add(a, c_add(t[0], c_add(t[1], t[2])));
+#pragma unroll
+    for (int j = 1; j <= 3; ++j) {
+        float2 m = a, n = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int k = 1; k <= 3; ++k) {
+            const int idx = (j * k) % 7;
+            m.x += C7[idx] * t[k - 1].x; m.y += C7[idx] * t[k - 1].y;
+            n.x += S7[idx] * d[k - 1].x; n.y += S7[idx] * d[k - 1].y;
+        }
+        v[j] = make_float2(m.x - n.y, m.y + n.x);
+        v[7 - j] = make_float2(m.x + n.y, m.y - n.x);
+    }
+}
+
+// One in-place Stockham stage of radix R over nvec padded vectors: every thread loads
+// and transforms up to IT butterflies into registers, then (after a barrier) stores them.
+template <int R, int IT>
+OCS_D void fft_stage_inplace(float2 *buf, int vstride, int nvec, int n, int ns, const float2 *tw) {
+    const int nb = n / R;
+    const int tstep = n / (ns * R);
+    float2 v[IT][R];
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int b = threadIdx.x + it * blockDim.x;
+        if (b < nb * nvec) {
+            const int vec = b / nb, j = b - vec * nb;
+            const float2 *x = buf + vec * vstride;
+            const int jm = j % ns;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                float2 a = x[pad_idx(j + r * nb)];
+                if (r > 0 && jm > 0) a = c_mul(a, __ldg(&tw[r * jm * tstep]));
+                v[it][r] = a;
+            }
+            dft_inv<R>(v[it]);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < IT; ++it) {
+        const int b = threadIdx.x + it * blockDim.x;
+        if (b < nb * nvec) {
+            const int vec = b / nb, j = b - vec * nb;
+            float2 *x = buf + vec * vstride;
+            const int jm = j % ns;
+            const int d = (j - jm) * R + jm;
+#pragma unroll
+            for (int r = 0; r < R; ++r) x[pad_idx(d + r * ns)] = v[it][r];
+        }
+    }
+    __syncthreads();
+}
+
+// Power-of-two length N known at compile time: radix-8 stages, then one radix-4 or -2
+// stage; NVEC vectors, T threads.
+template <int N, int NVEC, int T, int NS = 1>
+OCS_D void ifft_pow2(float2 *buf, int vstride, const float2 *tw) {
+    if constexpr (NS < N) {
+        constexpr int REM = N / NS;
+        constexpr int R = (REM % 8 == 0) ? 8 : REM;
+        constexpr int IT = ((N / R) * NVEC + T - 1) / T;
+        fft_stage_inplace<R, IT>(buf, vstride, NVEC, N, NS, tw);
+        ifft_pow2<N, NVEC, T, NS * R>(buf, vstride, tw);
+    }
+}
+
+// One out-of-place Stockham stage (any length, runtime radix R <= 8): src -> dst.
+template <int R>
+OCS_D void fft_stage_pp(const float2 *src, float2 *dst, int vstride, int nvec, int n, int ns,
+                        const float2 *tw) {
+    const int nb = n / R;
+    const int tstep = n / (ns * R);
+    for (int b = threadIdx.x; b < nb * nvec; b += blockDim.x) {
+        const int vec = b / nb, j = b - vec * nb;
+        const float2 *x = src + vec * vstride;
+        float2 *y = dst + vec * vstride;
+        const int jm = j % ns;
+        float2 v[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            float2 a = x[pad_idx(j + r * nb)];
+            if (r > 0 && jm > 0) a = c_mul(a, __ldg(&tw[r * jm * tstep]));
+            v[r] = a;
+        }
+        dft_inv<R>(v);
+        const int d = (j - jm) * R + jm;
+#pragma unroll
+        for (int r = 0; r < R; ++r) y[pad_idx(d + r * ns)] = v[r];
+    }
+}
+
+// Mixed-radix inverse FFT with a runtime plan, ping-ponging between a and b.  Returns the
+// buffer that holds the result.
+OCS_D float2 *ifft_generic(float2 *a, float2 *b, int vstride, int nvec, const FftPlan &plan) {
+    int ns = 1;
+    float2 *src = a, *dst = b;
+    for (int s = 0; s < plan.nstages; ++s) {
+        const int R = plan.radix[s];
+        switch (R) {
+            case 8: fft_stage_pp<8>(src, dst, vstride, nvec, plan.n, ns, plan.tw); break;
+            case 4: fft_stage_pp<4>(src, dst, vstride, nvec, plan.n, ns, plan.tw); break;
+            case 2: fft_stage_pp<2>(src, dst, vstride, nvec, plan.n, ns, plan.tw); break;
+            case 3: fft_stage_pp<3>(src, dst, vstride, nvec, plan.n, ns, plan.tw); break;
+            case 5: fft_stage_pp<5>(src, dst, vstride, nvec, plan.n, ns, plan.tw); break;
+            default: fft_stage_pp<7>(src, dst, vstride, nvec, plan.n, ns, plan.tw); break;
+        }
+        __syncthreads();
+        float2 *t = src; src = dst; dst = t;
+        ns *= R;
+    }
+    return src;
+}
+
+}  // namespace ocs

@@ -1,0 +1,432 @@
+// Per-pulse linear-wave surface synthesis: the OceanSurface.t setter
+// (oceansar/surfaces/ocean.py:418-526) on sm_100a.
+//
+// Every field the reference computes is Re(ifft2(M_f(k) * c(t))) (+ a constant / swell
+// term), with c(t) = wave_coefs * exp(-i omega t) (ocean.py:427) and M_f a per-field
+// spectral multiplier (i kx for Diffx, -kx^2 for Diffxx, i kx/|k| for Dx, ...).  Two real
+// fields A, B are packed into ONE complex transform:
+//     Z = H(M_A c) + i H(M_B c),  H(X)[k] = (X[k] + conj(X[-k])) / 2,
+// so ifft2(Z) = A + iB exactly (H(X) is the Hermitian part whose inverse DFT is Re(ifft2 X)).
+// The 2-D inverse DFT runs as two shared-memory passes:
+//   pass 1 (rows, x): one CTA per row pair (r, Ny-r).  The phase evolution, multipliers
+//          and Hermitian packing are computed on the fly from c and omega (read once per
+//          pulse), then each packed row is transformed and written to a scratch plane.
+//   pass 2 (columns, y): one CTA per (transform, W-column tile); column transforms, then
+//          the 1/(Nx Ny) scale, the additive terms and the unpacking into two float32
+//          fields.
+// A third, element-wise kernel applies the choppy-wave combinations (ocean.py:451-482).
+#include <math.h>
+#include <string.h>
+
+#include "fft.cuh"
+
+namespace ocs {
+
+constexpr int kMaxPacked = 12;          // transforms per call (24 real fields)
+
+struct SurfaceArgs {
+    int nx, ny;
+    const float2 *coefs;
+    const float *omega;
+    const float *kx;
+    const float *ky;
+    float kmin_half;
+    float t;
+    float inv_n;
+    int npair;
+    int code[2 * kMaxPacked];
+    float *dst[2 * kMaxPacked];
+    float add[2 * kMaxPacked];
+    float2 swm[2 * kMaxPacked];
+    const float2 *swell_exp;
+    float2 swell_rot;
+    float2 *scratch;
+    FftPlan px, py;
+};
+
+// Spectral multiplier of field `code` at wavenumber (kx, ky) (ocean.py:431-526).
+OCS_D float2 field_mult(int code, float kxv, float kyv, float kmin_half, float om) {
+    float k = __fsqrt_rn(fadd(fmul(kxv, kxv), fmul(kyv, kyv)));
+    bool good = k > kmin_half;
+    float kxn = good ? __fdiv_rn(kxv, k) : 0.f;
+    float kyn = good ? __fdiv_rn(kyv, k) : 0.f;
+    float kinv = good ? __frcp_rn(k) : 0.f;
+    switch (code) {
+        case OCS_FIELD_DZ: return make_float2(1.f, 0.f);
+        case OCS_FIELD_DX: return make_float2(0.f, kxn);                 // -Im(ifft2(kxn c))
+        case OCS_FIELD_DY: return make_float2(0.f, kyn);
+        case OCS_FIELD_DIFFX: return make_float2(0.f, kxv);              // Re(ifft2(i kx c))
+        case OCS_FIELD_DIFFY: return make_float2(0.f, kyv);
+        case OCS_FIELD_DIFFXX: return make_float2(-kxv * kxv, 0.f);
+        case OCS_FIELD_DIFFYY: return make_float2(-kyv * kyv, 0.f);
+        case OCS_FIELD_DIFFXY: return make_float2(-kxv * kyv, 0.f);
+        case OCS_FIELD_VX: return make_float2(kxn * om, 0.f);            // -Im(ifft2(kxn (-i w) c))
+        case OCS_FIELD_VY: return make_float2(kyn * om, 0.f);
+        case OCS_FIELD_VZ: return make_float2(0.f, -om);
+        case OCS_FIELD_AX: return make_float2(0.f, -kxv * kinv * om * om);
+        case OCS_FIELD_AY: return make_float2(0.f, -kyv * kinv * om * om);
+        case OCS_FIELD_AZ: return make_float2(-om * om, 0.f);
+        case OCS_FIELD_HMTF: {
+            // M_h = i k w (w + i mu) / (w^2 + mu^2) * (dlnS/dlnk - Vg/c), zero for k > 2 pi/20
+            const float kmax = 0.3141592653589793f, mu = 0.0025f, fac = -3.5f;
+            if (k > kmax) return make_float2(0.f, 0.f);
+            float den = om * om + mu * mu;
+            float2 num = make_float2(-k * om * mu, k * om * om);
+            return make_float2(num.x / den * fac, num.y / den * fac);
+        }
+        case OCS_FIELD_AUX_XX: return make_float2(-kxv * kxv * kinv, 0.f);
+        case OCS_FIELD_AUX_YY: return make_float2(-kyv * kyv * kinv, 0.f);
+        case OCS_FIELD_AUX_XXX: return make_float2(0.f, -kxv * kxv * kxv * kinv);
+        case OCS_FIELD_AUX_YYY: return make_float2(0.f, -kyv * kyv * kyv * kinv);
+        case OCS_FIELD_AUX_XXY: return make_float2(0.f, -kxv * kxv * kyv * kinv);
+        default: return make_float2(0.f, 0.f);
+    }
+}
+
+// c(t) = c * exp(-i fl(omega t)) in complex64 (ocean.py:424-427).
+OCS_D float2 phased(const SurfaceArgs &a, int y, int x) {
+    size_t i = (size_t)y * a.nx + x;
+    float2 c = a.coefs[i];
+    float ph = -fmul(a.omega[i], a.t);
+    float s, co;
+    sincosf(ph, &s, &co);
+    return make_float2(fsub(fmul(c.x, co), fmul(c.y, s)), fadd(fmul(c.x, s), fmul(c.y, co)));
+}
+
+// Threads per CTA of the two passes for a power-of-two length N (0 = any length).
+template <int N> __host__ __device__ constexpr int rows_threads() {
+    return N == 0 ? 256 : (N / 8 < 64 ? 64 : (N / 8 > 512 ? 512 : N / 8));
+}
+template <int N, int TILE> __host__ __device__ constexpr int cols_threads() {
+    return N == 0 ? 256 : (N * TILE / 16 < 64 ? 64 : (N * TILE / 16 > 1024 ? 1024 : N * TILE / 16));
+}
+
+// Pass 1.  Shared memory: c(t) of rows r and mr ([2][nx], unpadded), then the two padded
+// FFT rows (and, for non-power-of-two lengths, two more for the ping-pong).  Mirror pairs:
+// (r,x) <-> (mr,mx) and (r,mx) <-> (mr,x).
+template <int N>
+__global__ void __launch_bounds__(rows_threads<N>(), 1)
+surface_rows_kernel(const __grid_constant__ SurfaceArgs a) {
+    extern __shared__ __align__(16) float2 sbuf[];
+    const int nx = (N > 0) ? N : a.nx;
+    const int ny = a.ny;
+    const int r = blockIdx.x;
+    const int mr = (ny - r) % ny;
+    const int vstride = padded_len(nx);
+    float2 *cA = sbuf, *cB = sbuf + nx;
+    float2 *rowA = sbuf + 2 * nx, *rowB = rowA + vstride;
+    const float kyr = a.ky[r], kymr = a.ky[mr];
+    const float *omA = a.omega + (size_t)r * nx, *omB = a.omega + (size_t)mr * nx;
+
+    for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+        cA[x] = phased(a, r, x);
+        cB[x] = phased(a, mr, x);
+    }
+    __syncthreads();
+
+    const int nq = nx / 2 + 1;
+    for (int p = 0; p < a.npair; ++p) {
+        const int ca = a.code[2 * p], cb = a.code[2 * p + 1];
+        for (int x = threadIdx.x; x < nq; x += blockDim.x) {
+            const int mx = (nx - x) % nx;
+            const float kxx = a.kx[x], kxm = a.kx[mx];
+            const float kxs[4] = {kxx, kxm, kxx, kxm};
+            const float kys[4] = {kyr, kyr, kymr, kymr};
+            const float2 cq[4] = {cA[x], cA[mx], cB[x], cB[mx]};
+            const float oq[4] = {omA[x], omA[mx], omB[x], omB[mx]};
+            float2 XA[4], XB[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                XA[j] = c_mul(field_mult(ca, kxs[j], kys[j], a.kmin_half, oq[j]), cq[j]);
+                XB[j] = (cb >= 0) ? c_mul(field_mult(cb, kxs[j], kys[j], a.kmin_half, oq[j]), cq[j])
+                                  : make_float2(0.f, 0.f);
+            }
+            // Z(j) = (XA[j] + conj XA[mir]) / 2 + i (XB[j] + conj XB[mir]) / 2
+            float2 Z[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int m = 3 - j;
+                float2 ha = make_float2(0.5f * (XA[j].x + XA[m].x), 0.5f * (XA[j].y - XA[m].y));
+                float2 hb = make_float2(0.5f * (XB[j].x + XB[m].x), 0.5f * (XB[j].y - XB[m].y));
+                Z[j] = make_float2(ha.x - hb.y, ha.y + hb.x);
+            }
+            rowA[pad_idx(x)] = Z[0];
+            rowA[pad_idx(mx)] = Z[1];
+            rowB[pad_idx(x)] = Z[2];
+            rowB[pad_idx(mx)] = Z[3];
+        }
+        __syncthreads();
+        const float2 *res = rowA;
+        if constexpr (N > 0) {
+            ifft_pow2<N, 2, rows_threads<N>()>(rowA, vstride, a.px.tw);
+        } else {
+            res = ifft_generic(rowA, rowB + vstride, vstride, 2, a.px);
+        }
+        float2 *outA = a.scratch + ((size_t)p * ny + r) * nx;
+        float2 *outB = a.scratch + ((size_t)p * ny + mr) * nx;
+        for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+            outA[x] = res[pad_idx(x)];
+            if (mr != r) outB[x] = res[vstride + pad_idx(x)];
+        }
+        __syncthreads();
+    }
+}
+
+// Pass 2.  One CTA per (transform p, tile of TILE columns).
+template <int N, int TILE>
+__global__ void __launch_bounds__(cols_threads<N, TILE>(), 1)
+surface_cols_kernel(const __grid_constant__ SurfaceArgs a) {
+    extern __shared__ __align__(16) float2 sbuf[];
+    const int nx = a.nx;
+    const int ny = (N > 0) ? N : a.ny;
+    const int p = blockIdx.y;
+    const int x0 = blockIdx.x * TILE;
+    const int vstride = padded_len(ny);
+    const float2 *src = a.scratch + (size_t)p * ny * nx;
+    for (int i = threadIdx.x; i < ny * TILE; i += blockDim.x) {
+        const int y = i / TILE, w = i - y * TILE;
+        const int x = x0 + w;
+        sbuf[w * vstride + pad_idx(y)] = (x < nx) ? src[(size_t)y * nx + x] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const float2 *res = sbuf;
+    if constexpr (N > 0) {
+        ifft_pow2<N, TILE, cols_threads<N, TILE>()>(sbuf, vstride, a.py.tw);
+    } else {
+        res = ifft_generic(sbuf, sbuf + TILE * vstride, vstride, TILE, a.py);
+    }
+    float *dA = a.dst[2 * p], *dB = a.dst[2 * p + 1];
+    const float addA = a.add[2 * p], addB = a.add[2 * p + 1];
+    const float2 smA = a.swm[2 * p], smB = a.swm[2 * p + 1];
+    const bool sw = a.swell_exp != nullptr;
+    for (int i = threadIdx.x; i < ny * TILE; i += blockDim.x) {
+        const int y = i / TILE, w = i - y * TILE;
+        const int x = x0 + w;
+        if (x >= nx) continue;
+        float2 z = res[w * vstride + pad_idx(y)];
+        float va = fadd(z.x * a.inv_n, addA);
+        float vb = fadd(z.y * a.inv_n, addB);
+        if (sw) {
+            float2 s = c_mul(a.swell_exp[(size_t)y * nx + x], a.swell_rot);
+            va = fadd(va, fsub(fmul(smA.x, s.x), fmul(smA.y, s.y)));
+            vb = fadd(vb, fsub(fmul(smB.x, s.x), fmul(smB.y, s.y)));
+        }
+        dA[(size_t)y * nx + x] = va;
+        if (dB) dB[(size_t)y * nx + x] = vb;
+    }
+}
+
+// Choppy-wave slopes and curvatures from the auxiliary fields (ocean.py:451-456, 468-482).
+struct ChoppyArgs {
+    long long n;
+    const float *ax, *ay, *axx, *ayy, *axxx, *ayyy, *axxy, *fxx, *fyy, *fxy;
+    float *diffx, *diffy, *diffxx, *diffyy, *diffxy;
+    const float2 *swell_exp;
+    float2 swell_rot;
+    float2 sw_dx, sw_dy, sw_dxx, sw_dyy, sw_dxy;
+};
+
+__global__ void surface_choppy_kernel(ChoppyArgs c) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < c.n;
+         i += (long long)gridDim.x * blockDim.x) {
+        float2 s = make_float2(0.f, 0.f);
+        if (c.swell_exp) s = c_mul(c.swell_exp[i], c.swell_rot);
+        const float ax = c.ax[i], ay = c.ay[i], axx = c.axx[i], ayy = c.ayy[i];
+        if (c.diffx) {
+            c.diffx[i] = fadd(ax / (1.f + axx), fsub(fmul(c.sw_dx.x, s.x), fmul(c.sw_dx.y, s.y)));
+            c.diffy[i] = fadd(ay / (1.f + ayy), fsub(fmul(c.sw_dy.x, s.x), fmul(c.sw_dy.y, s.y)));
+        }
+        if (c.diffxx) {
+            const float px = 1.f + axx, py = 1.f + ayy;
+            float vxx = (px * c.fxx[i] - c.axxx[i] * ax) / powf(px, 3.f);
+            float vyy = (py * c.fyy[i] - c.ayyy[i] * ay) / powf(py, 3.f);
+            float vxy = (px * c.fxy[i] - c.axxy[i] * ax) / (powf(px, 2.f) * py);
+            c.diffxx[i] = fadd(vxx, fsub(fmul(c.sw_dxx.x, s.x), fmul(c.sw_dxx.y, s.y)));
+            c.diffyy[i] = fadd(vyy, fsub(fmul(c.sw_dyy.x, s.x), fmul(c.sw_dyy.y, s.y)));
+            c.diffxy[i] = fadd(vxy, fsub(fmul(c.sw_dxy.x, s.x), fmul(c.sw_dxy.y, s.y)));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Host side.
+static bool make_plan(int n, FftPlan &pl) {
+    pl.n = n;
+    pl.nstages = 0;
+    int m = n;
+    // radix 8 first, then a single 4 or 2 for the remaining power of two, then 3, 5, 7
+    while (m % 8 == 0) { if (pl.nstages >= kMaxStages) return false; pl.radix[pl.nstages++] = 8; m /= 8; }
+    while (m % 4 == 0) { if (pl.nstages >= kMaxStages) return false; pl.radix[pl.nstages++] = 4; m /= 4; }
+    while (m % 2 == 0) { if (pl.nstages >= kMaxStages) return false; pl.radix[pl.nstages++] = 2; m /= 2; }
+    const int others[3] = {3, 5, 7};
+    for (int k = 0; k < 3; ++k)
+        while (m % others[k] == 0) {
+            if (pl.nstages >= kMaxStages) return false;
+            pl.radix[pl.nstages++] = others[k];
+            m /= others[k];
+        }
+    return m == 1;
+}
+
+
+__global__ void twiddle_kernel(float2 *tw, int n) {
+    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
+        double s, c;
+        sincospi(2.0 * (double)m / (double)n, &s, &c);
+        tw[m] = make_float2((float)c, (float)s);
+    }
+}
+
+static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// Workspace layout: [twiddles x (nx) | twiddles y (ny) | scratch planes npair*ny*nx].
+static size_t ws_twx(int) { return 0; }
+static size_t ws_twy(int nx) { return align256((size_t)nx * sizeof(float2)); }
+static size_t ws_scratch(int nx, int ny) { return ws_twy(nx) + align256((size_t)ny * sizeof(float2)); }
+
+template <int N>
+static cudaError_t launch_rows_n(const SurfaceArgs &a, cudaStream_t st) {
+    const int nx = a.nx;
+    size_t smem = (2 * (size_t)nx + (N > 0 ? 2 : 4) * (size_t)padded_len(nx)) * sizeof(float2);
+    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(surface_rows_kernel<N>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    surface_rows_kernel<N><<<a.ny / 2 + 1, rows_threads<N>(), smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int N, int TILE>
+static cudaError_t launch_cols_n(const SurfaceArgs &a, cudaStream_t st) {
+    const int ny = a.ny;
+    size_t smem = (N > 0 ? 1 : 2) * (size_t)TILE * padded_len(ny) * sizeof(float2);
+    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(surface_cols_kernel<N, TILE>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid((a.nx + TILE - 1) / TILE, a.npair);
+    surface_cols_kernel<N, TILE><<<grid, cols_threads<N, TILE>(), smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+static cudaError_t launch_rows(const SurfaceArgs &a, cudaStream_t st) {
+    switch (a.nx) {
+        case 64: return launch_rows_n<64>(a, st);
+        case 128: return launch_rows_n<128>(a, st);
+        case 256: return launch_rows_n<256>(a, st);
+        case 512: return launch_rows_n<512>(a, st);
+        case 1024: return launch_rows_n<1024>(a, st);
+        case 2048: return launch_rows_n<2048>(a, st);
+        case 4096: return launch_rows_n<4096>(a, st);
+        case 8192: return launch_rows_n<8192>(a, st);
+        default: return launch_rows_n<0>(a, st);
+    }
+}
+
+static cudaError_t launch_cols(const SurfaceArgs &a, cudaStream_t st) {
+    switch (a.ny) {
+        case 64: return launch_cols_n<64, 4>(a, st);
+        case 128: return launch_cols_n<128, 4>(a, st);
+        case 256: return launch_cols_n<256, 4>(a, st);
+        case 512: return launch_cols_n<512, 4>(a, st);
+        case 1024: return launch_cols_n<1024, 4>(a, st);
+        case 2048: return launch_cols_n<2048, 4>(a, st);
+        case 4096: return launch_cols_n<4096, 4>(a, st);
+        case 8192: return launch_cols_n<8192, 2>(a, st);
+        default: return launch_cols_n<0, 4>(a, st);
+    }
+}
+
+}  // namespace ocs
+
+using namespace ocs;
+
+extern "C" int64_t ocs_surface_workspace_bytes(int32_t nx, int32_t ny, int32_t nfields) {
+    if (nx < 2 || ny < 2 || nfields < 1 || nfields > 2 * kMaxPacked) return -1;
+    int npair = (nfields + 1) / 2;
+    return (int64_t)(ws_scratch(nx, ny) + (size_t)npair * nx * ny * sizeof(float2));
+}
+
+extern "C" int ocs_surface_prepare(int32_t nx, int32_t ny, void *workspace, void *stream) {
+    if (!workspace || nx < 2 || ny < 2) return OCS_ERR_ARG;
+    FftPlan px, py;
+    if (!make_plan(nx, px) || !make_plan(ny, py)) return OCS_ERR_UNSUPPORTED;
+    char *ws = (char *)workspace;
+    cudaStream_t st = (cudaStream_t)stream;
+    twiddle_kernel<<<(nx + 255) / 256, 256, 0, st>>>((float2 *)(ws + ws_twx(nx)), nx);
+    twiddle_kernel<<<(ny + 255) / 256, 256, 0, st>>>((float2 *)(ws + ws_twy(nx)), ny);
+    return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
+}
+
+extern "C" int ocs_surface_update(const ocs_surface_desc *d, float t, void *stream) {
+    if (!d || !d->coefs_d || !d->omega_d || !d->kx_d || !d->ky_d || !d->workspace_d) return OCS_ERR_ARG;
+    const int nx = d->nx, ny = d->ny;
+    if (nx < 2 || ny < 2 || d->nfields < 1 || d->nfields > 2 * kMaxPacked) return OCS_ERR_ARG;
+    if (nx > 8192 || ny > 8192) return OCS_ERR_SIZE;
+    SurfaceArgs a;
+    memset(&a, 0, sizeof(a));
+    a.nx = nx;
+    a.ny = ny;
+    a.coefs = (const float2 *)d->coefs_d;
+    a.omega = d->omega_d;
+    a.kx = d->kx_d;
+    a.ky = d->ky_d;
+    a.kmin_half = d->kmin_half;
+    a.t = t;
+    a.inv_n = (float)(1.0 / ((double)nx * (double)ny));
+    a.npair = (d->nfields + 1) / 2;
+    for (int i = 0; i < 2 * a.npair; ++i) {
+        if (i < d->nfields) {
+            if (d->codes[i] < 0 || d->codes[i] >= OCS_FIELD_COUNT || !d->dst_d[i]) return OCS_ERR_ARG;
+            a.code[i] = d->codes[i];
+            a.dst[i] = d->dst_d[i];
+            a.add[i] = d->add ? d->add[i] : 0.f;
+            a.swm[i] = d->swell_mult ? make_float2(d->swell_mult[2 * i], d->swell_mult[2 * i + 1])
+                                     : make_float2(0.f, 0.f);
+        } else {
+            a.code[i] = -1;
+            a.dst[i] = nullptr;
+        }
+    }
+    a.swell_exp = (const float2 *)d->swell_exp_d;
+    a.swell_rot = make_float2(d->swell_rot_re, d->swell_rot_im);
+    if (!make_plan(nx, a.px) || !make_plan(ny, a.py)) return OCS_ERR_UNSUPPORTED;
+    char *ws = (char *)d->workspace_d;
+    a.px.tw = (const float2 *)(ws + ws_twx(nx));
+    a.py.tw = (const float2 *)(ws + ws_twy(nx));
+    a.scratch = (float2 *)(ws + ws_scratch(nx, ny));
+    cudaStream_t st = (cudaStream_t)stream;
+
+    cudaError_t e = launch_rows(a, st);
+    if (e != cudaSuccess) return e == cudaErrorInvalidValue ? OCS_ERR_SIZE : OCS_ERR_CUDA;
+    e = launch_cols(a, st);
+    if (e != cudaSuccess) return e == cudaErrorInvalidValue ? OCS_ERR_SIZE : OCS_ERR_CUDA;
+    return OCS_OK;
+}
+
+extern "C" int ocs_surface_choppy(const ocs_choppy_desc *d, void *stream) {
+    if (!d || d->n <= 0 || !d->ax_d || !d->ay_d || !d->axx_d || !d->ayy_d) return OCS_ERR_ARG;
+    ChoppyArgs c;
+    memset(&c, 0, sizeof(c));
+    c.n = d->n;
+    c.ax = d->ax_d; c.ay = d->ay_d; c.axx = d->axx_d; c.ayy = d->ayy_d;
+    c.axxx = d->axxx_d; c.ayyy = d->ayyy_d; c.axxy = d->axxy_d;
+    c.fxx = d->fxx_d; c.fyy = d->fyy_d; c.fxy = d->fxy_d;
+    c.diffx = d->diffx_d; c.diffy = d->diffy_d;
+    c.diffxx = d->diffxx_d; c.diffyy = d->diffyy_d; c.diffxy = d->diffxy_d;
+    if ((c.diffx == nullptr) != (c.diffy == nullptr)) return OCS_ERR_ARG;
+    if (c.diffxx && (!c.diffyy || !c.diffxy || !c.axxx || !c.ayyy || !c.axxy || !c.fxx || !c.fyy || !c.fxy))
+        return OCS_ERR_ARG;
+    c.swell_exp = (const float2 *)d->swell_exp_d;
+    c.swell_rot = make_float2(d->swell_rot_re, d->swell_rot_im);
+    const float *m = d->swell_mult;
+    if (m) {
+        c.sw_dx = make_float2(m[0], m[1]); c.sw_dy = make_float2(m[2], m[3]);
+        c.sw_dxx = make_float2(m[4], m[5]); c.sw_dyy = make_float2(m[6], m[7]);
+        c.sw_dxy = make_float2(m[8], m[9]);
+    }
+    long long blocks = (d->n + 255) / 256;
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    surface_choppy_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(c);
+    return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
+}
