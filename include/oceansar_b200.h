@@ -127,6 +127,106 @@ typedef struct {
 /* Choppy-wave slopes / curvatures from the auxiliary fields (ocean.py:451-456, 468-482). */
 int ocs_surface_choppy(const ocs_choppy_desc *desc, void *stream);
 
+/* ------------------------------------------------------------------------------------
+ * One radar pulse of the raw-data generator.
+ *
+ * Replaces the body of the azimuth loop of sar_raw (oceansar/radarsim/sar_raw_nompi.py:
+ * 351-535) once the surface fields of the pulse exist: slant range (:366-369), Kodis
+ * specular field (:392-400, nrcs/kodis.py:38-73), Romeiser Bragg RCS refreshed when
+ * `refresh` is set (:431-458, nrcs/romeiser97.py:252-393), Bragg phases and random
+ * sub-grid scatterers (:470-480, closure/random_scatterers.py:28-31), antenna pattern and
+ * ATI / XTI channel phases (:485-495, radarsim/antenna.py:5-25), accumulated into range
+ * bins (chan_profile_numba).  All device arrays stay resident between pulses.
+ */
+enum { OCS_PREC_F64 = 0, OCS_PREC_MIXED = 1 };
+enum { OCS_POL_VV = 0, OCS_POL_HH = 1, OCS_POL_DP = 2 };
+enum { OCS_SPREAD_ELFOUHAILY = 0, OCS_SPREAD_COS2S = 1 };
+
+typedef struct {
+    int32_t nx, ny;                      /* facet grid                                       */
+    int32_t npol;                        /* 1, or 2 for pol == OCS_POL_DP (hh then vv)       */
+    int32_t pol;                         /* OCS_POL_*                                       */
+    int32_t nch;                         /* channels, <= 8                                  */
+    /* float32 [ny][nx] surface fields of this pulse */
+    const float *dx_d, *dy_d, *dz_d, *diffx_d, *diffy_d, *diffxx_d, *diffyy_d, *diffxy_d, *hmtf_d;
+    const float *y_d;                    /* float32 [ny] azimuth coordinate of each row      */
+    /* float64 [nx] per ground-range column: slant range minus its minimum, sin / cos / tan
+     * of the incidence angle, incidence angle, Bragg phase speed sin(inc) sqrt(g/kb + ...) */
+    const double *sr_col_d, *sin_inc_d, *cos_inc_d, *tan_inc_d, *inc_d, *c_b_d;
+    double inc_angle;                    /* nominal incidence [rad]                          */
+    double sr0, gr0;                     /* slant / ground range of the scene centre         */
+    double k0, f0;                       /* radar wavenumber, carrier frequency              */
+    double az_now;                       /* (t_now - t_span/2) * v_ground                    */
+    double min_sr, binsize;              /* range window start, range bin size               */
+    double t_step;                       /* 1 / prf                                          */
+    int32_t az_step, az_steps;           /* this pulse, pulses in the raw cube               */
+    int64_t tind;                        /* int(t_now * prf) of the scatterer series         */
+    double ant_l_tx, ant_l_rx;           /* antenna lengths                                  */
+    const double *b_ati, *b_xti;         /* host [nch] along- / cross-track baselines        */
+    int32_t do_kodis, do_bragg, refresh, use_hmtf;
+    double kodis_R_re, kodis_R_im;       /* (eps - sqrt eps)/(eps + sqrt eps), eps = 73+18j  */
+    float facet_dx, facet_dy;            /* surface dx, dy (float32)                         */
+    double bragg_d;                      /* Bragg filter threshold d                         */
+    double wind_dir, wind_U;             /* effective wind for the Bragg spectrum            */
+    int32_t spread;                      /* OCS_SPREAD_*                                     */
+    double spread_ck_p, spread_ck_m, spread_a0, spread_ap, spread_am;  /* Elfouhaily Delta(k) */
+    const double *spec_k_d, *spec_s_d;   /* float64 [spec_n] omni-directional spectrum table */
+    int32_t spec_n;
+    double sqrt_eps_re, sqrt_eps_im;     /* sqrt(73+18j)                                     */
+    void *scat_d;                        /* [npol][2][ny][nx] sqrt(RCS): float64 (F64) or float32 (MIXED) */
+    const double *s_m_d, *s_p_d;         /* complex128 scatterer series (rndscat_m, rndscat_p) */
+    int64_t n_m, n_p;
+    const int32_t *ind0_m_d, *ind0_p_d;  /* int32 [ny][nx] start indices                     */
+    const float *sinc_d;                 /* float32 [161] calc_sinc_vec(8, 20, over_fs)      */
+    void *raw_d;                         /* [npol*nch][az_steps][nbins] complex128 (F64) / complex64 (MIXED) */
+    int32_t nbins;                       /* rg_samp                                          */
+    double *nrcs_spec_d;                 /* float64 [az_steps]: += sum |E_spec|^2            */
+    double *nrcs_bragg_d;                /* float64 [npol][az_steps]: += sum RCS at refresh  */
+} ocs_pulse_desc;
+
+/* Accumulate one pulse into raw_d (OCS_PREC_F64: the float64 drop-in; OCS_PREC_MIXED:
+ * float64 range / phase reduction, float32 elsewhere). */
+int ocs_pulse(const ocs_pulse_desc *desc, int precision, void *stream);
+
+/* ------------------------------------------------------------------------------------
+ * Standalone NRCS models (float64).
+ *
+ * ocs_rcs_romeiser replaces RCSRomeiser97.rcs / rcs_numba (oceansar/nrcs/romeiser97.py:
+ * 95-107, 252-393) on a [ny][nx] grid: out_*_d[l][y][x] is the RCS of Bragg line l.
+ * Azimuth and incidence angles are read at az_d[y*az_row_stride + x*az_col_stride] (and
+ * likewise inc_d), so a [ny] column vector uses strides (1, 0) and a [nx] row (0, 1).
+ */
+typedef struct {
+    int32_t nx, ny;
+    const double *az_d;  int64_t az_row_stride, az_col_stride;
+    const double *inc_d; int64_t inc_row_stride, inc_col_stride;
+    const double *diffx_d, *diffy_d;     /* float64 [ny][nx] slopes                          */
+    double k0, d, dx, dy, wind_dir, wind_U;
+    int32_t pol, spread;                 /* OCS_POL_*, OCS_SPREAD_*                          */
+    double spread_ck_p, spread_ck_m, spread_a0, spread_ap, spread_am;
+    const double *spec_k_d, *spec_s_d;   /* omni-directional spectrum table                  */
+    int32_t spec_n;
+    double sqrt_eps_re, sqrt_eps_im;
+    double *out_hh_d, *out_vv_d;         /* float64 [2][ny][nx] each, or NULL                */
+} ocs_rcs_desc;
+
+int ocs_rcs_romeiser(const ocs_rcs_desc *desc, void *stream);
+
+/* ocs_field_kodis replaces RCSKodis.field (oceansar/nrcs/kodis.py:38-73): complex128
+ * [ny][nx] specular field for float32 slopes / curvatures and float64 slant range. */
+typedef struct {
+    int32_t nx, ny;
+    const double *az_d; int64_t az_row_stride, az_col_stride;
+    const double *sin_inc_d, *cos_inc_d, *tan_inc_d;   /* float64 [nx]                       */
+    const double *sr_d;                                /* float64 [ny][nx]                   */
+    const float *diffx_d, *diffy_d, *diffxx_d, *diffyy_d, *diffxy_d;
+    double k0, R_re, R_im;
+    double dx, dy;                                     /* facet sizes (stationary-point window) */
+    double *out_d;                                     /* complex128 [ny][nx]                */
+} ocs_kodis_desc;
+
+int ocs_field_kodis(const ocs_kodis_desc *desc, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

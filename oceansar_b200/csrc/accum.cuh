@@ -42,12 +42,13 @@ struct CtaBins {
     T *acc;          // [NOUT][nbw][2]
     int cta_base;
     int nbw;
+    int nout;        // outputs in use (<= NOUT); the others are never written
     int nbins;       // valid output bins [0, nbins)
     T *out;          // global output, output o at out + 2*o*out_stride
     long long out_stride;
 
     __device__ void add(int o, int b, T re, T im) {
-        if (b < 0 || b >= nbins) return;
+        if (o >= nout || b < 0 || b >= nbins) return;
         int lb = b - cta_base;
         if (lb >= 0 && lb < nbw) {
             atomicAdd(&acc[(o * nbw + lb) * 2], re);
@@ -64,7 +65,7 @@ struct CtaBins {
 
     // After a __syncthreads(): add the CTA's bins to global memory.
     __device__ void flush_to_global() {
-        for (int i = threadIdx.x; i < NOUT * nbw; i += blockDim.x) {
+        for (int i = threadIdx.x; i < nout * nbw; i += blockDim.x) {
             int o = i / nbw, lb = i % nbw;
             int b = cta_base + lb;
             if (b < 0 || b >= nbins) continue;

@@ -39,6 +39,7 @@ chan_profile_kernel(const double *__restrict__ srg, const cplx<T> *__restrict__ 
     CtaBins<T, 1> cb;
     cb.acc = acc;
     cb.nbw = cta_nbw;
+    cb.nout = 1;
     cb.nbins = nbins;
     cb.out = out + 2 * row * out_row_stride;
     cb.out_stride = 0;

@@ -1,0 +1,354 @@
+// One radar pulse of the raw-data generator on sm_100a: the body of the azimuth loop of
+// sar_raw (oceansar/radarsim/sar_raw_nompi.py:349-535) after the surface update, fused
+// into one kernel per pulse so that no per-facet intermediate ever reaches HBM:
+//
+//   slant range of every facet (:366-369), Kodis specular field (:392-400),
+//   Romeiser Bragg RCS refreshed every ocean_dt (:431-458, stored as sqrt(RCS) between
+//   refreshes), Bragg phases + random sub-grid scatterers (:470-480), antenna pattern and
+//   per-channel ATI / XTI phases (:485-495), and the range-profile accumulation
+//   (range_profile.py:83-116) through the register-window engine of accum.cuh.
+//
+// Layout: a CTA owns BX consecutive ground-range columns (one per thread) and a strip of
+// rows; each thread walks its column down the strip, so a warp reads 32 consecutive
+// float32 of every field (coalesced) and its range bins drift slowly, keeping the
+// register windows warm.  Per-row quantities (azimuth, antenna pattern, ATI phase) are
+// computed once per CTA into shared memory.
+//
+// Precision forms (template T):
+//   double -- the drop-in: every operation in float64 in the reference's order; slant
+//             range and the bin / LUT indices bit-identical to numpy.
+//   float  -- mixed: slant range, bin / LUT indices and the 2 k0 r phase reduction in
+//             float64, everything else (NRCS, scene, accumulation) in float32.
+#include <string.h>
+
+#include "accum.cuh"
+#include "physics.cuh"
+
+namespace ocs {
+
+constexpr int kPulseCols = 128;     // columns (threads) per CTA
+constexpr int kPulseRows = 64;      // rows per CTA strip
+constexpr int kMaxCh = 8;
+constexpr int kPulseNbw = 160;      // CTA shared bin window
+
+struct PulseArgs {
+    int nx, ny, npol, nch;
+    int out0, nout;                         // outputs [out0, out0+nout) of npol*nch, o = pol*nch + ch
+    const float *dx_f, *dy_f, *dz_f, *diffx, *diffy, *diffxx, *diffyy, *diffxy, *hmtf;
+    const float *y;                         // [ny] float32 azimuth coordinates
+    const double *sr_col, *sin_inc, *cos_inc, *tan_inc, *inc, *c_b;   // [nx]
+    double inc_angle, sr0, gr0, k0, az_now, min_sr, binsize, t_step;
+    int az_step;
+    long long tind;                         // int(t_now * prf)
+    double ltx_over_l, lrx_over_l;          // antenna length / wavelength
+    double b_ati[kMaxCh], b_xti[kMaxCh];
+    int do_kodis, do_bragg, refresh, use_hmtf;
+    KodisParams kodis;
+    RomeiserParams rom;
+    void *scat;                             // [npol][2][ny][nx] sqrt(RCS) (T)
+    const double *s_m, *s_p;                // complex128 random-scatterer series
+    long long n_m, n_p;
+    const int *ind0_m, *ind0_p;             // [ny][nx]
+    const float *sinc;                      // [8*20 + 1]
+    void *raw;                              // [npol*nch][az_steps][rg_samp] complex T
+    long long raw_out_stride, raw_row;      // elements between outputs, offset of this pulse row
+    int nbins;
+    double *nrcs_spec;                      // [az_steps]  sum |E_spec|^2
+    double *nrcs_bragg;                     // [npol][az_steps] sum RCS (refresh pulses)
+    int az_steps;
+};
+
+template <typename T> OCS_D cplx<T> cexp_phase(double ph);
+template <> OCS_D cplx<double> cexp_phase<double>(double ph) { return cexpi(ph); }
+template <> OCS_D cplx<float> cexp_phase<float>(double ph) { return cexpi((float)reduce_2pi(ph)); }
+
+// Block-wide sum of a double; thread 0 adds it to *dst.
+OCS_D void block_atomic_sum(double v, double *dst, double *sred) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sred[w] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += sred[i];
+        if (s != 0.0) atomicAdd(dst, s);
+    }
+}
+
+template <typename T, int NOUT, int S>
+__global__ void __launch_bounds__(kPulseCols)
+pulse_kernel(const __grid_constant__ PulseArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr int noff = S - kSincTaps + 1;
+    constexpr int wtab_len = noff * (kSincOvs + 1) * S;
+    T *wtab = reinterpret_cast<T *>(smem);
+    T *bins = wtab + wtab_len;                                        // [NOUT][nbw][2]
+    double *r_az = reinterpret_cast<double *>(bins + NOUT * kPulseNbw * 2);
+    double *r_sinaz = r_az + kPulseRows;
+    double *r_azp = r_sinaz + kPulseRows;
+    double *r_cazp = r_azp + kPulseRows;
+    double *r_sazp = r_cazp + kPulseRows;
+    cplx<T> *r_fac = reinterpret_cast<cplx<T> *>(r_sazp + kPulseRows);   // [rows][nch]
+    double *sred = reinterpret_cast<double *>(r_fac + kPulseRows * a.nch);
+
+    const int x = blockIdx.x * kPulseCols + threadIdx.x;
+    const int y0 = blockIdx.y * kPulseRows;
+    const int nrows = min(kPulseRows, a.ny - y0);
+
+    build_wtab<T, S>(wtab, a.sinc, kSincTaps, kSincOvs);
+    // per-row quantities (sar_raw_nompi.py:353-363, 485-493)
+    for (int i = threadIdx.x; i < nrows; i += blockDim.x) {
+        const double az = dsub((double)a.y[y0 + i], a.az_now);
+        const double sin_az = ddiv(az, a.sr0);
+        const double azp = asin(az / a.gr0);
+        r_az[i] = az;
+        r_sinaz[i] = sin_az;
+        r_azp[i] = azp;
+        r_cazp[i] = cos(azp);
+        r_sazp[i] = sin(azp);
+        const double bp = np_sinc(a.ltx_over_l * sin_az) * np_sinc(a.lrx_over_l * sin_az);
+        for (int c = 0; c < a.nch; ++c) {
+            const c128 ati = cexpi((-a.k0 * a.b_ati[c]) * sin_az);
+            r_fac[i * a.nch + c] = {(T)(bp * ati.re), (T)(bp * ati.im)};
+        }
+    }
+
+    CtaBins<T, NOUT> cb;
+    cb.acc = bins;
+    cb.nbw = kPulseNbw;
+    cb.nout = a.nout;
+    cb.nbins = a.nbins;
+    cb.out = reinterpret_cast<T *>(a.raw) + 2 * ((long long)a.out0 * a.raw_out_stride + a.raw_row);
+    cb.out_stride = a.raw_out_stride;
+    {
+        // window base: bin of this CTA's first column at its first row, undisplaced
+        const int xc = min(blockIdx.x * kPulseCols, a.nx - 1);
+        const double az = (double)a.y[y0] - a.az_now;
+        const double srg = a.sr_col[xc] + az * 0.5 * (az / a.sr0);
+        cb.cta_base = (int)floor((srg - a.min_sr) / a.binsize) - 24;
+    }
+    cb.zero();
+    __syncthreads();
+
+    BinWindow<T, S, NOUT> win;
+    win.reset();
+    double spec_sum = 0.0, bragg_sum[2] = {0.0, 0.0};
+    if (x < a.nx) {
+        const double sr_c = a.sr_col[x], sin_i = a.sin_inc[x], cos_i = a.cos_inc[x];
+        const double inc_c = a.inc[x];
+        const double dinc0 = inc_c - a.inc_angle;
+        const double tan_i = a.do_kodis ? a.tan_inc[x] : 0.0;
+        const double cap = a.do_bragg ? ((2.0 * a.k0) * a.t_step) * a.c_b[x] * (double)(a.az_step + 1) : 0.0;
+        const double two_k0 = 2.0 * a.k0;
+        const long long npix = (long long)a.nx * a.ny;
+        T *scat = reinterpret_cast<T *>(a.scat);
+        for (int i = 0; i < nrows; ++i) {
+            const int yy = y0 + i;
+            const long long idx = (long long)yy * a.nx + x;
+            const float fdx = a.dx_f[idx], fdy = a.dy_f[idx], fdz = a.dz_f[idx];
+            const double az = r_az[i], sin_az = r_sinaz[i];
+            // slant range: sr - cos_inc*Dz + az/2*sin_az + Dx*sin_inc + Dy*sin_az, float64,
+            // left to right, no fused multiply-adds (bit-identical with numpy)
+            double srs = dsub(sr_c, dmul(cos_i, (double)fdz));
+            srs = dadd(srs, dmul(az * 0.5, sin_az));
+            srs = dadd(srs, dmul((double)fdx, sin_i));
+            srs = dadd(srs, dmul((double)fdy, sin_az));
+            int bin_d, lut;
+            bin_and_lut(srs, a.min_sr, a.binsize, kSincOvs, bin_d, lut);
+
+            cplx<T> scene[2] = {{(T)0, (T)0}, {(T)0, (T)0}};      // per polarisation
+            if (a.do_kodis) {
+                const cplx<T> e = kodis_facet<T>(a.kodis, srs, sin_i, cos_i, tan_i, r_cazp[i], r_sazp[i],
+                                                 a.diffx[idx], a.diffy[idx], a.diffxx[idx], a.diffyy[idx],
+                                                 a.diffxy[idx]);
+                const T s4 = (T)3.5449077018110318;                 // sqrt(4 pi)
+                const cplx<T> es = {e.re * s4, e.im * s4};
+                scene[0] = es;
+                scene[1] = es;
+                spec_sum += (double)es.re * es.re + (double)es.im * es.im;
+            }
+            if (a.do_bragg) {
+                T sc[2][2];                                            // [pol][line]
+                if (a.refresh) {
+                    T hh[2], vv[2];
+                    romeiser_facet<T>(a.rom, (T)inc_c, (T)r_azp[i], (T)r_cazp[i], (T)r_sazp[i],
+                                      (T)a.diffx[idx], (T)a.diffy[idx], hh, vv);
+                    if (a.use_hmtf) {
+                        float hm = a.hmtf[idx];
+                        hm = hm < -1.f ? -1.f : hm;
+                        const T f = (T)(1.f + hm);
+                        hh[0] *= f; hh[1] *= f; vv[0] *= f; vv[1] *= f;
+                    }
+                    for (int p = 0; p < a.npol; ++p) {
+                        const T *r = (a.rom.pol == POL_VV || (a.rom.pol == POL_DP && p == 1)) ? vv : hh;
+                        bragg_sum[p] += (double)r[0] + (double)r[1];
+                        sc[p][0] = tsqrt(r[0]);
+                        sc[p][1] = tsqrt(r[1]);
+                        scat[(2 * p) * npix + idx] = sc[p][0];
+                        scat[(2 * p + 1) * npix + idx] = sc[p][1];
+                    }
+                } else {
+                    for (int p = 0; p < a.npol; ++p) {
+                        sc[p][0] = scat[(2 * p) * npix + idx];
+                        sc[p][1] = scat[(2 * p + 1) * npix + idx];
+                    }
+                }
+                // Bragg phases: -2 k0 r -/+ 2 k0 t_step c_b (az_step + 1)
+                const double surf = (-two_k0) * srs;
+                const cplx<T> e0 = cexp_phase<T>(surf - cap);
+                const cplx<T> e1 = cexp_phase<T>(surf + cap);
+                const int i0 = (int)(((long long)a.ind0_m[idx] + a.tind) % a.n_m);
+                const int i1 = (int)(((long long)a.ind0_p[idx] + a.tind) % a.n_p);
+                const cplx<T> sm = {(T)a.s_m[2 * i0], (T)a.s_m[2 * i0 + 1]};
+                const cplx<T> sp = {(T)a.s_p[2 * i1], (T)a.s_p[2 * i1 + 1]};
+                for (int p = 0; p < a.npol; ++p) {
+                    const cplx<T> l0 = cmul(cplx<T>{sc[p][0] * e0.re, sc[p][0] * e0.im}, sm);
+                    const cplx<T> l1 = cmul(cplx<T>{sc[p][1] * e1.re, sc[p][1] * e1.im}, sp);
+                    scene[p] = cadd(scene[p], cadd(l0, l1));
+                }
+            }
+            // channels of this pass: antenna pattern x ATI phase (per row) x XTI phase
+            cplx<T> coef[NOUT];
+            double wave_dinc = 0.0;
+            bool need_dinc = false;
+#pragma unroll
+            for (int k = 0; k < NOUT; ++k) {
+                const int o = a.out0 + k;
+                if (k < a.nout && a.b_xti[o % a.nch] != 0.0) need_dinc = true;
+            }
+            if (need_dinc) wave_dinc = ((double)fdz * sin_i + (double)fdx * sin_i) / a.sr0;
+#pragma unroll
+            for (int k = 0; k < NOUT; ++k) {
+                if (k < a.nout) {
+                    const int o = a.out0 + k;
+                    const int p = o / a.nch, c = o - p * a.nch;
+                    cplx<T> v = cmul(scene[p], r_fac[i * a.nch + c]);
+                    if (a.b_xti[c] != 0.0) {
+                        const double ph = (-a.k0 * a.b_xti[c]) * (dinc0 + wave_dinc);
+                        v = cmul(v, cexp_phase<T>(ph));
+                    }
+                    coef[k] = v;
+                } else {
+                    coef[k] = {(T)0, (T)0};
+                }
+            }
+            if (bin_d > -(1 << 29))
+                win.add(bin_d - kSincTaps / 2, lut, coef, wtab, a.sinc, kSincTaps, kSincOvs, cb);
+        }
+    }
+    win.flush(cb);
+    __syncthreads();
+    cb.flush_to_global();
+    // NRCS bookkeeping (only the first output group accumulates it)
+    if (a.out0 == 0) {
+        if (a.do_kodis) block_atomic_sum(spec_sum, &a.nrcs_spec[a.az_step], sred);
+        if (a.do_bragg && a.refresh)
+            for (int p = 0; p < a.npol; ++p)
+                block_atomic_sum(bragg_sum[p], &a.nrcs_bragg[(long long)p * a.az_steps + a.az_step], sred);
+    }
+}
+
+template <typename T, int NOUT, int S>
+static int launch_pulse(const PulseArgs &a, cudaStream_t st) {
+    constexpr int noff = S - kSincTaps + 1;
+    constexpr int wtab_len = noff * (kSincOvs + 1) * S;
+    size_t smem = (size_t)wtab_len * sizeof(T) + (size_t)NOUT * kPulseNbw * 2 * sizeof(T) +
+                  5 * kPulseRows * sizeof(double) + (size_t)kPulseRows * a.nch * sizeof(cplx<T>) +
+                  32 * sizeof(double);
+    auto k = pulse_kernel<T, NOUT, S>;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return OCS_ERR_CUDA;
+    dim3 grid((a.nx + kPulseCols - 1) / kPulseCols, (a.ny + kPulseRows - 1) / kPulseRows);
+    k<<<grid, kPulseCols, smem, st>>>(a);
+    return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
+}
+
+}  // namespace ocs
+
+using namespace ocs;
+
+static int fill_pulse_args(const ocs_pulse_desc *d, PulseArgs &a) {
+    memset(&a, 0, sizeof(a));
+    if (!d || d->nx < 1 || d->ny < 1 || d->npol < 1 || d->npol > 2 || d->nch < 1 || d->nch > kMaxCh)
+        return OCS_ERR_ARG;
+    if (!d->dx_d || !d->dy_d || !d->dz_d || !d->y_d || !d->sr_col_d || !d->sin_inc_d || !d->cos_inc_d ||
+        !d->inc_d || !d->sinc_d || !d->raw_d)
+        return OCS_ERR_ARG;
+    if (d->do_kodis && (!d->diffx_d || !d->diffy_d || !d->diffxx_d || !d->diffyy_d || !d->diffxy_d ||
+                        !d->tan_inc_d || !d->nrcs_spec_d))
+        return OCS_ERR_ARG;
+    if (d->do_bragg && (!d->diffx_d || !d->diffy_d || !d->c_b_d || !d->scat_d || !d->s_m_d || !d->s_p_d ||
+                        !d->ind0_m_d || !d->ind0_p_d || d->n_m < 1 || d->n_p < 1 || !d->spec_k_d ||
+                        !d->spec_s_d || d->spec_n < 2 || !d->nrcs_bragg_d))
+        return OCS_ERR_ARG;
+    if (d->do_bragg && d->use_hmtf && !d->hmtf_d) return OCS_ERR_ARG;
+    if (d->az_step < 0 || d->az_step >= d->az_steps || d->nbins < 1) return OCS_ERR_ARG;
+    if ((d->npol == 2) != (d->pol == POL_DP)) return OCS_ERR_ARG;
+    a.nx = d->nx; a.ny = d->ny; a.npol = d->npol; a.nch = d->nch;
+    a.dx_f = d->dx_d; a.dy_f = d->dy_d; a.dz_f = d->dz_d;
+    a.diffx = d->diffx_d; a.diffy = d->diffy_d;
+    a.diffxx = d->diffxx_d; a.diffyy = d->diffyy_d; a.diffxy = d->diffxy_d; a.hmtf = d->hmtf_d;
+    a.y = d->y_d;
+    a.sr_col = d->sr_col_d; a.sin_inc = d->sin_inc_d; a.cos_inc = d->cos_inc_d; a.tan_inc = d->tan_inc_d;
+    a.inc = d->inc_d; a.c_b = d->c_b_d;
+    a.inc_angle = d->inc_angle; a.sr0 = d->sr0; a.gr0 = d->gr0; a.k0 = d->k0; a.az_now = d->az_now;
+    a.min_sr = d->min_sr; a.binsize = d->binsize; a.t_step = d->t_step; a.az_step = d->az_step;
+    a.tind = d->tind;
+    a.ltx_over_l = d->ant_l_tx * d->f0 / 2.99792458e8;
+    a.lrx_over_l = d->ant_l_rx * d->f0 / 2.99792458e8;
+    for (int c = 0; c < d->nch; ++c) { a.b_ati[c] = d->b_ati[c]; a.b_xti[c] = d->b_xti[c]; }
+    a.do_kodis = d->do_kodis; a.do_bragg = d->do_bragg; a.refresh = d->refresh; a.use_hmtf = d->use_hmtf;
+    a.kodis.k0 = d->k0;
+    a.kodis.R_re = d->kodis_R_re; a.kodis.R_im = d->kodis_R_im;
+    a.kodis.hdx = (double)d->facet_dx * 0.5; a.kodis.hdy = (double)d->facet_dy * 0.5;
+    RomeiserParams &r = a.rom;
+    r.k0 = d->k0; r.d = d->bragg_d; r.dx = (double)d->facet_dx; r.dy = (double)d->facet_dy;
+    r.wind_dir = d->wind_dir; r.wind_U = d->wind_U; r.pol = d->pol; r.spread = d->spread;
+    r.ck_p = d->spread_ck_p; r.ck_m = d->spread_ck_m; r.a0 = d->spread_a0; r.ap = d->spread_ap;
+    r.am = d->spread_am;
+    r.tab_k = d->spec_k_d; r.tab_s = d->spec_s_d; r.tab_n = d->spec_n;
+    r.eps_re = 73.0; r.eps_im = 18.0;
+    r.seps_re = d->sqrt_eps_re; r.seps_im = d->sqrt_eps_im;
+    r.eps2_re = 73.0 * 73.0 - 18.0 * 18.0; r.eps2_im = 2.0 * 73.0 * 18.0;
+    a.scat = d->scat_d; a.s_m = d->s_m_d; a.s_p = d->s_p_d; a.n_m = d->n_m; a.n_p = d->n_p;
+    a.ind0_m = d->ind0_m_d; a.ind0_p = d->ind0_p_d;
+    a.sinc = d->sinc_d;
+    a.raw = d->raw_d;
+    a.nbins = d->nbins;
+    a.raw_out_stride = (long long)d->az_steps * d->nbins;
+    a.raw_row = (long long)d->az_step * d->nbins;
+    a.nrcs_spec = d->nrcs_spec_d; a.nrcs_bragg = d->nrcs_bragg_d; a.az_steps = d->az_steps;
+    return OCS_OK;
+}
+
+extern "C" int ocs_pulse(const ocs_pulse_desc *d, int precision, void *stream) {
+    PulseArgs a;
+    int st = fill_pulse_args(d, a);
+    if (st != OCS_OK) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nout = d->npol * d->nch;
+    if (precision == OCS_PREC_F64) {
+        for (int o = 0; o < nout; o += 2) {
+            a.out0 = o;
+            a.nout = nout - o < 2 ? nout - o : 2;
+            st = (a.nout == 1) ? launch_pulse<double, 1, 12>(a, s) : launch_pulse<double, 2, 12>(a, s);
+            if (st != OCS_OK) return st;
+            a.refresh = 0;                  // later groups read the refreshed RCS
+        }
+        return OCS_OK;
+    }
+    if (precision == OCS_PREC_MIXED) {
+        for (int o = 0; o < nout; o += 4) {
+            a.out0 = o;
+            a.nout = nout - o < 4 ? nout - o : 4;
+            if (a.nout == 1) st = launch_pulse<float, 1, 16>(a, s);
+            else if (a.nout == 2) st = launch_pulse<float, 2, 16>(a, s);
+            else st = launch_pulse<float, 4, 12>(a, s);
+            if (st != OCS_OK) return st;
+            a.refresh = 0;
+        }
+        return OCS_OK;
+    }
+    return OCS_ERR_ARG;
+}

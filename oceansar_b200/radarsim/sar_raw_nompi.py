@@ -1,0 +1,319 @@
+"""The raw-data generator ``sar_raw`` (``oceansar/radarsim/sar_raw_nompi.py:32-641``) on the GPU.
+
+``RawGenerator`` does the reference's set-up on the host -- in the same order, so that the
+global numpy RNG produces the same surface, the same random scatterer series and the same
+noise for the same seed -- and then keeps everything per pulse on the device:
+
+* ``OceanSurface.set_t`` -> ``ocs_surface_update`` (surface fields of the pulse),
+* ``ocs_pulse`` -> slant range, Kodis specular field, Romeiser Bragg RCS (refreshed when
+  ``t_now - t_last > ocean_dt``, ``:432``), Bragg phases and sub-grid scatterers, antenna
+  pattern, ATI / XTI phases and the accumulation into the raw cube.
+
+``precision='f64'`` is the drop-in (float64 throughout, slant range and bin indices
+bit-identical with numpy); ``precision='mixed'`` keeps the slant range, the bin / LUT indices
+and the 2 k0 r phase reduction in float64 and runs the rest in float32, with a complex64
+raw cube.  ``sar_raw`` wraps it with the reference's signature and writes the raw file.
+"""
+import ctypes
+import math
+
+import numpy as np
+import torch
+from scipy import linalg
+
+from .. import _capi, _device, nrcs, swell_spec
+from .._structs import PulseDesc
+from ..closure import grid_coherence, randomscat_ts
+from ..ocs_io.cfg import ConfigFile
+from ..surfaces import OceanSurface
+from ..utils import geometry as geo
+from ..utils.misc import db2lin, optimize_fftsize
+from .range_profile import calc_sinc_vec
+
+C_LIGHT = 2.99792458e8
+G = 9.80665
+PRECISIONS = {'f64': 0, 'mixed': 1}
+
+
+def sinc_bp(sin_angle, L, f0, field=False):
+    """Uniform-aperture pattern (``oceansar/radarsim/antenna.py:5-25``, no squint)."""
+    pattern = np.sinc(L / (C_LIGHT / f0) * sin_angle)
+    return pattern if field else pattern ** 2
+
+
+class RawGenerator(object):
+    """Device-resident state of one ``sar_raw`` scene; see the module docstring.
+
+    ``overrides`` may fix ``az_steps`` / ``rg_samp`` / ``rg_samp_orig`` (the reference
+    derives them from the geometry, ``sar_raw_nompi.py:264-278``).
+    """
+
+    def __init__(self, cfg, precision='f64', overrides=None, seed=None, stream=None):
+        if precision not in PRECISIONS:
+            raise ValueError('precision must be f64 or mixed')
+        self.precision = precision
+        self.stream = stream
+        if isinstance(cfg, str):
+            cfg = ConfigFile(cfg)
+        self.cfg = cfg
+        ov = dict(overrides or {})
+        if seed is not None:
+            np.random.seed(seed)
+        srg, sar, oc = cfg.srg, cfg.sar, cfg.ocean
+        self.nesz = srg.nesz
+        self.wh_tol = srg.wh_tol
+        self.use_hmtf = bool(srg.use_hmtf)
+        self.scat_spec_enable = bool(srg.scat_spec_enable)
+        self.scat_bragg_enable = bool(srg.scat_bragg_enable)
+        if self.scat_spec_enable and srg.scat_spec_mode != 'kodis':
+            if srg.scat_spec_mode in ('fa', 'spa'):
+                raise NotImplementedError('Kirchhoff (fa / spa) specular scattering is not built')
+            raise NotImplementedError('RCS mode %s for specular scattering not implemented' % srg.scat_spec_mode)
+        if self.scat_bragg_enable and srg.scat_bragg_model != 'romeiser97':
+            raise NotImplementedError('RCS model %s for Bragg scattering not implemented' % srg.scat_bragg_model)
+        self.inc_angle = np.deg2rad(sar.inc_angle)
+        self.f0 = f0 = sar.f0
+        self.pol = pol = sar.pol
+        self.do_hh = pol in ('DP', 'hh')
+        self.do_vv = pol not in ('hh',)
+        self.npol = 2 if pol == 'DP' else 1
+        self.prf = sar.prf
+        self.num_ch = int(sar.num_ch)
+        if self.num_ch > 8:
+            raise ValueError('at most 8 channels')
+        alt = sar.alt
+        v_ground = sar.v_ground
+        self.rg_bw = sar.rg_bw
+        self.over_fs = sar.over_fs
+        self.ocean_dt = oc.dt
+        self.chan_sinc_vec = calc_sinc_vec(8, 20, Fs=self.over_fs)
+
+        # ---- surface (global RNG draw 1: random_cg, then swell) -------------------------
+        compute = ['D', 'Diff']
+        if self.scat_spec_enable:
+            compute.append('Diff2')
+        if self.use_hmtf:
+            compute.append('hMTF')
+        if hasattr(oc, 'use_buoy_data') and oc.use_buoy_data:
+            raise NotImplementedError('buoy-spectrum input is not built')
+        dir_swell = swell_spec.ardhuin_swell_spec if oc.swell_dir_enable else None
+        s = self.surface = OceanSurface()
+        s.init(oc.Lx, oc.Ly, oc.dx, oc.dy, oc.cutoff_wl, oc.spec_model, oc.spread_model,
+               np.deg2rad(oc.wind_dir), oc.wind_fetch, oc.wind_U, oc.current_mag,
+               np.deg2rad(oc.current_dir), oc.dir_swell_dir, oc.freq_r, oc.sigf, oc.sigs, oc.Hs,
+               oc.swell_dir_enable, oc.swell_enable, oc.swell_ampl, np.deg2rad(oc.swell_dir),
+               oc.swell_wl, compute, oc.opt_res, oc.fft_max_prime, choppy_enable=oc.choppy_enable,
+               depth=oc.depth, dirspectrum_func=None, dir_swell_spec=dir_swell)
+        self.frozen = bool(getattr(oc, 'frozen_ocean', False))
+
+        # ---- geometry (:231-278) ----------------------------------------------------------
+        self.sr0 = sr0 = geo.inc_to_sr(self.inc_angle, alt)
+        self.gr0 = gr0 = geo.inc_to_gr(self.inc_angle, alt)
+        sr, inc, _ = geo.gr_to_geo(s.x + gr0, alt)
+        self.sr_near = sr[0] - self.wh_tol + C_LIGHT / 2 / (self.rg_bw * self.over_fs)
+        sr -= np.min(sr)
+        self.inc = inc.reshape(1, inc.size)
+        self.sr = sr.reshape(1, sr.size)
+        self.sin_inc = np.sin(self.inc)
+        self.cos_inc = np.cos(self.inc)
+        self.k0 = k0 = 2. * np.pi * f0 / C_LIGHT
+        self.sr_res = C_LIGHT / (2. * self.rg_bw)
+        self.ant_l_tx = sar.ant_L_tx
+        self.ant_l_rx = sar.ant_L_rx
+        b_ati = sar.b_ati
+        if not type(b_ati) == np.ndarray:
+            b_ati = np.arange(self.num_ch) * b_ati
+        b_xti = sar.b_xti
+        if not type(b_xti) == np.ndarray:
+            b_xti = np.arange(self.num_ch) * b_xti
+        self.b_ati, self.b_xti = np.asarray(b_ati, float), np.asarray(b_xti, float)
+        if v_ground == 'auto':
+            v_ground = geo.orbit_to_vel(alt, ground=True)
+        self.v_ground = v_ground
+        self.t_step = 1. / self.prf
+        self.t_span = (1.5 * (sr0 * (C_LIGHT / f0) / self.ant_l_tx) + s.Ly) / v_ground
+        self.az_steps = int(ov.get('az_steps', int(np.floor(self.t_span / self.t_step))))
+        max_sr = (np.max(sr) + self.wh_tol + (np.max(s.y) + (self.t_span / 2.) * v_ground) ** 2. / (2. * sr0))
+        self.min_sr = np.min(sr) - self.wh_tol
+        self.rg_samp_orig = int(ov.get('rg_samp_orig',
+                                       int(np.ceil(((max_sr - self.min_sr) / self.sr_res) * self.over_fs))))
+        self.rg_samp = int(ov.get('rg_samp', int(optimize_fftsize(self.rg_samp_orig))))
+        self.surface_area = s.dx * s.dy * s.Nx * s.Ny
+
+        # ---- scattering models (:293-340; global RNG draw 2: rndscat_p then rndscat_m) ---
+        if self.scat_spec_enable:
+            self.rcs_spec = nrcs.RCSKodis(self.inc, k0, s.dx, s.dy)
+        if self.scat_bragg_enable:
+            tau_c = grid_coherence(oc.wind_U, s.dx, f0)
+            self.rndscat_p = randomscat_ts(tau_c, (s.Ny, s.Nx), self.prf)
+            self.rndscat_m = randomscat_ts(tau_c, (s.Ny, s.Nx), self.prf)
+            k_b = 2. * k0 * self.sin_inc
+            self.c_b = self.sin_inc * np.sqrt(G / k_b + 0.072e-3 * k_b)
+            cdir = np.deg2rad(oc.current_dir)
+            cur = oc.current_mag * np.array([np.cos(cdir), np.sin(cdir)])
+            udir = np.deg2rad(oc.wind_dir)
+            u_eff = oc.wind_U * np.array([np.cos(udir), np.sin(udir)]) - cur
+            self.rcs_bragg = nrcs.RCSRomeiser97(k0, self.inc, pol, s.dx, s.dy, linalg.norm(u_eff),
+                                                np.arctan2(u_eff[1], u_eff[0]), s.wind_fetch,
+                                                srg.scat_bragg_spec, srg.scat_bragg_spread,
+                                                srg.scat_bragg_d, rmss_x=s.rmss_x, rmss_y=s.rmss_y,
+                                                use_lut=bool(srg.use_lut))
+        self._alloc()
+        self.t_last_rcs_bragg = -1.
+
+    # ------------------------------------------------------------------------------------
+    def _alloc(self):
+        s = self.surface
+        cdt = np.complex128 if self.precision == 'f64' else np.complex64
+        sdt = np.float64 if self.precision == 'f64' else np.float32
+        nout = self.npol * self.num_ch
+        self.raw_d = _device.zeros((nout, self.az_steps, self.rg_samp), cdt)
+        self.nrcs_spec_d = _device.zeros((self.az_steps,), np.float64)
+        self.nrcs_bragg_d = _device.zeros((self.npol, self.az_steps), np.float64)
+        col = lambda a: _device.to_device(np.ravel(a), np.float64)  # noqa: E731
+        self._cols = dict(sr=col(self.sr), sin=col(self.sin_inc), cos=col(self.cos_inc),
+                          tan=col(np.tan(self.inc)), inc=col(self.inc))
+        self._y_d = _device.to_device(s.y, np.float32)
+        self._sinc_d = _device.to_device(self.chan_sinc_vec, np.float32)
+        self._b_ati = (ctypes.c_double * self.num_ch)(*[float(v) for v in self.b_ati])
+        self._b_xti = (ctypes.c_double * self.num_ch)(*[float(v) for v in self.b_xti])
+        d = self.desc = PulseDesc()
+        d.nx, d.ny, d.npol, d.nch = s.Nx, s.Ny, self.npol, self.num_ch
+        d.pol = nrcs.POL_CODES[self.pol]
+        f = s.field
+        d.dx_d, d.dy_d, d.dz_d = f('Dx').data_ptr(), f('Dy').data_ptr(), f('Dz').data_ptr()
+        d.diffx_d, d.diffy_d = f('Diffx').data_ptr(), f('Diffy').data_ptr()
+        if self.scat_spec_enable:
+            d.diffxx_d, d.diffyy_d, d.diffxy_d = (f('Diffxx').data_ptr(), f('Diffyy').data_ptr(),
+                                                  f('Diffxy').data_ptr())
+        if self.use_hmtf:
+            d.hmtf_d = f('hMTF').data_ptr()
+        d.y_d = self._y_d.data_ptr()
+        c = self._cols
+        d.sr_col_d, d.sin_inc_d, d.cos_inc_d = c['sr'].data_ptr(), c['sin'].data_ptr(), c['cos'].data_ptr()
+        d.tan_inc_d, d.inc_d = c['tan'].data_ptr(), c['inc'].data_ptr()
+        d.inc_angle, d.sr0, d.gr0, d.k0, d.f0 = (float(self.inc_angle), float(self.sr0), float(self.gr0),
+                                                 float(self.k0), float(self.f0))
+        d.min_sr, d.binsize, d.t_step = float(self.min_sr), float(self.sr_res / self.over_fs), float(self.t_step)
+        d.az_steps = self.az_steps
+        d.ant_l_tx, d.ant_l_rx = float(self.ant_l_tx), float(self.ant_l_rx)
+        d.b_ati, d.b_xti = self._b_ati, self._b_xti
+        d.do_kodis, d.do_bragg, d.use_hmtf = int(self.scat_spec_enable), int(self.scat_bragg_enable), \
+            int(self.use_hmtf)
+        d.facet_dx, d.facet_dy = float(s.dx), float(s.dy)
+        if self.scat_spec_enable:
+            d.kodis_R_re, d.kodis_R_im = float(self.rcs_spec.R.real), float(self.rcs_spec.R.imag)
+        if self.scat_bragg_enable:
+            self.rcs_bragg.fill(d)
+            d.bragg_d = float(self.rcs_bragg.d)
+            self._c_b_d = col(self.c_b)
+            d.c_b_d = self._c_b_d.data_ptr()
+            self._scat_d = torch.empty((self.npol, 2, s.Ny, s.Nx), dtype=torch.float64 if sdt == np.float64
+                                       else torch.float32, device=_device.device())
+            d.scat_d = self._scat_d.data_ptr()
+            sm, im = self.rndscat_m.device()
+            sp, ip = self.rndscat_p.device()
+            d.s_m_d, d.s_p_d, d.n_m, d.n_p = sm.data_ptr(), sp.data_ptr(), int(self.rndscat_m.N), \
+                int(self.rndscat_p.N)
+            d.ind0_m_d, d.ind0_p_d = im.data_ptr(), ip.data_ptr()
+        d.sinc_d = self._sinc_d.data_ptr()
+        d.raw_d = self.raw_d.data_ptr()
+        d.nbins = self.rg_samp
+        d.nrcs_spec_d = self.nrcs_spec_d.data_ptr()
+        d.nrcs_bragg_d = self.nrcs_bragg_d.data_ptr()
+        self._refreshes = []
+
+    # ------------------------------------------------------------------------------------
+    def pulse(self, az_step, update_surface=True):
+        """One iteration of the azimuth loop (``sar_raw_nompi.py:349-535``).
+
+        ``update_surface=False`` keeps whatever the surface field buffers hold (used to
+        feed externally computed fields, stage by stage)."""
+        t_now = az_step * self.t_step
+        az_now = (t_now - self.t_span / 2.) * self.v_ground
+        if update_surface and ((not self.frozen) or az_step == 0):
+            # a frozen ocean keeps the t = 0 surface (the reference leaves it unset)
+            self.surface.set_t(t_now, stream=self.stream)
+        d = self.desc
+        d.az_step = int(az_step)
+        d.az_now = float(az_now)
+        d.refresh = 0
+        if self.scat_bragg_enable:
+            d.tind = self.rndscat_m.tind(t_now)
+            if (t_now - self.t_last_rcs_bragg) > self.ocean_dt:
+                d.refresh = 1
+                self.t_last_rcs_bragg = t_now
+                self._refreshes.append(az_step)
+        _capi.call("ocs_pulse", ctypes.addressof(d), PRECISIONS[self.precision],
+                   _device.stream_ptr(self.stream))
+
+    def run(self, steps=None):
+        for a in (range(self.az_steps) if steps is None else steps):
+            self.pulse(a)
+
+    # ------------------------------------------------------------------------------------
+    def nrcs_avg(self):
+        """NRCS_avg[pol, az] (``:427-467``): specular plus Bragg, per unit surface area."""
+        spec = self.nrcs_spec_d.cpu().numpy()
+        bragg = self.nrcs_bragg_d.cpu().numpy()
+        out = np.zeros((self.npol, self.az_steps))
+        last = None
+        filled = np.zeros_like(bragg)
+        for a in range(self.az_steps):
+            if a in self._refreshes:
+                last = a
+            if last is not None:
+                filled[:, a] = bragg[:, last]
+        for p in range(self.npol):
+            if self.scat_spec_enable:
+                out[p] += spec / self.surface_area
+            if self.scat_bragg_enable:
+                out[p] += filled[p] / self.surface_area
+        return out
+
+    def raw(self):
+        """Accumulated raw cube [pol, ch, az, rg_samp] before calibration (host copy)."""
+        r = self.raw_d.cpu().numpy()
+        return r.reshape(self.npol, self.num_ch, self.az_steps, self.rg_samp)
+
+    def finish(self, add_noise=True):
+        """Truncation, calibration factor and noise (``:552-574``) -> (raw, NRCS_avg)."""
+        t_span, v = self.t_span, self.v_ground
+        az_axis = np.arange(-t_span / 2. * v, t_span / 2. * v,
+                            self.sr0 * C_LIGHT / (np.pi * self.f0 * self.ant_l_tx * 10.))
+        pattern = (sinc_bp(az_axis / self.sr0, self.ant_l_tx, self.f0, field=True) *
+                   sinc_bp(az_axis / self.sr0, self.ant_l_rx, self.f0, field=True))
+        self.cal_factor = (1. / np.sqrt(np.trapezoid(np.abs(pattern) ** 2., az_axis) *
+                                        self.sr_res / np.sin(self.inc_angle)))
+        raw = self.raw()[:, :, :, :self.rg_samp_orig].astype(np.complex128)
+        out = []
+        for p in range(self.npol):
+            r = raw[p]
+            noise = 0.
+            if add_noise:
+                noise = (db2lin(self.nesz, amplitude=True) / np.sqrt(2.) *
+                         (np.random.normal(size=r.shape) + 1j * np.random.normal(size=r.shape)))
+            out.append(r * self.cal_factor + noise)
+        return np.stack(out), self.nrcs_avg()
+
+
+def sar_raw(cfg_file, output_file, ocean_file, reuse_ocean_file, errors_file, reuse_errors_file,
+            plot_save=True, precision='f64'):
+    """Drop-in for ``sar_raw_nompi.sar_raw``: simulate and write the raw file.
+
+    The raw file and the ocean state file are ``.npz`` containers holding the reference's
+    variable names (``raw_data_r``/``raw_data_i`` [pol, ch, az, rg], ``NRCS_avg``, ...).
+    ``errors_file`` / ``plot_save`` are accepted and unused, as in the reference.
+    """
+    cfg = ConfigFile(cfg_file)
+    gen = RawGenerator(cfg, precision=precision)
+    if ocean_file and not reuse_ocean_file:
+        gen.surface.save(ocean_file)
+    gen.run()
+    total_raw, nrcs_avg = gen.finish(add_noise=True)
+    if output_file:
+        np.savez(output_file, raw_data_r=total_raw.real, raw_data_i=total_raw.imag, NRCS_avg=nrcs_avg,
+                 inc_angle=np.rad2deg(gen.inc_angle), f0=gen.f0, num_ch=gen.num_ch, ant_L=gen.ant_l_tx,
+                 prf=gen.prf, v_ground=gen.v_ground, orbit_alt=cfg.sar.alt, sr0=gen.sr_near,
+                 rg_sampling=gen.rg_bw * gen.over_fs, rg_bw=gen.rg_bw, b_ati=gen.b_ati, b_xti=gen.b_xti)
+    return total_raw, nrcs_avg

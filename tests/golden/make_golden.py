@@ -198,7 +198,8 @@ def gen_kodis():
     diffy = (0.1 * rs.randn(Ny, Nx)).astype(np.float32)
     diffxx[0, 0] = 1.0; diffyy[0, 0] = 1.0; diffxy[0, 0] = 1.0       # J == 0 exactly
     sr = 1000.0 + rs.uniform(0, 50, (Ny, Nx))
-    y = np.linspace(-100, 100, Ny).astype(np.float32)
+    # float64 azimuth angles, as sar_raw_nompi.py:363 produces them
+    y = np.linspace(-100, 100, Ny).astype(np.float32).astype(np.float64)
     # a full [Ny, Nx] azimuth-angle array: with the [Ny, 1] vector that sar_raw passes,
     # kodis.py:61 raises IndexError as soon as a stationary point lies outside column 0
     az = np.repeat(np.arcsin(y / 3e4).reshape(Ny, 1), Nx, axis=1)
