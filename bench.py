@@ -1,0 +1,409 @@
+"""Benchmark: raw echoes/s (facet x pulse x channel) of the B200 raw-data generator.
+
+Workload (the two-channel along-track case): a 2048 x 2048 linear-wave surface at 1 m
+(Elfouhaily spectrum, cos^2 spreading, U10 = 7 m/s at 45 deg, deep water), C band
+5.405 GHz, 514 km altitude, 7600 m/s, 35 deg incidence, 2 along-track channels with a 10 m
+baseline, 4096 pulses at 1500 Hz, 2048 range bins, Kodis specular + Romeiser Bragg NRCS,
+vv.  Synthetic seeded input (no dataset exists for this path).  One step = one full scene:
+the surface synthesis and the fused pulse kernel for all 4096 pulses, replayed from a CUDA
+graph.  The working set (coefficients, scratch planes, fields, RCS, raw cube) is ~0.5 GB,
+far above the 126 MB L2, so no L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision mixed|f64] [--small]
+
+``--impl reference`` times the CPU restatement of the reference's numba path (the oracle)
+on the host cores, on a bounded window of pulses of the same workload, and prints the same
+JSON line with "impl": "reference".  Multi-GPU runs (torchrun) are replicas: every rank
+simulates its own scene (seed + rank); value = all ranks' echoes / max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "raw echoes/s (facet*pulse*chan)"
+UNIT = "echoes/s"
+
+C2 = dict(name="C-band 2-channel ATI, 2048x2048 surface, 4096 pulses, 2048 bins",
+          L=2048, d=1.0, wind_U=7.0, wind_dir=45.0, prf=1500.0, pulses=4096, bins=2048, num_ch=2,
+          b_ati=10.0, b_xti=0.0, ant_l=2.742, pol="vv", inc=35.0)
+C1 = dict(name="C-band 1-channel, 512x512 surface, 256 pulses, 512 bins",
+          L=512, d=1.0, wind_U=10.0, wind_dir=0.0, prf=1000.0, pulses=256, bins=512, num_ch=1,
+          b_ati=0.0, b_xti=0.0, ant_l=35.7, pol="vv", inc=35.0)
+
+CFG = """[sar]
+f0=5.405e9
+inc_angle={inc}
+pol={pol}
+squint=0
+prf={prf}
+rg_bw=50e6
+over_fs=1.1
+alt=514e3
+v_ground=7600.
+heading=0.
+ant_L_tx={ant_l}
+ant_L_rx={ant_l}
+num_ch={num_ch}
+b_ati={b_ati}
+b_xti={b_xti}
+sigma_n_tx=0.
+phase_n_tx=0.
+sigma_beta_tx=0.
+phase_beta_tx=0.
+sigma_n_rx=0.
+phase_n_rx=0.
+sigma_beta_rx=0.
+phase_beta_rx=0.
+
+[ocean]
+Lx={L}
+Ly={L}
+dx={d}
+dy={d}
+opt_res=True
+fft_max_prime=2
+dt=0.05
+depth=1e5
+wind_dir={wind_dir}
+wind_U={wind_U}
+wind_fetch=500e3
+swell_dir_enable=False
+sigf=0.007
+freq_r=0.079
+dir_swell_dir=120
+sigs=8
+Hs=0.8
+swell_enable=False
+swell_wl=60
+swell_dir=20
+swell_ampl=0.3
+spec_model=elfouhaily
+spread_model=cos2s
+cutoff_wl=auto
+current_mag=0
+current_dir=0.
+choppy_enable=False
+frozen_ocean=False
+
+[srg]
+use_hmtf=False
+nesz=-300.
+wh_tol=2.73
+scat_spec_enable=True
+scat_spec_mode=kodis
+scat_bragg_enable=True
+scat_bragg_model=romeiser97
+scat_bragg_spec=elfouhaily
+scat_bragg_spread=cos2s
+scat_bragg_d=0.125
+use_lut=False
+"""
+
+
+def write_cfg(c, path):
+    with open(path, "w") as f:
+        f.write(CFG.format(**c))
+    return path
+
+
+def overrides(c):
+    return dict(az_steps=c["pulses"], rg_samp=c["bins"], rg_samp_orig=c["bins"])
+
+
+def echoes(c, pulses=None):
+    return float(c["L"] / c["d"]) ** 2 * (c["pulses"] if pulses is None else pulses) * c["num_ch"]
+
+
+# ----------------------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if self.proc is None:
+            return out
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) >= 9:
+                    rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return out
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        out.update(sm_mhz=float(np.median(sm)) if sm else None, sm_max_mhz=max(mx) if mx else None,
+                   reasons=reasons, samples=len(rows))
+        return out
+
+
+# ----------------------------------------------------------------------------------------
+def dist_info():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline(c, cfg_path, pulses, seed=0):
+    """Oracle (CPU restatement of the reference's numba path) over a bounded pulse window."""
+    from oracle.sar_raw import SarRawSim
+    sim = SarRawSim(cfg_path, overrides=overrides(c), seed=seed)
+    sim.pulse(0)                               # JIT-free warm-up (FFT plans, first refresh)
+    t0 = time.perf_counter()
+    for a in range(1, 1 + pulses):
+        sim.pulse(a)
+    dt = time.perf_counter() - t0
+    return echoes(c, pulses) / dt, dt
+
+
+def run_reference(args, c, cfg_path):
+    world, rank, _ = dist_info()
+    if rank != 0:
+        return
+    from oracle.sar_raw import SarRawSim
+    sim = SarRawSim(cfg_path, overrides=overrides(c), seed=0)
+    steps = []
+    pulses = 2 if args.small else 3
+    a = 0
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        for _ in range(pulses):
+            sim.pulse(a % sim.az_steps)
+            a += 1
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            steps.append((echoes(c, pulses) / dt, dt))
+    value = float(np.mean([v for v, _ in steps]))
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": float(np.mean([d for _, d in steps]) * 1e3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": c["name"], "sample": "%d pulses per step" % pulses},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+                             "sample": "%d pulses of the %dx%d scene per step, after one warm-up pulse; "
+                                       "numpy FFT (single thread) + serial C accumulation" %
+                                       (pulses, c["L"], c["L"])},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------------------
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "f64"])
+    ap.add_argument("--small", action="store_true", help="512^2 single-channel case (quick check)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--profile-pulses", type=int, default=0,
+                    help="run this many pulses with plain launches (for ncu) and exit")
+    args = ap.parse_args()
+    c = C1 if args.small else C2
+    tmpd = tempfile.mkdtemp(prefix="ocs_bench_")
+    cfg_path = write_cfg(c, os.path.join(tmpd, "scene.cfg"))
+    if args.impl == "reference":
+        run_reference(args, c, cfg_path)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from oceansar_b200.radarsim.sar_raw_nompi import RawGenerator
+
+    world, rank, local = dist_info()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=120))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(gen, steps, warmup):
+        for _ in range(warmup):
+            gen.replay()
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            gen.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1) / steps)
+
+    # ---- main arm ---------------------------------------------------------------------
+    gen = RawGenerator(cfg_path, precision=args.precision, overrides=overrides(c), seed=1000 + rank)
+    if args.profile_pulses:
+        gen.run(range(args.profile_pulses))
+        torch.cuda.synchronize()
+        print("profiled %d pulses" % args.profile_pulses)
+        return
+    gen.capture()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = timed(gen, args.steps, args.warmup)
+    clk = clocks.stop()
+    value = echoes(c) * world / (ms * 1e-3)
+    launches = gen.kernel_launches_per_scene() * args.steps
+
+    # ---- per-kernel timing and roofline (dominant kernel) -----------------------------
+    npl = 64
+    surf_ms, pulse_ms, _, _ = gen.time_stages(range(64, 64 + npl))
+    nf = float(gen.surface.Nx * gen.surface.Ny)
+    fields_pulse = 5 + (3 if gen.scat_spec_enable else 0)
+    scat_b = (8 if args.precision == "f64" else 4) * 2 * gen.npol
+    pulse_bytes = nf * (4 * fields_pulse + scat_b + 8)          # fields + sqrt(RCS) + ind0
+    nfields = len(gen.surface._raw)
+    surf_bytes = nf * (8 + 4 + 4 * nfields)                      # coefs + omega + fields out
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        peak = json.load(open(peaks_path))["hbm_gbs"]
+        peak_src = "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
+    kern = {"surface_update": {"ms": surf_ms, "bytes": surf_bytes},
+            "pulse": {"ms": pulse_ms, "bytes": pulse_bytes}}
+    for k in kern.values():
+        k["GBps"] = k["bytes"] / (k["ms"] * 1e-3) / 1e9
+        k["frac"] = k["GBps"] / peak
+    dom = max(kern, key=lambda k: kern[k]["ms"])
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(args.precision, {}).get(dom)
+        except (ValueError, OSError):
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": kern[dom]["GBps"], "peak": peak, "unit": "GB/s",
+                "frac": kern[dom]["frac"], "traffic": traffic, "kernel": dom, "peak_source": peak_src,
+                "per_kernel": {k: {"ms": round(v["ms"], 5), "GBps": round(v["GBps"], 1),
+                                   "frac": round(v["frac"], 4), "alg_bytes": v["bytes"]}
+                               for k, v in kern.items()}}
+
+    # ---- end to end through the public API with host buffers ---------------------------
+    s = gen.surface
+    host_in = {"coefs": torch.from_numpy(s.wave_coefs).pin_memory(),
+               "omega": torch.from_numpy(s.omega).pin_memory()}
+    if gen.scat_bragg_enable:
+        host_in["ind0_m"] = torch.from_numpy(gen.rndscat_m.ind0.astype(np.int32)).pin_memory()
+        host_in["ind0_p"] = torch.from_numpy(gen.rndscat_p.ind0.astype(np.int32)).pin_memory()
+    dev_in = {"coefs": s._coefs_d, "omega": s._omega_d}
+    if gen.scat_bragg_enable:
+        dev_in["ind0_m"] = gen.rndscat_m.device()[1]
+        dev_in["ind0_p"] = gen.rndscat_p.device()[1]
+    host_out = torch.empty(gen.raw_d.shape, dtype=gen.raw_d.dtype).pin_memory()
+    h2d = sum(t.numel() * t.element_size() for t in host_in.values())
+    d2h = host_out.numel() * host_out.element_size()
+
+    def e2e_step():
+        for k, t in host_in.items():
+            dev_in[k].copy_(t, non_blocking=True)
+        gen.replay()
+        host_out.copy_(gen.raw_d, non_blocking=True)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    e2e = {"value": echoes(c) * world / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms}
+
+    # ---- FP64 drop-in form on the same workload (secondary figure) ---------------------
+    fp64 = None
+    if not args.no_fp64 and args.precision == "mixed":
+        del gen
+        torch.cuda.empty_cache()
+        g64 = RawGenerator(cfg_path, precision="f64", overrides=overrides(c), seed=1000 + rank)
+        g64.capture()
+        ms64 = timed(g64, 1, 1)
+        fp64 = {"value": echoes(c) * world / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64}
+        del g64
+        torch.cuda.empty_cache()
+
+    # ---- CPU baseline (oracle port) -------------------------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        pulses = 2 if args.small else 3
+        v, dt = cpu_baseline(c, cfg_path, pulses)
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": "%d pulses of the %dx%d scene (%.1f s), after one warm-up pulse; numpy FFT "
+                         "(single thread) + serial C accumulation" % (pulses, c["L"], c["L"], dt)}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f64",
+                "data": "synthetic",
+                "config": {"workload": c["name"], "grid": [c["L"], c["L"]], "pulses": c["pulses"],
+                           "channels": c["num_ch"], "range_bins": c["bins"], "precision": args.precision,
+                           "parallelism": "replicas" if world > 1 else "single-gpu",
+                           "l2": "inputs larger than L2 (~0.5 GB working set)",
+                           "graph": "whole scene replayed from one CUDA graph"},
+                "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
+                "cpu_baseline": cpu, "fp64": fp64}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -17,17 +17,28 @@
 
 namespace ocs {
 
+// Row stride (elements) of the pre-shifted weight table: S slots padded so that rows start
+// on 8 different 4-bank groups (a row is read with 16-byte vector loads by lanes whose
+// rows differ).
+template <typename T, int S> __host__ __device__ constexpr int wtab_stride() {
+    return sizeof(T) == 4 ? (S == 16 ? 20 : S) : (S == 12 ? 14 : (S == 16 ? 18 : S));
+}
+
+template <typename T, int S> __host__ __device__ constexpr int wtab_len(int taps, int ovs) {
+    return (S - taps + 1) * (ovs + 1) * wtab_stride<T, S>();
+}
+
 // Pre-shifted weight table: (S - taps + 1) offsets x (ovs + 1) LUT positions x S slots.
 template <typename T, int S>
 __device__ void build_wtab(T *wtab, const float *sinc, int taps, int ovs) {
-    const int noff = S - taps + 1;
-    const int total = noff * (ovs + 1) * S;
+    constexpr int W = wtab_stride<T, S>();
+    const int total = wtab_len<T, S>(taps, ovs);
     for (int i = threadIdx.x; i < total; i += blockDim.x) {
-        int s = i % S;
-        int lut = (i / S) % (ovs + 1);
-        int off = i / (S * (ovs + 1));
+        int s = i % W;
+        int lut = (i / W) % (ovs + 1);
+        int off = i / (W * (ovs + 1));
         int j = s - off;
-        wtab[i] = (j >= 0 && j < taps) ? (T)sinc[lut + j * ovs] : (T)0;
+        wtab[i] = (s < S && j >= 0 && j < taps) ? (T)sinc[lut + j * ovs] : (T)0;
     }
 }
 
@@ -136,7 +147,7 @@ struct BinWindow {
         lo = min(lo, off);
         hi = max(hi, off + taps - 1);
         using V = typename vec4_of<T>::type;
-        const V *w = reinterpret_cast<const V *>(wtab + (off * (ovs + 1) + lut) * S);
+        const V *w = reinterpret_cast<const V *>(wtab + (off * (ovs + 1) + lut) * wtab_stride<T, S>());
         constexpr int PER = sizeof(V) / sizeof(T);
 #pragma unroll
         for (int v = 0; v < S / PER; ++v) {

@@ -22,8 +22,8 @@ chan_profile_kernel(const double *__restrict__ srg, const cplx<T> *__restrict__ 
                     int nbins, long long out_row_stride, int chunk, int cta_nbw) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *wtab = reinterpret_cast<T *>(smem_raw);
-    const int wtab_len = (S - taps + 1) * (ovs + 1) * S;
-    T *acc = wtab + ((wtab_len + 3) & ~3);
+    const int wlen = wtab_len<T, S>(taps, ovs);
+    T *acc = wtab + ((wlen + 3) & ~3);
 
     // Row handling (profile_integrator_1d): facets of row r accumulate into out row r.
     // A CTA covers facets [f0, f0 + blockDim*chunk) of one row.
@@ -77,8 +77,8 @@ static int launch_chan_profile(const double *srg, const void *scene, long long n
                                T *out, int nbins, cudaStream_t stream) {
     if (taps < 1 || taps > S || ovs < 1 || npts < 0 || naz < 1 || nbins < 0) return OCS_ERR_ARG;
     if (npts == 0 || nbins == 0) return OCS_OK;
-    const int wtab_len = (S - taps + 1) * (ovs + 1) * S;
-    const size_t wtab_bytes = (size_t)((wtab_len + 3) & ~3) * sizeof(T);
+    const int wlen = wtab_len<T, S>(taps, ovs);
+    const size_t wtab_bytes = (size_t)((wlen + 3) & ~3) * sizeof(T);
     const size_t budget = 96 * 1024;
     if (wtab_bytes > budget / 2) return OCS_ERR_UNSUPPORTED;
     long long cap = (long long)((budget - wtab_bytes) / (2 * sizeof(T)));
@@ -93,7 +93,7 @@ static int launch_chan_profile(const double *srg, const void *scene, long long n
     if (grid > 0x7fffffffLL) return OCS_ERR_SIZE;
     size_t smem = wtab_bytes + (size_t)nbw * 2 * sizeof(T);
     auto kern = chan_profile_kernel<T, S>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (ensure_smem((const void *)kern, smem) != cudaSuccess)
         return OCS_ERR_CUDA;
     kern<<<(unsigned)grid, kProfThreads, smem, stream>>>(
         srg, reinterpret_cast<const cplx<T> *>(scene), naz * npts, npts, binsize, min_sr, sinc, taps,

@@ -3,6 +3,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "oceansar_b200.h"
 
 #define OCS_HD __host__ __device__ __forceinline__
@@ -70,6 +74,57 @@ OCS_D void bin_and_lut(double srg, double min_sr, double binsize, int ovs, int &
     }
     bin_d = (int)fl;
     lut = (int)rint(dmul((double)ovs, dsub(1.0, dsub(bin_f, fl))));
+}
+
+// Raise a kernel's dynamic shared-memory limit once per (kernel, device): later launches,
+// including those recorded into a CUDA graph, then issue no attribute call.
+inline cudaError_t ensure_smem(const void *kernel, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, size_t> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    auto key = std::make_pair(kernel, dev);
+    auto it = done.find(key);
+    if (it != done.end() && it->second >= bytes) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) done[key] = bytes;
+    return e;
+}
+
+// CTAs of `kernel` that fit on the whole device at once (cached per kernel, block size,
+// shared memory and device): the grid size of persistent kernels.
+inline int resident_ctas(const void *kernel, int threads, size_t smem) {
+    static std::mutex mu;
+    static std::map<std::pair<std::pair<const void *, int>, std::pair<int, size_t>>, int> done;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+    std::lock_guard<std::mutex> lock(mu);
+    auto key = std::make_pair(std::make_pair(kernel, dev), std::make_pair(threads, smem));
+    auto it = done.find(key);
+    if (it != done.end()) return it->second;
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess) return -1;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
+    int n = per_sm * sms;
+    done[key] = n;
+    return n;
+}
+
+// Mixed-precision form of bin_and_lut: the division becomes a multiplication by the
+// reciprocal bin size (a one-ulp difference in bin_f; the floor / round-half-even steps
+// are unchanged).
+OCS_D void bin_and_lut_fast(double srg, double min_sr, double inv_binsize, int ovs, int &bin_d, int &lut) {
+    double bin_f = (srg - min_sr) * inv_binsize;
+    double fl = floor(bin_f);
+    if (!(fabs(fl) < 1.0e9)) {
+        bin_d = -(1 << 30);
+        lut = 0;
+        return;
+    }
+    bin_d = (int)fl;
+    lut = (int)rint((double)ovs * (1.0 - (bin_f - fl)));
 }
 
 }  // namespace ocs

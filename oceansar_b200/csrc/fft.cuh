@@ -25,7 +25,13 @@ struct FftPlan {
 };
 
 OCS_HD int pad_idx(int i) { return i + (i >> 3); }
-OCS_HD int padded_len(int n) { return n + (n >> 3) + 1; }
+// Vector stride in shared memory: the padded length rounded up to 4 (mod 16) float2 slots,
+// so that the column tiles' transposed stores (4 vectors x 4 consecutive elements per
+// half-warp) fall on 16 different 8-byte banks.
+OCS_HD int padded_len(int n) {
+    int v = n + (n >> 3) + 1;
+    return v + ((4 - (v & 15)) & 15);
+}
 
 OCS_D float2 c_mul(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
 OCS_D float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
@@ -133,7 +139,7 @@ OCS_D void fft_stage_inplace(float2 *buf, int vstride, int nvec, int n, int ns, 
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 float2 a = x[pad_idx(j + r * nb)];
-                if (r > 0 && jm > 0) a = c_mul(a, __ldg(&tw[r * jm * tstep]));
+                if (r > 0 && jm > 0) a = c_mul(a, tw[r * jm * tstep]);
                 v[it][r] = a;
             }
             dft_inv<R>(v[it]);

@@ -162,11 +162,22 @@ OCS_D cplx<T> kodis_facet(const KodisParams &kp, double sr, double sin_inc, doub
     float J = __fsub_rn(__fmul_rn(diffxx, diffyy), __fmul_rn(diffxy, diffxy));
     if (J == 0.f) return {(T)0, (T)0};                  // J -> NaN: never stationary
     const float J_abs = fabsf(J);
-    const double inv_j = (double)(1.f / J_abs);
-    const double ty = (double)diffy - tan_inc * sin_az;
-    const double tx = (double)diffx - tan_inc * cos_az;
-    const double delta_x = inv_j * ((double)diffxy * ty - (double)diffyy * tx);
-    const double delta_y = inv_j * ((double)diffxy * tx - (double)diffxx * ty);
+    double delta_x, delta_y;
+    if (sizeof(T) == 8) {
+        const double inv_j = (double)(1.f / J_abs);
+        const double ty = (double)diffy - tan_inc * sin_az;
+        const double tx = (double)diffx - tan_inc * cos_az;
+        delta_x = inv_j * ((double)diffxy * ty - (double)diffyy * tx);
+        delta_y = inv_j * ((double)diffxy * tx - (double)diffxx * ty);
+    } else {
+        // mixed form: the stationary-point offsets in float32 (only the facet-window test
+        // and the small range offset depend on them)
+        const float inv_j = __frcp_rn(J_abs);
+        const float ty = diffy - (float)(tan_inc * sin_az);
+        const float tx = diffx - (float)(tan_inc * cos_az);
+        delta_x = (double)(inv_j * (diffxy * ty - diffyy * tx));
+        delta_y = (double)(inv_j * (diffxy * tx - diffxx * ty));
+    }
     const double hdx = kp.hdx, hdy = kp.hdy;
     if (!((-hdx < delta_x) && (delta_x < hdx) && (-hdy < delta_y) && (delta_y < hdy)))
         return {(T)0, (T)0};
@@ -187,7 +198,7 @@ OCS_D cplx<T> kodis_facet(const KodisParams &kp, double sr, double sin_inc, doub
         e = {(T)c, (T)s};
     } else {
         float s, c;
-        sincosf((float)reduce_2pi(ph), &s, &c);
+        __sincosf((float)reduce_2pi(ph), &s, &c);
         e = {(T)c, (T)s};
     }
     v = cmul(v, e);

@@ -27,7 +27,7 @@
 namespace ocs {
 
 constexpr int kPulseCols = 128;     // columns (threads) per CTA
-constexpr int kPulseRows = 64;      // rows per CTA strip
+constexpr int kPulseRows = 32;      // rows per tile
 constexpr int kMaxCh = 8;
 constexpr int kPulseNbw = 160;      // CTA shared bin window
 
@@ -37,7 +37,8 @@ struct PulseArgs {
     const float *dx_f, *dy_f, *dz_f, *diffx, *diffy, *diffxx, *diffyy, *diffxy, *hmtf;
     const float *y;                         // [ny] float32 azimuth coordinates
     const double *sr_col, *sin_inc, *cos_inc, *tan_inc, *inc, *c_b;   // [nx]
-    double inc_angle, sr0, gr0, k0, az_now, min_sr, binsize, t_step;
+    double inc_angle, sr0, gr0, k0, az_now, min_sr, binsize, inv_binsize, t_step;
+    int any_xti;
     int az_step;
     long long tind;                         // int(t_now * prf)
     double ltx_over_l, lrx_over_l;          // antenna length / wavelength
@@ -47,7 +48,8 @@ struct PulseArgs {
     RomeiserParams rom;
     void *scat;                             // [npol][2][ny][nx] sqrt(RCS) (T)
     const double *s_m, *s_p;                // complex128 random-scatterer series
-    long long n_m, n_p;
+    int n_m, n_p;
+    int tmod_m, tmod_p;                     // int(t_now * prf) mod n_m, n_p
     const int *ind0_m, *ind0_p;             // [ny][nx]
     const float *sinc;                      // [8*20 + 1]
     void *raw;                              // [npol*nch][az_steps][rg_samp] complex T
@@ -58,9 +60,39 @@ struct PulseArgs {
     int az_steps;
 };
 
+// Inputs of one facet, loaded one row ahead of use.
+template <typename T> struct FacetIn {
+    float dx, dy, dz, diffx, diffy, diffxx, diffyy, diffxy;
+    T scat[2][2];
+    int ind0_m, ind0_p;
+    template <typename A>
+    OCS_D void load(const A &a, long long idx, long long npix, const T *scat_buf, bool load_scat) {
+        dx = a.dx_f[idx];
+        dy = a.dy_f[idx];
+        dz = a.dz_f[idx];
+        if (a.diffx) { diffx = a.diffx[idx]; diffy = a.diffy[idx]; }
+        if (a.do_kodis) { diffxx = a.diffxx[idx]; diffyy = a.diffyy[idx]; diffxy = a.diffxy[idx]; }
+        if (a.do_bragg) { ind0_m = a.ind0_m[idx]; ind0_p = a.ind0_p[idx]; }
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+            if (load_scat && p < a.npol) {
+                scat[p][0] = scat_buf[(2 * p) * npix + idx];
+                scat[p][1] = scat_buf[(2 * p + 1) * npix + idx];
+            } else {
+                scat[p][0] = (T)0;
+                scat[p][1] = (T)0;
+            }
+        }
+    }
+};
+
 template <typename T> OCS_D cplx<T> cexp_phase(double ph);
 template <> OCS_D cplx<double> cexp_phase<double>(double ph) { return cexpi(ph); }
-template <> OCS_D cplx<float> cexp_phase<float>(double ph) { return cexpi((float)reduce_2pi(ph)); }
+template <> OCS_D cplx<float> cexp_phase<float>(double ph) {
+    float s, c;
+    __sincosf((float)reduce_2pi(ph), &s, &c);
+    return {c, s};
+}
 
 // Block-wide sum of a double; thread 0 adds it to *dst.
 OCS_D void block_atomic_sum(double v, double *dst, double *sred) {
@@ -77,13 +109,12 @@ OCS_D void block_atomic_sum(double v, double *dst, double *sred) {
 }
 
 template <typename T, int NOUT, int S>
-__global__ void __launch_bounds__(kPulseCols)
+__global__ void __launch_bounds__(kPulseCols, sizeof(T) == 4 ? 4 : 2)
 pulse_kernel(const __grid_constant__ PulseArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
-    constexpr int noff = S - kSincTaps + 1;
-    constexpr int wtab_len = noff * (kSincOvs + 1) * S;
+    constexpr int wlen = wtab_len<T, S>(kSincTaps, kSincOvs);
     T *wtab = reinterpret_cast<T *>(smem);
-    T *bins = wtab + wtab_len;                                        // [NOUT][nbw][2]
+    T *bins = wtab + wlen;                                            // [NOUT][nbw][2]
     double *r_az = reinterpret_cast<double *>(bins + NOUT * kPulseNbw * 2);
     double *r_sinaz = r_az + kPulseRows;
     double *r_azp = r_sinaz + kPulseRows;
@@ -92,11 +123,16 @@ pulse_kernel(const __grid_constant__ PulseArgs a) {
     cplx<T> *r_fac = reinterpret_cast<cplx<T> *>(r_sazp + kPulseRows);   // [rows][nch]
     double *sred = reinterpret_cast<double *>(r_fac + kPulseRows * a.nch);
 
-    const int x = blockIdx.x * kPulseCols + threadIdx.x;
-    const int y0 = blockIdx.y * kPulseRows;
-    const int nrows = min(kPulseRows, a.ny - y0);
-
     build_wtab<T, S>(wtab, a.sinc, kSincTaps, kSincOvs);
+    const int tiles_x = (a.nx + kPulseCols - 1) / kPulseCols;
+    const int tiles = tiles_x * ((a.ny + kPulseRows - 1) / kPulseRows);
+    double spec_sum = 0.0, bragg_sum[2] = {0.0, 0.0};
+    // persistent CTAs: each walks tiles of kPulseCols columns x kPulseRows rows
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const int x = (tile % tiles_x) * kPulseCols + threadIdx.x;
+    const int y0 = (tile / tiles_x) * kPulseRows;
+    const int nrows = min(kPulseRows, a.ny - y0);
+    __syncthreads();                    // previous tile's bins and row tables are consumed
     // per-row quantities (sar_raw_nompi.py:353-363, 485-493)
     for (int i = threadIdx.x; i < nrows; i += blockDim.x) {
         const double az = dsub((double)a.y[y0 + i], a.az_now);
@@ -123,7 +159,7 @@ pulse_kernel(const __grid_constant__ PulseArgs a) {
     cb.out_stride = a.raw_out_stride;
     {
         // window base: bin of this CTA's first column at its first row, undisplaced
-        const int xc = min(blockIdx.x * kPulseCols, a.nx - 1);
+        const int xc = min((tile % tiles_x) * kPulseCols, a.nx - 1);
         const double az = (double)a.y[y0] - a.az_now;
         const double srg = a.sr_col[xc] + az * 0.5 * (az / a.sr0);
         cb.cta_base = (int)floor((srg - a.min_sr) / a.binsize) - 24;
@@ -133,35 +169,38 @@ pulse_kernel(const __grid_constant__ PulseArgs a) {
 
     BinWindow<T, S, NOUT> win;
     win.reset();
-    double spec_sum = 0.0, bragg_sum[2] = {0.0, 0.0};
     if (x < a.nx) {
         const double sr_c = a.sr_col[x], sin_i = a.sin_inc[x], cos_i = a.cos_inc[x];
         const double inc_c = a.inc[x];
         const double dinc0 = inc_c - a.inc_angle;
         const double tan_i = a.do_kodis ? a.tan_inc[x] : 0.0;
         const double cap = a.do_bragg ? ((2.0 * a.k0) * a.t_step) * a.c_b[x] * (double)(a.az_step + 1) : 0.0;
+        const float cap_r = (float)reduce_2pi(cap);
         const double two_k0 = 2.0 * a.k0;
         const long long npix = (long long)a.nx * a.ny;
         T *scat = reinterpret_cast<T *>(a.scat);
+        const bool load_scat = a.do_bragg && !a.refresh;
+        // software pipeline: the inputs of row i+1 are loaded while row i is processed
+        FacetIn<T> cur, nxt;
+        cur.load(a, (long long)y0 * a.nx + x, npix, scat, load_scat);
         for (int i = 0; i < nrows; ++i) {
-            const int yy = y0 + i;
-            const long long idx = (long long)yy * a.nx + x;
-            const float fdx = a.dx_f[idx], fdy = a.dy_f[idx], fdz = a.dz_f[idx];
+            const long long idx = (long long)(y0 + i) * a.nx + x;
+            if (i + 1 < nrows) nxt.load(a, idx + a.nx, npix, scat, load_scat);
             const double az = r_az[i], sin_az = r_sinaz[i];
             // slant range: sr - cos_inc*Dz + az/2*sin_az + Dx*sin_inc + Dy*sin_az, float64,
             // left to right, no fused multiply-adds (bit-identical with numpy)
-            double srs = dsub(sr_c, dmul(cos_i, (double)fdz));
+            double srs = dsub(sr_c, dmul(cos_i, (double)cur.dz));
             srs = dadd(srs, dmul(az * 0.5, sin_az));
-            srs = dadd(srs, dmul((double)fdx, sin_i));
-            srs = dadd(srs, dmul((double)fdy, sin_az));
+            srs = dadd(srs, dmul((double)cur.dx, sin_i));
+            srs = dadd(srs, dmul((double)cur.dy, sin_az));
             int bin_d, lut;
-            bin_and_lut(srs, a.min_sr, a.binsize, kSincOvs, bin_d, lut);
+            if (sizeof(T) == 8) bin_and_lut(srs, a.min_sr, a.binsize, kSincOvs, bin_d, lut);
+            else bin_and_lut_fast(srs, a.min_sr, a.inv_binsize, kSincOvs, bin_d, lut);
 
             cplx<T> scene[2] = {{(T)0, (T)0}, {(T)0, (T)0}};      // per polarisation
             if (a.do_kodis) {
                 const cplx<T> e = kodis_facet<T>(a.kodis, srs, sin_i, cos_i, tan_i, r_cazp[i], r_sazp[i],
-                                                 a.diffx[idx], a.diffy[idx], a.diffxx[idx], a.diffyy[idx],
-                                                 a.diffxy[idx]);
+                                                 cur.diffx, cur.diffy, cur.diffxx, cur.diffyy, cur.diffxy);
                 const T s4 = (T)3.5449077018110318;                 // sqrt(4 pi)
                 const cplx<T> es = {e.re * s4, e.im * s4};
                 scene[0] = es;
@@ -173,57 +212,70 @@ pulse_kernel(const __grid_constant__ PulseArgs a) {
                 if (a.refresh) {
                     T hh[2], vv[2];
                     romeiser_facet<T>(a.rom, (T)inc_c, (T)r_azp[i], (T)r_cazp[i], (T)r_sazp[i],
-                                      (T)a.diffx[idx], (T)a.diffy[idx], hh, vv);
+                                      (T)cur.diffx, (T)cur.diffy, hh, vv);
                     if (a.use_hmtf) {
                         float hm = a.hmtf[idx];
                         hm = hm < -1.f ? -1.f : hm;
                         const T f = (T)(1.f + hm);
                         hh[0] *= f; hh[1] *= f; vv[0] *= f; vv[1] *= f;
                     }
-                    for (int p = 0; p < a.npol; ++p) {
-                        const T *r = (a.rom.pol == POL_VV || (a.rom.pol == POL_DP && p == 1)) ? vv : hh;
-                        bragg_sum[p] += (double)r[0] + (double)r[1];
-                        sc[p][0] = tsqrt(r[0]);
-                        sc[p][1] = tsqrt(r[1]);
-                        scat[(2 * p) * npix + idx] = sc[p][0];
-                        scat[(2 * p + 1) * npix + idx] = sc[p][1];
+#pragma unroll
+                    for (int p = 0; p < 2; ++p) {
+                        if (p < a.npol) {
+                            const bool use_vv = a.rom.pol == POL_VV || (a.rom.pol == POL_DP && p == 1);
+                            const T r0 = use_vv ? vv[0] : hh[0], r1 = use_vv ? vv[1] : hh[1];
+                            bragg_sum[p] += (double)r0 + (double)r1;
+                            sc[p][0] = tsqrt(r0);
+                            sc[p][1] = tsqrt(r1);
+                            scat[(2 * p) * npix + idx] = sc[p][0];
+                            scat[(2 * p + 1) * npix + idx] = sc[p][1];
+                        }
                     }
                 } else {
-                    for (int p = 0; p < a.npol; ++p) {
-                        sc[p][0] = scat[(2 * p) * npix + idx];
-                        sc[p][1] = scat[(2 * p + 1) * npix + idx];
-                    }
+#pragma unroll
+                    for (int p = 0; p < 2; ++p) { sc[p][0] = cur.scat[p][0]; sc[p][1] = cur.scat[p][1]; }
                 }
                 // Bragg phases: -2 k0 r -/+ 2 k0 t_step c_b (az_step + 1)
-                const double surf = (-two_k0) * srs;
-                const cplx<T> e0 = cexp_phase<T>(surf - cap);
-                const cplx<T> e1 = cexp_phase<T>(surf + cap);
-                const int i0 = (int)(((long long)a.ind0_m[idx] + a.tind) % a.n_m);
-                const int i1 = (int)(((long long)a.ind0_p[idx] + a.tind) % a.n_p);
-                const cplx<T> sm = {(T)a.s_m[2 * i0], (T)a.s_m[2 * i0 + 1]};
-                const cplx<T> sp = {(T)a.s_p[2 * i1], (T)a.s_p[2 * i1 + 1]};
-                for (int p = 0; p < a.npol; ++p) {
-                    const cplx<T> l0 = cmul(cplx<T>{sc[p][0] * e0.re, sc[p][0] * e0.im}, sm);
-                    const cplx<T> l1 = cmul(cplx<T>{sc[p][1] * e1.re, sc[p][1] * e1.im}, sp);
-                    scene[p] = cadd(scene[p], cadd(l0, l1));
+                cplx<T> e0, e1;
+                if (sizeof(T) == 8) {
+                    const double surf = (-two_k0) * srs;
+                    e0 = cexp_phase<T>(surf - cap);
+                    e1 = cexp_phase<T>(surf + cap);
+                } else {
+                    const float rs = (float)reduce_2pi((-two_k0) * srs);
+                    float s0, c0, s1, c1;
+                    __sincosf(rs - cap_r, &s0, &c0);
+                    __sincosf(rs + cap_r, &s1, &c1);
+                    e0 = {(T)c0, (T)s0};
+                    e1 = {(T)c1, (T)s1};
+                }
+                int i0 = cur.ind0_m + a.tmod_m;
+                i0 = i0 >= a.n_m ? i0 - a.n_m : i0;
+                int i1 = cur.ind0_p + a.tmod_p;
+                i1 = i1 >= a.n_p ? i1 - a.n_p : i1;
+                const double2 smd = reinterpret_cast<const double2 *>(a.s_m)[i0];
+                const double2 spd = reinterpret_cast<const double2 *>(a.s_p)[i1];
+                const cplx<T> sm = {(T)smd.x, (T)smd.y};
+                const cplx<T> sp = {(T)spd.x, (T)spd.y};
+#pragma unroll
+                for (int p = 0; p < 2; ++p) {
+                    if (p < a.npol) {
+                        const cplx<T> l0 = cmul(cplx<T>{sc[p][0] * e0.re, sc[p][0] * e0.im}, sm);
+                        const cplx<T> l1 = cmul(cplx<T>{sc[p][1] * e1.re, sc[p][1] * e1.im}, sp);
+                        scene[p] = cadd(scene[p], cadd(l0, l1));
+                    }
                 }
             }
             // channels of this pass: antenna pattern x ATI phase (per row) x XTI phase
             cplx<T> coef[NOUT];
             double wave_dinc = 0.0;
-            bool need_dinc = false;
-#pragma unroll
-            for (int k = 0; k < NOUT; ++k) {
-                const int o = a.out0 + k;
-                if (k < a.nout && a.b_xti[o % a.nch] != 0.0) need_dinc = true;
-            }
-            if (need_dinc) wave_dinc = ((double)fdz * sin_i + (double)fdx * sin_i) / a.sr0;
+            if (a.any_xti) wave_dinc = ((double)cur.dz * sin_i + (double)cur.dx * sin_i) / a.sr0;
 #pragma unroll
             for (int k = 0; k < NOUT; ++k) {
                 if (k < a.nout) {
                     const int o = a.out0 + k;
                     const int p = o / a.nch, c = o - p * a.nch;
-                    cplx<T> v = cmul(scene[p], r_fac[i * a.nch + c]);
+                    cplx<T> v = cmul(p == 0 ? scene[0] : scene[1], r_fac[i * a.nch + c]);
                     if (a.b_xti[c] != 0.0) {
                         const double ph = (-a.k0 * a.b_xti[c]) * (dinc0 + wave_dinc);
                         v = cmul(v, cexp_phase<T>(ph));
@@ -235,11 +287,13 @@ pulse_kernel(const __grid_constant__ PulseArgs a) {
             }
             if (bin_d > -(1 << 29))
                 win.add(bin_d - kSincTaps / 2, lut, coef, wtab, a.sinc, kSincTaps, kSincOvs, cb);
+            cur = nxt;
         }
     }
     win.flush(cb);
     __syncthreads();
     cb.flush_to_global();
+    }
     // NRCS bookkeeping (only the first output group accumulates it)
     if (a.out0 == 0) {
         if (a.do_kodis) block_atomic_sum(spec_sum, &a.nrcs_spec[a.az_step], sred);
@@ -251,16 +305,18 @@ pulse_kernel(const __grid_constant__ PulseArgs a) {
 
 template <typename T, int NOUT, int S>
 static int launch_pulse(const PulseArgs &a, cudaStream_t st) {
-    constexpr int noff = S - kSincTaps + 1;
-    constexpr int wtab_len = noff * (kSincOvs + 1) * S;
-    size_t smem = (size_t)wtab_len * sizeof(T) + (size_t)NOUT * kPulseNbw * 2 * sizeof(T) +
+    constexpr int wlen = wtab_len<T, S>(kSincTaps, kSincOvs);
+    size_t smem = (size_t)wlen * sizeof(T) + (size_t)NOUT * kPulseNbw * 2 * sizeof(T) +
                   5 * kPulseRows * sizeof(double) + (size_t)kPulseRows * a.nch * sizeof(cplx<T>) +
                   32 * sizeof(double);
     auto k = pulse_kernel<T, NOUT, S>;
-    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (ensure_smem((const void *)k, smem) != cudaSuccess)
         return OCS_ERR_CUDA;
-    dim3 grid((a.nx + kPulseCols - 1) / kPulseCols, (a.ny + kPulseRows - 1) / kPulseRows);
-    k<<<grid, kPulseCols, smem, st>>>(a);
+    const long long tiles = (long long)((a.nx + kPulseCols - 1) / kPulseCols) * ((a.ny + kPulseRows - 1) / kPulseRows);
+    const int resident = resident_ctas((const void *)k, kPulseCols, smem);
+    if (resident <= 0) return OCS_ERR_CUDA;
+    const long long grid = tiles < resident ? tiles : resident;
+    k<<<(unsigned)grid, kPulseCols, smem, st>>>(a);
     return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
 }
 
@@ -293,11 +349,16 @@ static int fill_pulse_args(const ocs_pulse_desc *d, PulseArgs &a) {
     a.sr_col = d->sr_col_d; a.sin_inc = d->sin_inc_d; a.cos_inc = d->cos_inc_d; a.tan_inc = d->tan_inc_d;
     a.inc = d->inc_d; a.c_b = d->c_b_d;
     a.inc_angle = d->inc_angle; a.sr0 = d->sr0; a.gr0 = d->gr0; a.k0 = d->k0; a.az_now = d->az_now;
-    a.min_sr = d->min_sr; a.binsize = d->binsize; a.t_step = d->t_step; a.az_step = d->az_step;
+    a.min_sr = d->min_sr; a.binsize = d->binsize; a.inv_binsize = 1.0 / d->binsize;
+    a.t_step = d->t_step; a.az_step = d->az_step;
     a.tind = d->tind;
     a.ltx_over_l = d->ant_l_tx * d->f0 / 2.99792458e8;
     a.lrx_over_l = d->ant_l_rx * d->f0 / 2.99792458e8;
-    for (int c = 0; c < d->nch; ++c) { a.b_ati[c] = d->b_ati[c]; a.b_xti[c] = d->b_xti[c]; }
+    for (int c = 0; c < d->nch; ++c) {
+        a.b_ati[c] = d->b_ati[c];
+        a.b_xti[c] = d->b_xti[c];
+        if (d->b_xti[c] != 0.0) a.any_xti = 1;
+    }
     a.do_kodis = d->do_kodis; a.do_bragg = d->do_bragg; a.refresh = d->refresh; a.use_hmtf = d->use_hmtf;
     a.kodis.k0 = d->k0;
     a.kodis.R_re = d->kodis_R_re; a.kodis.R_im = d->kodis_R_im;
@@ -311,7 +372,12 @@ static int fill_pulse_args(const ocs_pulse_desc *d, PulseArgs &a) {
     r.eps_re = 73.0; r.eps_im = 18.0;
     r.seps_re = d->sqrt_eps_re; r.seps_im = d->sqrt_eps_im;
     r.eps2_re = 73.0 * 73.0 - 18.0 * 18.0; r.eps2_im = 2.0 * 73.0 * 18.0;
-    a.scat = d->scat_d; a.s_m = d->s_m_d; a.s_p = d->s_p_d; a.n_m = d->n_m; a.n_p = d->n_p;
+    a.scat = d->scat_d; a.s_m = d->s_m_d; a.s_p = d->s_p_d;
+    if (d->do_bragg) {
+        if (d->n_m > (1LL << 30) || d->n_p > (1LL << 30) || d->tind < 0) return OCS_ERR_SIZE;
+        a.n_m = (int)d->n_m; a.n_p = (int)d->n_p;
+        a.tmod_m = (int)(d->tind % d->n_m); a.tmod_p = (int)(d->tind % d->n_p);
+    }
     a.ind0_m = d->ind0_m_d; a.ind0_p = d->ind0_p_d;
     a.sinc = d->sinc_d;
     a.raw = d->raw_d;

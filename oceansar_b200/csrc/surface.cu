@@ -24,6 +24,10 @@ namespace ocs {
 
 constexpr int kMaxPacked = 12;          // transforms per call (24 real fields)
 
+struct MultDesc {
+    signed char imag, sign, a, b, c, d, hmtf, pad;
+};
+
 struct SurfaceArgs {
     int nx, ny;
     const float2 *coefs;
@@ -35,6 +39,7 @@ struct SurfaceArgs {
     float inv_n;
     int npair;
     int code[2 * kMaxPacked];
+    MultDesc mult[2 * kMaxPacked];
     float *dst[2 * kMaxPacked];
     float add[2 * kMaxPacked];
     float2 swm[2 * kMaxPacked];
@@ -44,43 +49,51 @@ struct SurfaceArgs {
     FftPlan px, py;
 };
 
-// Spectral multiplier of field `code` at wavenumber (kx, ky) (ocean.py:431-526).
-OCS_D float2 field_mult(int code, float kxv, float kyv, float kmin_half, float om) {
-    float k = __fsqrt_rn(fadd(fmul(kxv, kxv), fmul(kyv, kyv)));
-    bool good = k > kmin_half;
-    float kxn = good ? __fdiv_rn(kxv, k) : 0.f;
-    float kyn = good ? __fdiv_rn(kyv, k) : 0.f;
-    float kinv = good ? __frcp_rn(k) : 0.f;
+// Spectral multiplier M of every field (ocean.py:431-526): Re(ifft2(M c)) is the field.
+// Except for the hydrodynamic MTF, M = sign * kx^a * ky^b * kinv^c * omega^d, purely real
+// or purely imaginary; MultDesc holds that recipe so the device evaluates it with uniform
+// loops (kinv = 1/|k| where |k| > min(kx_res, ky_res)/2, else 0; ocean.py:141-148).
+static MultDesc mult_desc(int code) {
+    //                                     imag sign a  b  c  d  hmtf
     switch (code) {
-        case OCS_FIELD_DZ: return make_float2(1.f, 0.f);
-        case OCS_FIELD_DX: return make_float2(0.f, kxn);                 // -Im(ifft2(kxn c))
-        case OCS_FIELD_DY: return make_float2(0.f, kyn);
-        case OCS_FIELD_DIFFX: return make_float2(0.f, kxv);              // Re(ifft2(i kx c))
-        case OCS_FIELD_DIFFY: return make_float2(0.f, kyv);
-        case OCS_FIELD_DIFFXX: return make_float2(-kxv * kxv, 0.f);
-        case OCS_FIELD_DIFFYY: return make_float2(-kyv * kyv, 0.f);
-        case OCS_FIELD_DIFFXY: return make_float2(-kxv * kyv, 0.f);
-        case OCS_FIELD_VX: return make_float2(kxn * om, 0.f);            // -Im(ifft2(kxn (-i w) c))
-        case OCS_FIELD_VY: return make_float2(kyn * om, 0.f);
-        case OCS_FIELD_VZ: return make_float2(0.f, -om);
-        case OCS_FIELD_AX: return make_float2(0.f, -kxv * kinv * om * om);
-        case OCS_FIELD_AY: return make_float2(0.f, -kyv * kinv * om * om);
-        case OCS_FIELD_AZ: return make_float2(-om * om, 0.f);
-        case OCS_FIELD_HMTF: {
-            // M_h = i k w (w + i mu) / (w^2 + mu^2) * (dlnS/dlnk - Vg/c), zero for k > 2 pi/20
-            const float kmax = 0.3141592653589793f, mu = 0.0025f, fac = -3.5f;
-            if (k > kmax) return make_float2(0.f, 0.f);
-            float den = om * om + mu * mu;
-            float2 num = make_float2(-k * om * mu, k * om * om);
-            return make_float2(num.x / den * fac, num.y / den * fac);
-        }
-        case OCS_FIELD_AUX_XX: return make_float2(-kxv * kxv * kinv, 0.f);
-        case OCS_FIELD_AUX_YY: return make_float2(-kyv * kyv * kinv, 0.f);
-        case OCS_FIELD_AUX_XXX: return make_float2(0.f, -kxv * kxv * kxv * kinv);
-        case OCS_FIELD_AUX_YYY: return make_float2(0.f, -kyv * kyv * kyv * kinv);
-        case OCS_FIELD_AUX_XXY: return make_float2(0.f, -kxv * kxv * kyv * kinv);
-        default: return make_float2(0.f, 0.f);
+        case OCS_FIELD_DZ: return {0, 1, 0, 0, 0, 0, 0, 0};
+        case OCS_FIELD_DX: return {1, 1, 1, 0, 1, 0, 0, 0};       // -Im(ifft2(kxn c))
+        case OCS_FIELD_DY: return {1, 1, 0, 1, 1, 0, 0, 0};
+        case OCS_FIELD_DIFFX: return {1, 1, 1, 0, 0, 0, 0, 0};    // Re(ifft2(i kx c))
+        case OCS_FIELD_DIFFY: return {1, 1, 0, 1, 0, 0, 0, 0};
+        case OCS_FIELD_DIFFXX: return {0, -1, 2, 0, 0, 0, 0, 0};
+        case OCS_FIELD_DIFFYY: return {0, -1, 0, 2, 0, 0, 0, 0};
+        case OCS_FIELD_DIFFXY: return {0, -1, 1, 1, 0, 0, 0, 0};
+        case OCS_FIELD_VX: return {0, 1, 1, 0, 1, 1, 0, 0};       // -Im(ifft2(kxn (-i w) c))
+        case OCS_FIELD_VY: return {0, 1, 0, 1, 1, 1, 0, 0};
+        case OCS_FIELD_VZ: return {1, -1, 0, 0, 0, 1, 0, 0};
+        case OCS_FIELD_AX: return {1, -1, 1, 0, 1, 2, 0, 0};
+        case OCS_FIELD_AY: return {1, -1, 0, 1, 1, 2, 0, 0};
+        case OCS_FIELD_AZ: return {0, -1, 0, 0, 0, 2, 0, 0};
+        case OCS_FIELD_HMTF: return {0, 1, 0, 0, 0, 0, 1, 0};
+        case OCS_FIELD_AUX_XX: return {0, -1, 2, 0, 1, 0, 0, 0};
+        case OCS_FIELD_AUX_YY: return {0, -1, 0, 2, 1, 0, 0, 0};
+        case OCS_FIELD_AUX_XXX: return {1, -1, 3, 0, 1, 0, 0, 0};
+        case OCS_FIELD_AUX_YYY: return {1, -1, 0, 3, 1, 0, 0, 0};
+        case OCS_FIELD_AUX_XXY: return {1, -1, 2, 1, 1, 0, 0, 0};
+        default: return {0, 0, 0, 0, 0, 0, 0, 0};
     }
+}
+
+OCS_D float2 field_mult(const MultDesc &m, float kxv, float kyv, float k, float kinv, float om) {
+    if (m.hmtf) {
+        // M_h = i k w (w + i mu) / (w^2 + mu^2) * (dlnS/dlnk - Vg/c), zero for k > 2 pi/20
+        const float kmax = 0.3141592653589793f, mu = 0.0025f, fac = -3.5f;
+        if (k > kmax) return make_float2(0.f, 0.f);
+        const float den = om * om + mu * mu;
+        return make_float2(-k * om * mu / den * fac, k * om * om / den * fac);
+    }
+    float v = (float)m.sign;
+    for (int i = 0; i < m.a; ++i) v *= kxv;
+    for (int i = 0; i < m.b; ++i) v *= kyv;
+    if (m.c) v *= kinv;
+    for (int i = 0; i < m.d; ++i) v *= om;
+    return m.imag ? make_float2(0.f, v) : make_float2(v, 0.f);
 }
 
 // c(t) = c * exp(-i fl(omega t)) in complex64 (ocean.py:424-427).
@@ -95,7 +108,7 @@ OCS_D float2 phased(const SurfaceArgs &a, int y, int x) {
 
 // Threads per CTA of the two passes for a power-of-two length N (0 = any length).
 template <int N> __host__ __device__ constexpr int rows_threads() {
-    return N == 0 ? 256 : (N / 8 < 64 ? 64 : (N / 8 > 512 ? 512 : N / 8));
+    return N == 0 ? 256 : (N / 4 < 64 ? 64 : (N / 4 > 1024 ? 1024 : N / 4));
 }
 template <int N, int TILE> __host__ __device__ constexpr int cols_threads() {
     return N == 0 ? 256 : (N * TILE / 16 < 64 ? 64 : (N * TILE / 16 > 1024 ? 1024 : N * TILE / 16));
@@ -105,7 +118,7 @@ template <int N, int TILE> __host__ __device__ constexpr int cols_threads() {
 // FFT rows (and, for non-power-of-two lengths, two more for the ping-pong).  Mirror pairs:
 // (r,x) <-> (mr,mx) and (r,mx) <-> (mr,x).
 template <int N>
-__global__ void __launch_bounds__(rows_threads<N>(), 1)
+__global__ void __launch_bounds__(rows_threads<N>(), rows_threads<N>() <= 512 ? 2 : 1)
 surface_rows_kernel(const __grid_constant__ SurfaceArgs a) {
     extern __shared__ __align__(16) float2 sbuf[];
     const int nx = (N > 0) ? N : a.nx;
@@ -115,6 +128,9 @@ surface_rows_kernel(const __grid_constant__ SurfaceArgs a) {
     const int vstride = padded_len(nx);
     float2 *cA = sbuf, *cB = sbuf + nx;
     float2 *rowA = sbuf + 2 * nx, *rowB = rowA + vstride;
+    float2 *stw = rowB + vstride;                 // power-of-two lengths: twiddles in smem
+    if (N > 0)
+        for (int i = threadIdx.x; i < nx; i += blockDim.x) stw[i] = a.px.tw[i];
     const float kyr = a.ky[r], kymr = a.ky[mr];
     const float *omA = a.omega + (size_t)r * nx, *omB = a.omega + (size_t)mr * nx;
 
@@ -126,39 +142,42 @@ surface_rows_kernel(const __grid_constant__ SurfaceArgs a) {
 
     const int nq = nx / 2 + 1;
     for (int p = 0; p < a.npair; ++p) {
-        const int ca = a.code[2 * p], cb = a.code[2 * p + 1];
+        const MultDesc ca = a.mult[2 * p], cb = a.mult[2 * p + 1];
+        const bool has_b = a.code[2 * p + 1] >= 0;
         for (int x = threadIdx.x; x < nq; x += blockDim.x) {
             const int mx = (nx - x) % nx;
             const float kxx = a.kx[x], kxm = a.kx[mx];
-            const float kxs[4] = {kxx, kxm, kxx, kxm};
-            const float kys[4] = {kyr, kyr, kymr, kymr};
-            const float2 cq[4] = {cA[x], cA[mx], cB[x], cB[mx]};
-            const float oq[4] = {omA[x], omA[mx], omB[x], omB[mx]};
-            float2 XA[4], XB[4];
+            // mirror pairs: (r, x) <-> (mr, mx) and (r, mx) <-> (mr, x)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                XA[j] = c_mul(field_mult(ca, kxs[j], kys[j], a.kmin_half, oq[j]), cq[j]);
-                XB[j] = (cb >= 0) ? c_mul(field_mult(cb, kxs[j], kys[j], a.kmin_half, oq[j]), cq[j])
-                                  : make_float2(0.f, 0.f);
+            for (int pr = 0; pr < 2; ++pr) {
+                const int xa = pr == 0 ? x : mx, xb = pr == 0 ? mx : x;   // columns of the pair
+                const float kxa = pr == 0 ? kxx : kxm, kxb = pr == 0 ? kxm : kxx;
+                const float2 c1 = cA[xa], c2 = cB[xb];
+                const float o1 = omA[xa], o2 = omB[xb];
+                const float k1 = __fsqrt_rn(fadd(fmul(kxa, kxa), fmul(kyr, kyr)));
+                const float k2 = __fsqrt_rn(fadd(fmul(kxb, kxb), fmul(kymr, kymr)));
+                const float ki1 = k1 > a.kmin_half ? __frcp_rn(k1) : 0.f;
+                const float ki2 = k2 > a.kmin_half ? __frcp_rn(k2) : 0.f;
+                const float2 xa1 = c_mul(field_mult(ca, kxa, kyr, k1, ki1, o1), c1);
+                const float2 xa2 = c_mul(field_mult(ca, kxb, kymr, k2, ki2, o2), c2);
+                float2 xb1 = make_float2(0.f, 0.f), xb2 = make_float2(0.f, 0.f);
+                if (has_b) {
+                    xb1 = c_mul(field_mult(cb, kxa, kyr, k1, ki1, o1), c1);
+                    xb2 = c_mul(field_mult(cb, kxb, kymr, k2, ki2, o2), c2);
+                }
+                // Z(p) = (XA(p) + conj XA(-p)) / 2 + i (XB(p) + conj XB(-p)) / 2
+                const float2 z1 = make_float2(0.5f * (xa1.x + xa2.x) - 0.5f * (xb1.y - xb2.y),
+                                              0.5f * (xa1.y - xa2.y) + 0.5f * (xb1.x + xb2.x));
+                const float2 z2 = make_float2(0.5f * (xa2.x + xa1.x) - 0.5f * (xb2.y - xb1.y),
+                                              0.5f * (xa2.y - xa1.y) + 0.5f * (xb2.x + xb1.x));
+                rowA[pad_idx(xa)] = z1;
+                rowB[pad_idx(xb)] = z2;
             }
-            // Z(j) = (XA[j] + conj XA[mir]) / 2 + i (XB[j] + conj XB[mir]) / 2
-            float2 Z[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int m = 3 - j;
-                float2 ha = make_float2(0.5f * (XA[j].x + XA[m].x), 0.5f * (XA[j].y - XA[m].y));
-                float2 hb = make_float2(0.5f * (XB[j].x + XB[m].x), 0.5f * (XB[j].y - XB[m].y));
-                Z[j] = make_float2(ha.x - hb.y, ha.y + hb.x);
-            }
-            rowA[pad_idx(x)] = Z[0];
-            rowA[pad_idx(mx)] = Z[1];
-            rowB[pad_idx(x)] = Z[2];
-            rowB[pad_idx(mx)] = Z[3];
         }
         __syncthreads();
         const float2 *res = rowA;
         if constexpr (N > 0) {
-            ifft_pow2<N, 2, rows_threads<N>()>(rowA, vstride, a.px.tw);
+            ifft_pow2<N, 2, rows_threads<N>()>(rowA, vstride, stw);
         } else {
             res = ifft_generic(rowA, rowB + vstride, vstride, 2, a.px);
         }
@@ -174,7 +193,7 @@ surface_rows_kernel(const __grid_constant__ SurfaceArgs a) {
 
 // Pass 2.  One CTA per (transform p, tile of TILE columns).
 template <int N, int TILE>
-__global__ void __launch_bounds__(cols_threads<N, TILE>(), 1)
+__global__ void __launch_bounds__(cols_threads<N, TILE>(), cols_threads<N, TILE>() <= 512 ? 2 : 1)
 surface_cols_kernel(const __grid_constant__ SurfaceArgs a) {
     extern __shared__ __align__(16) float2 sbuf[];
     const int nx = a.nx;
@@ -183,6 +202,9 @@ surface_cols_kernel(const __grid_constant__ SurfaceArgs a) {
     const int x0 = blockIdx.x * TILE;
     const int vstride = padded_len(ny);
     const float2 *src = a.scratch + (size_t)p * ny * nx;
+    float2 *stw = sbuf + TILE * vstride;          // power-of-two lengths: twiddles in smem
+    if (N > 0)
+        for (int i = threadIdx.x; i < ny; i += blockDim.x) stw[i] = a.py.tw[i];
     for (int i = threadIdx.x; i < ny * TILE; i += blockDim.x) {
         const int y = i / TILE, w = i - y * TILE;
         const int x = x0 + w;
@@ -191,7 +213,7 @@ surface_cols_kernel(const __grid_constant__ SurfaceArgs a) {
     __syncthreads();
     const float2 *res = sbuf;
     if constexpr (N > 0) {
-        ifft_pow2<N, TILE, cols_threads<N, TILE>()>(sbuf, vstride, a.py.tw);
+        ifft_pow2<N, TILE, cols_threads<N, TILE>()>(sbuf, vstride, stw);
     } else {
         res = ifft_generic(sbuf, sbuf + TILE * vstride, vstride, TILE, a.py);
     }
@@ -287,10 +309,10 @@ static size_t ws_scratch(int nx, int ny) { return ws_twy(nx) + align256((size_t)
 template <int N>
 static cudaError_t launch_rows_n(const SurfaceArgs &a, cudaStream_t st) {
     const int nx = a.nx;
-    size_t smem = (2 * (size_t)nx + (N > 0 ? 2 : 4) * (size_t)padded_len(nx)) * sizeof(float2);
+    size_t smem = (2 * (size_t)nx + (N > 0 ? 2 : 4) * (size_t)padded_len(nx) + (N > 0 ? nx : 0)) *
+                  sizeof(float2);
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(surface_rows_kernel<N>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = ensure_smem((const void *)surface_rows_kernel<N>, smem);
     if (e != cudaSuccess) return e;
     surface_rows_kernel<N><<<a.ny / 2 + 1, rows_threads<N>(), smem, st>>>(a);
     return cudaGetLastError();
@@ -299,10 +321,9 @@ static cudaError_t launch_rows_n(const SurfaceArgs &a, cudaStream_t st) {
 template <int N, int TILE>
 static cudaError_t launch_cols_n(const SurfaceArgs &a, cudaStream_t st) {
     const int ny = a.ny;
-    size_t smem = (N > 0 ? 1 : 2) * (size_t)TILE * padded_len(ny) * sizeof(float2);
+    size_t smem = ((N > 0 ? 1 : 2) * (size_t)TILE * padded_len(ny) + (N > 0 ? ny : 0)) * sizeof(float2);
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(surface_cols_kernel<N, TILE>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = ensure_smem((const void *)surface_cols_kernel<N, TILE>, smem);
     if (e != cudaSuccess) return e;
     dim3 grid((a.nx + TILE - 1) / TILE, a.npair);
     surface_cols_kernel<N, TILE><<<grid, cols_threads<N, TILE>(), smem, st>>>(a);
@@ -379,6 +400,7 @@ extern "C" int ocs_surface_update(const ocs_surface_desc *d, float t, void *stre
         if (i < d->nfields) {
             if (d->codes[i] < 0 || d->codes[i] >= OCS_FIELD_COUNT || !d->dst_d[i]) return OCS_ERR_ARG;
             a.code[i] = d->codes[i];
+            a.mult[i] = mult_desc(d->codes[i]);
             a.dst[i] = d->dst_d[i];
             a.add[i] = d->add ? d->add[i] : 0.f;
             a.swm[i] = d->swell_mult ? make_float2(d->swell_mult[2 * i], d->swell_mult[2 * i + 1])

@@ -251,6 +251,68 @@ class RawGenerator(object):
         for a in (range(self.az_steps) if steps is None else steps):
             self.pulse(a)
 
+    def reset(self):
+        """Clear the raw cube and NRCS accumulators and restart the Bragg refresh clock."""
+        self.raw_d.zero_()
+        self.nrcs_spec_d.zero_()
+        self.nrcs_bragg_d.zero_()
+        self.t_last_rcs_bragg = -1.
+        self._refreshes = []
+
+    # ------------------------------------------------------------------------------------
+    def capture(self):
+        """Record reset + every pulse of the scene into one CUDA graph.
+
+        The per-pulse host work (time, azimuth, refresh decision, launch arguments) is
+        done once, at capture; ``replay()`` then re-issues the whole scene with a single
+        graph launch.  One ordinary pass runs first (warm-up and lazy set-up)."""
+        self.reset()
+        self.run()
+        torch.cuda.synchronize()
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        g = torch.cuda.CUDAGraph()
+        saved, self.stream = self.stream, None
+        with torch.cuda.graph(g, stream=side):
+            self.reset()
+            self.run()
+        self.stream = saved
+        torch.cuda.current_stream().wait_stream(side)
+        self._graph = g
+        return g
+
+    def replay(self):
+        """Re-run the captured scene (raw cube and NRCS start from zero)."""
+        self._graph.replay()
+
+    def kernel_launches_per_scene(self):
+        """Kernels of this library launched by one pass over the scene."""
+        surf = 2 + (1 if self.surface._aux else 0)
+        nout = self.npol * self.num_ch
+        group = 2 if self.precision == 'f64' else 4
+        pulse = (nout + group - 1) // group
+        return self.az_steps * (surf + pulse)
+
+    def time_stages(self, steps):
+        """Average device time [ms] of the surface update and of the pulse kernel(s) over
+        ``steps`` pulses, from CUDA events on the launching stream."""
+        st = torch.cuda.current_stream()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+               torch.cuda.Event(enable_timing=True)) for _ in steps]
+        saved_last = self.t_last_rcs_bragg
+        for (e0, e1, e2), a in zip(ev, steps):
+            t_now = a * self.t_step
+            e0.record(st)
+            self.surface.set_t(t_now)
+            e1.record(st)
+            self.pulse(a, update_surface=False)
+            e2.record(st)
+        torch.cuda.synchronize()
+        self.t_last_rcs_bragg = saved_last
+        surf = [e0.elapsed_time(e1) for e0, e1, _ in ev]
+        puls = [e1.elapsed_time(e2) for _, e1, e2 in ev]
+        return float(np.mean(surf)), float(np.mean(puls)), surf, puls
+
     # ------------------------------------------------------------------------------------
     def nrcs_avg(self):
         """NRCS_avg[pol, az] (``:427-467``): specular plus Bragg, per unit surface area."""
