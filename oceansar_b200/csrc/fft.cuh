@@ -124,10 +124,11 @@ template <> OCS_D void dft_inv<7>(float2 *v) {
 
 // One in-place Stockham stage of radix R over nvec padded vectors: every thread loads
 // and transforms up to IT butterflies into registers, then (after a barrier) stores them.
+// tw: this stage's block of the stage-major twiddle table, w^(r*j*n/(ns*R)) at
+// [(r-1)*ns + j].
 template <int R, int IT>
 OCS_D void fft_stage_inplace(float2 *buf, int vstride, int nvec, int n, int ns, const float2 *tw) {
     const int nb = n / R;
-    const int tstep = n / (ns * R);
     float2 v[IT][R];
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
@@ -139,7 +140,7 @@ OCS_D void fft_stage_inplace(float2 *buf, int vstride, int nvec, int n, int ns, 
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 float2 a = x[pad_idx(j + r * nb)];
-                if (r > 0 && jm > 0) a = c_mul(a, tw[r * jm * tstep]);
+                if (r > 0 && jm > 0) a = c_mul(a, tw[(r - 1) * ns + jm]);
                 v[it][r] = a;
             }
             dft_inv<R>(v[it]);
@@ -162,7 +163,7 @@ OCS_D void fft_stage_inplace(float2 *buf, int vstride, int nvec, int n, int ns, 
 }
 
 // Power-of-two length N known at compile time: radix-8 stages, then one radix-4 or -2
-// stage; NVEC vectors, T threads.
+// stage; NVEC vectors, T threads; tw = the stage-major twiddle table.
 template <int N, int NVEC, int T, int NS = 1>
 OCS_D void ifft_pow2(float2 *buf, int vstride, const float2 *tw) {
     if constexpr (NS < N) {
@@ -170,7 +171,7 @@ OCS_D void ifft_pow2(float2 *buf, int vstride, const float2 *tw) {
         constexpr int R = (REM % 8 == 0) ? 8 : REM;
         constexpr int IT = ((N / R) * NVEC + T - 1) / T;
         fft_stage_inplace<R, IT>(buf, vstride, NVEC, N, NS, tw);
-        ifft_pow2<N, NVEC, T, NS * R>(buf, vstride, tw);
+        ifft_pow2<N, NVEC, T, NS * R>(buf, vstride, tw + (R - 1) * NS);
     }
 }
 

@@ -47,6 +47,7 @@ struct SurfaceArgs {
     float2 swell_rot;
     float2 *scratch;
     FftPlan px, py;
+    const float2 *stw_x, *stw_y;      // stage-major twiddles (power-of-two lengths)
 };
 
 // Spectral multiplier M of every field (ocean.py:431-526): Re(ifft2(M c)) is the field.
@@ -130,7 +131,7 @@ surface_rows_kernel(const __grid_constant__ SurfaceArgs a) {
     float2 *rowA = sbuf + 2 * nx, *rowB = rowA + vstride;
     float2 *stw = rowB + vstride;                 // power-of-two lengths: twiddles in smem
     if (N > 0)
-        for (int i = threadIdx.x; i < nx; i += blockDim.x) stw[i] = a.px.tw[i];
+        for (int i = threadIdx.x; i < nx; i += blockDim.x) stw[i] = a.stw_x[i];
     const float kyr = a.ky[r], kymr = a.ky[mr];
     const float *omA = a.omega + (size_t)r * nx, *omB = a.omega + (size_t)mr * nx;
 
@@ -204,7 +205,7 @@ surface_cols_kernel(const __grid_constant__ SurfaceArgs a) {
     const float2 *src = a.scratch + (size_t)p * ny * nx;
     float2 *stw = sbuf + TILE * vstride;          // power-of-two lengths: twiddles in smem
     if (N > 0)
-        for (int i = threadIdx.x; i < ny; i += blockDim.x) stw[i] = a.py.tw[i];
+        for (int i = threadIdx.x; i < ny; i += blockDim.x) stw[i] = a.stw_y[i];
     for (int i = threadIdx.x; i < ny * TILE; i += blockDim.x) {
         const int y = i / TILE, w = i - y * TILE;
         const int x = x0 + w;
@@ -291,6 +292,28 @@ static bool make_plan(int n, FftPlan &pl) {
 }
 
 
+// Stage-major twiddles of the power-of-two transform (radix 8, then 4 or 2): stage s with
+// radix R after radices of product ns holds w^(r*j*n/(ns*R)) at [(r-1)*ns + j],
+// 1 <= r < R, 0 <= j < ns, so that the lanes of a warp (consecutive j) read consecutive
+// entries.  Total length < n.
+__global__ void staged_twiddle_kernel(float2 *tw, int n) {
+    int base = 0;
+    for (int ns = 1; ns < n;) {
+        const int rem = n / ns;
+        const int R = (rem % 8 == 0) ? 8 : rem;
+        const int cnt = (R - 1) * ns;
+        const int tstep = n / (ns * R);
+        for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += gridDim.x * blockDim.x) {
+            const int r = e / ns + 1, j = e % ns;
+            double s, c;
+            sincospi(2.0 * (double)(r * j * tstep) / (double)n, &s, &c);
+            tw[base + e] = make_float2((float)c, (float)s);
+        }
+        base += cnt;
+        ns *= R;
+    }
+}
+
 __global__ void twiddle_kernel(float2 *tw, int n) {
     for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
         double s, c;
@@ -304,7 +327,10 @@ static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 // Workspace layout: [twiddles x (nx) | twiddles y (ny) | scratch planes npair*ny*nx].
 static size_t ws_twx(int) { return 0; }
 static size_t ws_twy(int nx) { return align256((size_t)nx * sizeof(float2)); }
-static size_t ws_scratch(int nx, int ny) { return ws_twy(nx) + align256((size_t)ny * sizeof(float2)); }
+static size_t ws_stx(int nx, int ny) { return ws_twy(nx) + align256((size_t)ny * sizeof(float2)); }
+static size_t ws_sty(int nx, int ny) { return ws_stx(nx, ny) + align256((size_t)nx * sizeof(float2)); }
+static size_t ws_scratch(int nx, int ny) { return ws_sty(nx, ny) + align256((size_t)ny * sizeof(float2)); }
+static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 
 template <int N>
 static cudaError_t launch_rows_n(const SurfaceArgs &a, cudaStream_t st) {
@@ -376,6 +402,8 @@ extern "C" int ocs_surface_prepare(int32_t nx, int32_t ny, void *workspace, void
     cudaStream_t st = (cudaStream_t)stream;
     twiddle_kernel<<<(nx + 255) / 256, 256, 0, st>>>((float2 *)(ws + ws_twx(nx)), nx);
     twiddle_kernel<<<(ny + 255) / 256, 256, 0, st>>>((float2 *)(ws + ws_twy(nx)), ny);
+    if (is_pow2(nx)) staged_twiddle_kernel<<<(nx + 255) / 256, 256, 0, st>>>((float2 *)(ws + ws_stx(nx, ny)), nx);
+    if (is_pow2(ny)) staged_twiddle_kernel<<<(ny + 255) / 256, 256, 0, st>>>((float2 *)(ws + ws_sty(nx, ny)), ny);
     return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
 }
 
@@ -416,6 +444,8 @@ extern "C" int ocs_surface_update(const ocs_surface_desc *d, float t, void *stre
     char *ws = (char *)d->workspace_d;
     a.px.tw = (const float2 *)(ws + ws_twx(nx));
     a.py.tw = (const float2 *)(ws + ws_twy(nx));
+    a.stw_x = (const float2 *)(ws + ws_stx(nx, ny));
+    a.stw_y = (const float2 *)(ws + ws_sty(nx, ny));
     a.scratch = (float2 *)(ws + ws_scratch(nx, ny));
     cudaStream_t st = (cudaStream_t)stream;
 
