@@ -260,12 +260,10 @@ def main():
         if world > 1:
             dist.barrier()
 
+    from oceansar_b200 import replicas
+
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, device="cuda")
 
     def timed(gen, steps, warmup):
         for _ in range(warmup):
@@ -283,7 +281,8 @@ def main():
         return max_over_ranks(e0.elapsed_time(e1) / steps)
 
     # ---- main arm ---------------------------------------------------------------------
-    gen = RawGenerator(cfg_path, precision=args.precision, overrides=overrides(c), seed=1000 + rank)
+    gen = RawGenerator(cfg_path, precision=args.precision, overrides=overrides(c),
+                       seed=replicas.replica_seed(1000, rank))
     if args.profile_pulses:
         gen.run(range(args.profile_pulses))
         torch.cuda.synchronize()
@@ -372,7 +371,8 @@ def main():
     if not args.no_fp64 and args.precision == "mixed":
         del gen
         torch.cuda.empty_cache()
-        g64 = RawGenerator(cfg_path, precision="f64", overrides=overrides(c), seed=1000 + rank)
+        g64 = RawGenerator(cfg_path, precision="f64", overrides=overrides(c),
+                           seed=replicas.replica_seed(1000, rank))
         g64.capture()
         ms64 = timed(g64, 1, 1)
         fp64 = {"value": echoes(c) * world / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64}
