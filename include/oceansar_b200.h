@@ -127,6 +127,15 @@ typedef struct {
 /* Choppy-wave slopes / curvatures from the auxiliary fields (ocean.py:451-456, 468-482). */
 int ocs_surface_choppy(const ocs_choppy_desc *desc, void *stream);
 
+/* ocs_surface_update for callers that cannot allocate device memory (no counterpart in the
+ * reference).  desc->workspace_d is ignored: the workspace is a 32 MiB device array
+ * compiled into the library, so ocs_surface_workspace_bytes(nx, ny, nfields) must be at
+ * most 32 MiB (else OCS_ERR_SIZE).  The first call on a device resolves that array's
+ * address (make it before any stream capture); all calls on a device share the array, so
+ * calls that overlap on the GPU race and must be serialised by the caller.  Allocates
+ * nothing. */
+int ocs_surface_update_noalloc(const ocs_surface_desc *desc, float t, void *stream);
+
 /* ------------------------------------------------------------------------------------
  * One radar pulse of the raw-data generator.
  *

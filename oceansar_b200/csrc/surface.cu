@@ -482,3 +482,56 @@ extern "C" int ocs_surface_choppy(const ocs_choppy_desc *d, void *stream) {
     surface_choppy_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(c);
     return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
 }
+
+// ---------------------------------------------------------------------------------------
+// Surface update without allocation.
+//
+// Some callers cannot allocate device memory: hosts that drive this library through the
+// bare C ABI with no device allocator of their own (for instance a ctypes binding in the
+// reference code base, which has no CUDA runtime beside this library), and real-time loops
+// that must never block on an allocation.  ocs_surface_update_noalloc serves them: its
+// workspace (twiddle tables and the packed FFT scratch planes) lives in the file-scope
+// device array below, so the caller passes only inputs and outputs.
+//
+// * Capacity: kNoAllocScratchBytes (32 MiB) per device, i.e. ocs_surface_workspace_bytes(
+//   nx, ny, nfields) must not exceed it (for example 1024 x 1024 with up to 6 fields or
+//   512 x 512 with up to 24); larger requests return OCS_ERR_SIZE.  The array is part of
+//   the loaded module, so every GPU that loads the library holds it until exit.
+// * Set-up: the first call on a device, with that device current, resolves the array's
+//   device address (cudaGetSymbolAddress) and caches it; make that first call before any
+//   stream capture.
+// * Sharing: every call on a device uses the same array, which keeps the last call's
+//   contents.  Each call rewrites the twiddle tables and overwrites the scratch planes
+//   completely before reading them, so nothing needs clearing, but calls that overlap on
+//   the GPU (different streams, or different host threads) race on the array and must be
+//   serialised by the caller.
+// * No cudaMalloc / cudaFree or any allocating library routine is called.
+constexpr size_t kNoAllocScratchBytes = 32u << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_ptr[64] = {nullptr};
+
+extern "C" int ocs_surface_update_noalloc(const ocs_surface_desc *d, float t, void *stream) {
+    if (!d) return OCS_ERR_ARG;
+    const int64_t need = ocs_surface_workspace_bytes(d->nx, d->ny, d->nfields);
+    if (need < 0) return OCS_ERR_ARG;
+    if ((size_t)need > kNoAllocScratchBytes) return OCS_ERR_SIZE;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return OCS_ERR_CUDA;
+    void *ws = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void *p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return OCS_ERR_CUDA;
+            g_noalloc_ptr[dev] = p;
+        }
+        ws = g_noalloc_ptr[dev];
+    }
+    int st = ocs_surface_prepare(d->nx, d->ny, ws, stream);
+    if (st != OCS_OK) return st;
+    ocs_surface_desc local = *d;
+    local.workspace_d = ws;
+    return ocs_surface_update(&local, t, stream);
+}
