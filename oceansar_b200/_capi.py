@@ -7,7 +7,9 @@ loaded, every entry point raises ``RuntimeError``.
 import ctypes
 import os
 
-_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "liboceansar_b200.so")
+# OCEANSAR_B200_LIB selects another build of the same library (e.g. a debug build).
+_LIB_PATH = os.environ.get("OCEANSAR_B200_LIB") or os.path.join(
+    os.path.dirname(os.path.abspath(__file__)), "_lib", "liboceansar_b200.so")
 
 OK = 0
 ERRORS = {

@@ -125,22 +125,27 @@ template <> OCS_D void dft_inv<7>(float2 *v) {
 // One in-place Stockham stage of radix R over nvec padded vectors: every thread loads
 // and transforms up to IT butterflies into registers, then (after a barrier) stores them.
 // tw: this stage's block of the stage-major twiddle table, w^(r*j*n/(ns*R)) at
-// [(r-1)*ns + j].
-template <int R, int IT>
-OCS_D void fft_stage_inplace(float2 *buf, int vstride, int nvec, int n, int ns, const float2 *tw) {
-    const int nb = n / R;
+// [(r-1)*ns + j].  N and NS are compile-time, so with nb = N/R and NS multiples of 8 the
+// padded index of element base + r*step is pad(base) + r*(step + step/8): every load and
+// store of a butterfly uses one base address plus constant offsets.
+template <int R, int IT, int N, int NS>
+OCS_D void fft_stage_inplace(float2 *buf, int vstride, int nvec, const float2 *tw) {
+    constexpr int nb = N / R;
+    static_assert(nb % 8 == 0, "power-of-two stages need N/R to be a multiple of 8");
+    constexpr int in_step = nb + nb / 8;                       // padded stride of the reads
+    constexpr int out_step = (NS % 8 == 0) ? NS + NS / 8 : NS; // padded stride of the writes
     float2 v[IT][R];
 #pragma unroll
     for (int it = 0; it < IT; ++it) {
         const int b = threadIdx.x + it * blockDim.x;
         if (b < nb * nvec) {
             const int vec = b / nb, j = b - vec * nb;
-            const float2 *x = buf + vec * vstride;
-            const int jm = j % ns;
+            const float2 *x = buf + vec * vstride + pad_idx(j);
+            const int jm = j % NS;
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                float2 a = x[pad_idx(j + r * nb)];
-                if (r > 0 && jm > 0) a = c_mul(a, tw[(r - 1) * ns + jm]);
+                float2 a = x[r * in_step];
+                if (r > 0 && jm > 0) a = c_mul(a, tw[(r - 1) * NS + jm]);
                 v[it][r] = a;
             }
             dft_inv<R>(v[it]);
@@ -152,11 +157,18 @@ OCS_D void fft_stage_inplace(float2 *buf, int vstride, int nvec, int n, int ns, 
         const int b = threadIdx.x + it * blockDim.x;
         if (b < nb * nvec) {
             const int vec = b / nb, j = b - vec * nb;
-            float2 *x = buf + vec * vstride;
-            const int jm = j % ns;
+            const int jm = j % NS;
             const int d = (j - jm) * R + jm;
+            float2 *x = buf + vec * vstride;
+            if (NS % 8 == 0 || NS == 1) {
+                // NS == 1: d = j*R, and pad(j*R + r) = pad(j*R) + r for r < R <= 8
+                float2 *y = x + pad_idx(d);
 #pragma unroll
-            for (int r = 0; r < R; ++r) x[pad_idx(d + r * ns)] = v[it][r];
+                for (int r = 0; r < R; ++r) y[r * out_step] = v[it][r];
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; ++r) x[pad_idx(d + r * NS)] = v[it][r];
+            }
         }
     }
     __syncthreads();
@@ -170,7 +182,7 @@ OCS_D void ifft_pow2(float2 *buf, int vstride, const float2 *tw) {
         constexpr int REM = N / NS;
         constexpr int R = (REM % 8 == 0) ? 8 : REM;
         constexpr int IT = ((N / R) * NVEC + T - 1) / T;
-        fft_stage_inplace<R, IT>(buf, vstride, NVEC, N, NS, tw);
+        fft_stage_inplace<R, IT, N, NS>(buf, vstride, NVEC, tw);
         ifft_pow2<N, NVEC, T, NS * R>(buf, vstride, tw + (R - 1) * NS);
     }
 }

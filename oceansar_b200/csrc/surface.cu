@@ -38,6 +38,7 @@ struct SurfaceArgs {
     float t;
     float inv_n;
     int npair;
+    int needs_omega;                  // some field's multiplier involves omega
     int code[2 * kMaxPacked];
     MultDesc mult[2 * kMaxPacked];
     float *dst[2 * kMaxPacked];
@@ -154,11 +155,15 @@ surface_rows_kernel(const __grid_constant__ SurfaceArgs a) {
                 const int xa = pr == 0 ? x : mx, xb = pr == 0 ? mx : x;   // columns of the pair
                 const float kxa = pr == 0 ? kxx : kxm, kxb = pr == 0 ? kxm : kxx;
                 const float2 c1 = cA[xa], c2 = cB[xb];
-                const float o1 = omA[xa], o2 = omB[xb];
-                const float k1 = __fsqrt_rn(fadd(fmul(kxa, kxa), fmul(kyr, kyr)));
-                const float k2 = __fsqrt_rn(fadd(fmul(kxb, kxb), fmul(kymr, kymr)));
-                const float ki1 = k1 > a.kmin_half ? __frcp_rn(k1) : 0.f;
-                const float ki2 = k2 > a.kmin_half ? __frcp_rn(k2) : 0.f;
+                const float o1 = a.needs_omega ? omA[xa] : 0.f, o2 = a.needs_omega ? omB[xb] : 0.f;
+                // |k| and 1/|k| from one reciprocal square root (1/|k| is 0 where |k| does not
+                // exceed min(kx_res, ky_res)/2, ocean.py:142-148)
+                const float q1 = fadd(fmul(kxa, kxa), fmul(kyr, kyr));
+                const float q2 = fadd(fmul(kxb, kxb), fmul(kymr, kymr));
+                const float r1 = q1 > 0.f ? rsqrtf(q1) : 0.f, r2 = q2 > 0.f ? rsqrtf(q2) : 0.f;
+                const float k1 = q1 * r1, k2 = q2 * r2;
+                const float ki1 = k1 > a.kmin_half ? r1 : 0.f;
+                const float ki2 = k2 > a.kmin_half ? r2 : 0.f;
                 const float2 xa1 = c_mul(field_mult(ca, kxa, kyr, k1, ki1, o1), c1);
                 const float2 xa2 = c_mul(field_mult(ca, kxb, kymr, k2, ki2, o2), c2);
                 float2 xb1 = make_float2(0.f, 0.f), xb2 = make_float2(0.f, 0.f);
@@ -429,6 +434,7 @@ extern "C" int ocs_surface_update(const ocs_surface_desc *d, float t, void *stre
             if (d->codes[i] < 0 || d->codes[i] >= OCS_FIELD_COUNT || !d->dst_d[i]) return OCS_ERR_ARG;
             a.code[i] = d->codes[i];
             a.mult[i] = mult_desc(d->codes[i]);
+            if (a.mult[i].d > 0 || a.mult[i].hmtf) a.needs_omega = 1;
             a.dst[i] = d->dst_d[i];
             a.add[i] = d->add ? d->add[i] : 0.f;
             a.swm[i] = d->swell_mult ? make_float2(d->swell_mult[2 * i], d->swell_mult[2 * i + 1])
