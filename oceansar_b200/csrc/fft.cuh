@@ -122,68 +122,113 @@ template <> OCS_D void dft_inv<7>(float2 *v) {
     }
 }
 
-// One in-place Stockham stage of radix R over nvec padded vectors: every thread loads
-// and transforms up to IT butterflies into registers, then (after a barrier) stores them.
-// tw: this stage's block of the stage-major twiddle table, w^(r*j*n/(ns*R)) at
-// [(r-1)*ns + j].  N and NS are compile-time, so with nb = N/R and NS multiples of 8 the
-// padded index of element base + r*step is pad(base) + r*(step + step/8): every load and
-// store of a butterfly uses one base address plus constant offsets.
-template <int R, int IT, int N, int NS>
-OCS_D void fft_stage_inplace(float2 *buf, int vstride, int nvec, const float2 *tw) {
+// Power-of-two lengths: NVEC vectors of compile-time length N, T threads.  Butterfly b
+// of a stage maps to vector b % NVEC and index b / NVEC (vector fastest), and vectors sit
+// pow2_vstride(N, NVEC) slots apart, so that the 16 lanes of a half-warp always hit 16
+// different 8-byte banks.  The first stage may read its inputs from a loader functor
+// (ld(vec, i) -> float2) instead of shared memory and the last stage may hand its outputs
+// to a storer functor (st(vec, i, value)) instead of writing them back: each saves one
+// pass over shared memory and a barrier.  Middle stages work in place: every thread loads
+// and transforms up to IT butterflies into registers, then, after a barrier, stores them.
+// tw: the stage-major twiddle table, w^(r*j*N/(NS*R)) of a stage at [(r-1)*NS + j].
+OCS_HD int pow2_vstride(int n, int nvec) {
+    int v = n + (n >> 3) + 1;
+    const int want = nvec >= 16 ? 0 : 16 / nvec;
+    return v + ((want - (v & 15)) & 15);
+}
+
+struct NoLoad {
+    OCS_D float2 operator()(int, int) const { return make_float2(0.f, 0.f); }
+};
+struct NoStore {
+    OCS_D void operator()(int, int, float2) const {}
+};
+
+template <int R, int IT, int N, int NS, int NVEC, bool FIRST, bool LAST, class Ld, class St>
+OCS_D void fft_stage_pow2(float2 *buf, int vstride, const float2 *tw, const Ld &ld, const St &st) {
     constexpr int nb = N / R;
     static_assert(nb % 8 == 0, "power-of-two stages need N/R to be a multiple of 8");
     constexpr int in_step = nb + nb / 8;                       // padded stride of the reads
     constexpr int out_step = (NS % 8 == 0) ? NS + NS / 8 : NS; // padded stride of the writes
-    float2 v[IT][R];
+    static_assert(NS == 1 || NS % 8 == 0, "stage spans must be 1 or multiples of 8");
+    if constexpr (FIRST || LAST) {
+        // independent butterflies: nothing else in shared memory is read (FIRST) or
+        // written (LAST) in this stage, so each result is written out immediately
 #pragma unroll
-    for (int it = 0; it < IT; ++it) {
-        const int b = threadIdx.x + it * blockDim.x;
-        if (b < nb * nvec) {
-            const int vec = b / nb, j = b - vec * nb;
-            const float2 *x = buf + vec * vstride + pad_idx(j);
-            const int jm = j % NS;
+        for (int it = 0; it < IT; ++it) {
+            const int b = threadIdx.x + it * blockDim.x;
+            if (b < nb * NVEC) {
+                const int vec = b % NVEC, j = b / NVEC;
+                const int jm = j % NS;
+                float2 v[R];
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                float2 a = x[r * in_step];
-                if (r > 0 && jm > 0) a = c_mul(a, tw[(r - 1) * NS + jm]);
-                v[it][r] = a;
+                for (int r = 0; r < R; ++r) {
+                    float2 a;
+                    if constexpr (FIRST) a = ld(vec, j + r * nb);
+                    else a = buf[vec * vstride + pad_idx(j) + r * in_step];
+                    if (r > 0 && jm > 0) a = c_mul(a, tw[(r - 1) * NS + jm]);
+                    v[r] = a;
+                }
+                dft_inv<R>(v);
+                const int d = (j - jm) * R + jm;
+                if constexpr (LAST) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) st(vec, d + r * NS, v[r]);
+                } else {
+                    float2 *y = buf + vec * vstride + pad_idx(d);
+#pragma unroll
+                    for (int r = 0; r < R; ++r) y[r * out_step] = v[r];
+                }
             }
-            dft_inv<R>(v[it]);
         }
-    }
-    __syncthreads();
+        if constexpr (!LAST) __syncthreads();
+    } else {
+        float2 v[IT][R];
 #pragma unroll
-    for (int it = 0; it < IT; ++it) {
-        const int b = threadIdx.x + it * blockDim.x;
-        if (b < nb * nvec) {
-            const int vec = b / nb, j = b - vec * nb;
-            const int jm = j % NS;
-            const int d = (j - jm) * R + jm;
-            float2 *x = buf + vec * vstride;
-            if (NS % 8 == 0 || NS == 1) {
-                // NS == 1: d = j*R, and pad(j*R + r) = pad(j*R) + r for r < R <= 8
-                float2 *y = x + pad_idx(d);
+        for (int it = 0; it < IT; ++it) {
+            const int b = threadIdx.x + it * blockDim.x;
+            if (b < nb * NVEC) {
+                const int vec = b % NVEC, j = b / NVEC;
+                const float2 *x = buf + vec * vstride + pad_idx(j);
+                const int jm = j % NS;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    float2 a = x[r * in_step];
+                    if (r > 0 && jm > 0) a = c_mul(a, tw[(r - 1) * NS + jm]);
+                    v[it][r] = a;
+                }
+                dft_inv<R>(v[it]);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int b = threadIdx.x + it * blockDim.x;
+            if (b < nb * NVEC) {
+                const int vec = b % NVEC, j = b / NVEC;
+                const int jm = j % NS;
+                float2 *y = buf + vec * vstride + pad_idx((j - jm) * R + jm);
 #pragma unroll
                 for (int r = 0; r < R; ++r) y[r * out_step] = v[it][r];
-            } else {
-#pragma unroll
-                for (int r = 0; r < R; ++r) x[pad_idx(d + r * NS)] = v[it][r];
             }
         }
+        __syncthreads();
     }
-    __syncthreads();
 }
 
-// Power-of-two length N known at compile time: radix-8 stages, then one radix-4 or -2
-// stage; NVEC vectors, T threads; tw = the stage-major twiddle table.
-template <int N, int NVEC, int T, int NS = 1>
-OCS_D void ifft_pow2(float2 *buf, int vstride, const float2 *tw) {
+// The whole transform: radix-8 stages, then one radix-4 or -2 stage.  Without a loader
+// the inputs are read from buf (and must be complete before the call); without a storer
+// the results are left in buf (complete when the call returns).
+template <int N, int NVEC, int T, bool HAS_LD, bool HAS_ST, int NS = 1, class Ld = NoLoad, class St = NoStore>
+OCS_D void ifft_pow2(float2 *buf, int vstride, const float2 *tw, const Ld &ld = Ld(), const St &st = St()) {
     if constexpr (NS < N) {
         constexpr int REM = N / NS;
         constexpr int R = (REM % 8 == 0) ? 8 : REM;
         constexpr int IT = ((N / R) * NVEC + T - 1) / T;
-        fft_stage_inplace<R, IT, N, NS>(buf, vstride, NVEC, tw);
-        ifft_pow2<N, NVEC, T, NS * R>(buf, vstride, tw + (R - 1) * NS);
+        constexpr bool first = HAS_LD && NS == 1;
+        constexpr bool last = HAS_ST && NS * R == N;
+        fft_stage_pow2<R, IT, N, NS, NVEC, first, last>(buf, vstride, tw, ld, st);
+        ifft_pow2<N, NVEC, T, HAS_LD, HAS_ST, NS * R>(buf, vstride, tw + (R - 1) * NS, ld, st);
     }
 }
 

@@ -116,6 +116,48 @@ template <int N, int TILE> __host__ __device__ constexpr int cols_threads() {
     return N == 0 ? 256 : (N * TILE / 16 < 64 ? 64 : (N * TILE / 16 > 1024 ? 1024 : N * TILE / 16));
 }
 
+// Output of the row transforms: vector 0 is row r, vector 1 row mr of one scratch plane.
+struct RowStore {
+    float2 *plane;
+    int nx, r, mr;
+    OCS_D void operator()(int vec, int x, float2 v) const {
+        if (vec == 1 && mr == r) return;
+        plane[(size_t)(vec ? mr : r) * nx + x] = v;
+    }
+};
+
+// Input of the column transforms: TILE consecutive columns of one scratch plane.
+struct ColLoad {
+    const float2 *plane;
+    int nx, x0;
+    OCS_D float2 operator()(int w, int y) const {
+        const int x = x0 + w;
+        return x < nx ? plane[(size_t)y * nx + x] : make_float2(0.f, 0.f);
+    }
+};
+
+// Output of the column transforms: scale, additive terms, swell, two float32 fields.
+struct ColStore {
+    float *dA, *dB;
+    const float2 *swell_exp;
+    float2 swell_rot, smA, smB;
+    float inv_n, addA, addB;
+    int nx, x0;
+    OCS_D void operator()(int w, int y, float2 z) const {
+        const int x = x0 + w;
+        if (x >= nx) return;
+        float va = fadd(z.x * inv_n, addA);
+        float vb = fadd(z.y * inv_n, addB);
+        if (swell_exp) {
+            const float2 s = c_mul(swell_exp[(size_t)y * nx + x], swell_rot);
+            va = fadd(va, fsub(fmul(smA.x, s.x), fmul(smA.y, s.y)));
+            vb = fadd(vb, fsub(fmul(smB.x, s.x), fmul(smB.y, s.y)));
+        }
+        dA[(size_t)y * nx + x] = va;
+        if (dB) dB[(size_t)y * nx + x] = vb;
+    }
+};
+
 // Pass 1.  Shared memory: c(t) of rows r and mr ([2][nx], unpadded), then the two padded
 // FFT rows (and, for non-power-of-two lengths, two more for the ping-pong).  Mirror pairs:
 // (r,x) <-> (mr,mx) and (r,mx) <-> (mr,x).
@@ -127,7 +169,7 @@ surface_rows_kernel(const __grid_constant__ SurfaceArgs a) {
     const int ny = a.ny;
     const int r = blockIdx.x;
     const int mr = (ny - r) % ny;
-    const int vstride = padded_len(nx);
+    const int vstride = (N > 0) ? pow2_vstride(nx, 2) : padded_len(nx);
     float2 *cA = sbuf, *cB = sbuf + nx;
     float2 *rowA = sbuf + 2 * nx, *rowB = rowA + vstride;
     float2 *stw = rowB + vstride;                 // power-of-two lengths: twiddles in smem
@@ -181,23 +223,25 @@ surface_rows_kernel(const __grid_constant__ SurfaceArgs a) {
             }
         }
         __syncthreads();
-        const float2 *res = rowA;
         if constexpr (N > 0) {
-            ifft_pow2<N, 2, rows_threads<N>()>(rowA, vstride, stw);
+            // the last stage writes straight into the scratch plane
+            const RowStore st{a.scratch + (size_t)p * ny * nx, nx, r, mr};
+            ifft_pow2<N, 2, rows_threads<N>(), false, true>(rowA, vstride, stw, NoLoad(), st);
         } else {
-            res = ifft_generic(rowA, rowB + vstride, vstride, 2, a.px);
-        }
-        float2 *outA = a.scratch + ((size_t)p * ny + r) * nx;
-        float2 *outB = a.scratch + ((size_t)p * ny + mr) * nx;
-        for (int x = threadIdx.x; x < nx; x += blockDim.x) {
-            outA[x] = res[pad_idx(x)];
-            if (mr != r) outB[x] = res[vstride + pad_idx(x)];
+            const float2 *res = ifft_generic(rowA, rowB + vstride, vstride, 2, a.px);
+            float2 *outA = a.scratch + ((size_t)p * ny + r) * nx;
+            float2 *outB = a.scratch + ((size_t)p * ny + mr) * nx;
+            for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+                outA[x] = res[pad_idx(x)];
+                if (mr != r) outB[x] = res[vstride + pad_idx(x)];
+            }
         }
         __syncthreads();
     }
 }
 
-// Pass 2.  One CTA per (transform p, tile of TILE columns).
+// Pass 2.  One CTA per (transform p, tile of TILE columns).  Power-of-two lengths read
+// the tile inside the first FFT stage and unpack the fields inside the last one.
 template <int N, int TILE>
 __global__ void __launch_bounds__(cols_threads<N, TILE>(), cols_threads<N, TILE>() <= 512 ? 2 : 1)
 surface_cols_kernel(const __grid_constant__ SurfaceArgs a) {
@@ -206,41 +250,26 @@ surface_cols_kernel(const __grid_constant__ SurfaceArgs a) {
     const int ny = (N > 0) ? N : a.ny;
     const int p = blockIdx.y;
     const int x0 = blockIdx.x * TILE;
-    const int vstride = padded_len(ny);
+    const int vstride = (N > 0) ? pow2_vstride(ny, TILE) : padded_len(ny);
     const float2 *src = a.scratch + (size_t)p * ny * nx;
-    float2 *stw = sbuf + TILE * vstride;          // power-of-two lengths: twiddles in smem
-    if (N > 0)
-        for (int i = threadIdx.x; i < ny; i += blockDim.x) stw[i] = a.stw_y[i];
-    for (int i = threadIdx.x; i < ny * TILE; i += blockDim.x) {
-        const int y = i / TILE, w = i - y * TILE;
-        const int x = x0 + w;
-        sbuf[w * vstride + pad_idx(y)] = (x < nx) ? src[(size_t)y * nx + x] : make_float2(0.f, 0.f);
-    }
-    __syncthreads();
-    const float2 *res = sbuf;
+    const ColStore st{a.dst[2 * p], a.dst[2 * p + 1], a.swell_exp, a.swell_rot, a.swm[2 * p],
+                      a.swm[2 * p + 1], a.inv_n, a.add[2 * p], a.add[2 * p + 1], nx, x0};
     if constexpr (N > 0) {
-        ifft_pow2<N, TILE, cols_threads<N, TILE>()>(sbuf, vstride, stw);
+        float2 *stw = sbuf + TILE * vstride;      // twiddles in smem (first used in stage 2)
+        for (int i = threadIdx.x; i < ny; i += blockDim.x) stw[i] = a.stw_y[i];
+        ifft_pow2<N, TILE, cols_threads<N, TILE>(), true, true>(sbuf, vstride, stw, ColLoad{src, nx, x0}, st);
     } else {
-        res = ifft_generic(sbuf, sbuf + TILE * vstride, vstride, TILE, a.py);
-    }
-    float *dA = a.dst[2 * p], *dB = a.dst[2 * p + 1];
-    const float addA = a.add[2 * p], addB = a.add[2 * p + 1];
-    const float2 smA = a.swm[2 * p], smB = a.swm[2 * p + 1];
-    const bool sw = a.swell_exp != nullptr;
-    for (int i = threadIdx.x; i < ny * TILE; i += blockDim.x) {
-        const int y = i / TILE, w = i - y * TILE;
-        const int x = x0 + w;
-        if (x >= nx) continue;
-        float2 z = res[w * vstride + pad_idx(y)];
-        float va = fadd(z.x * a.inv_n, addA);
-        float vb = fadd(z.y * a.inv_n, addB);
-        if (sw) {
-            float2 s = c_mul(a.swell_exp[(size_t)y * nx + x], a.swell_rot);
-            va = fadd(va, fsub(fmul(smA.x, s.x), fmul(smA.y, s.y)));
-            vb = fadd(vb, fsub(fmul(smB.x, s.x), fmul(smB.y, s.y)));
+        for (int i = threadIdx.x; i < ny * TILE; i += blockDim.x) {
+            const int y = i / TILE, w = i - y * TILE;
+            const int x = x0 + w;
+            sbuf[w * vstride + pad_idx(y)] = (x < nx) ? src[(size_t)y * nx + x] : make_float2(0.f, 0.f);
         }
-        dA[(size_t)y * nx + x] = va;
-        if (dB) dB[(size_t)y * nx + x] = vb;
+        __syncthreads();
+        const float2 *res = ifft_generic(sbuf, sbuf + TILE * vstride, vstride, TILE, a.py);
+        for (int i = threadIdx.x; i < ny * TILE; i += blockDim.x) {
+            const int y = i / TILE, w = i - y * TILE;
+            st(w, y, res[w * vstride + pad_idx(y)]);
+        }
     }
 }
 
@@ -340,8 +369,8 @@ static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 template <int N>
 static cudaError_t launch_rows_n(const SurfaceArgs &a, cudaStream_t st) {
     const int nx = a.nx;
-    size_t smem = (2 * (size_t)nx + (N > 0 ? 2 : 4) * (size_t)padded_len(nx) + (N > 0 ? nx : 0)) *
-                  sizeof(float2);
+    size_t smem = (N > 0) ? (3 * (size_t)nx + 2 * (size_t)pow2_vstride(nx, 2)) * sizeof(float2)
+                          : (2 * (size_t)nx + 4 * (size_t)padded_len(nx)) * sizeof(float2);
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
     cudaError_t e = ensure_smem((const void *)surface_rows_kernel<N>, smem);
     if (e != cudaSuccess) return e;
@@ -352,7 +381,8 @@ static cudaError_t launch_rows_n(const SurfaceArgs &a, cudaStream_t st) {
 template <int N, int TILE>
 static cudaError_t launch_cols_n(const SurfaceArgs &a, cudaStream_t st) {
     const int ny = a.ny;
-    size_t smem = ((N > 0 ? 1 : 2) * (size_t)TILE * padded_len(ny) + (N > 0 ? ny : 0)) * sizeof(float2);
+    size_t smem = (N > 0) ? ((size_t)TILE * pow2_vstride(ny, TILE) + ny) * sizeof(float2)
+                          : 2 * (size_t)TILE * padded_len(ny) * sizeof(float2);
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
     cudaError_t e = ensure_smem((const void *)surface_cols_kernel<N, TILE>, smem);
     if (e != cudaSuccess) return e;
