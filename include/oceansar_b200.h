@@ -191,7 +191,11 @@ typedef struct {
     int32_t nbins;                       /* rg_samp                                          */
     double *nrcs_spec_d;                 /* float64 [az_steps]: += sum |E_spec|^2            */
     double *nrcs_bragg_d;                /* float64 [npol][az_steps]: += sum RCS at refresh  */
+    void *rowtab_d;                      /* ocs_pulse_workspace_bytes(ny, nch) bytes         */
 } ocs_pulse_desc;
+
+/* Workspace of ocs_pulse (per-pulse table of the row quantities); < 0 on invalid sizes. */
+int64_t ocs_pulse_workspace_bytes(int32_t ny, int32_t nch);
 
 /* Accumulate one pulse into raw_d (OCS_PREC_F64: the float64 drop-in; OCS_PREC_MIXED:
  * float64 range / phase reduction, float32 elsewhere). */

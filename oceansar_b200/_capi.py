@@ -39,10 +39,12 @@ SIGNATURES = {
     "ocs_surface_choppy": [c_ptr, c_ptr],
     "ocs_surface_update_noalloc": [c_ptr, c_flt, c_ptr],
     "ocs_pulse": [c_ptr, c_int, c_ptr],
+    "ocs_pulse_workspace_bytes": [ctypes.c_int32, ctypes.c_int32],
     "ocs_rcs_romeiser": [c_ptr, c_ptr],
     "ocs_field_kodis": [c_ptr, c_ptr],
 }
-_RESTYPE = {"ocs_version": ctypes.c_char_p, "ocs_surface_workspace_bytes": ctypes.c_int64}
+_RESTYPE = {"ocs_version": ctypes.c_char_p, "ocs_surface_workspace_bytes": ctypes.c_int64,
+            "ocs_pulse_workspace_bytes": ctypes.c_int64}
 
 _lib = None
 

@@ -32,7 +32,7 @@ class PulseDesc(ctypes.Structure):
                 ("scat_d", P), ("s_m_d", P), ("s_p_d", P), ("n_m", I64), ("n_p", I64),
                 ("ind0_m_d", P), ("ind0_p_d", P),
                 ("sinc_d", P), ("raw_d", P), ("nbins", I32),
-                ("nrcs_spec_d", P), ("nrcs_bragg_d", P)]
+                ("nrcs_spec_d", P), ("nrcs_bragg_d", P), ("rowtab_d", P)]
 
 
 class RcsDesc(ctypes.Structure):

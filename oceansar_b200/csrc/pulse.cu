@@ -27,7 +27,7 @@
 namespace ocs {
 
 constexpr int kPulseCols = 128;     // columns (threads) per CTA
-constexpr int kPulseRows = 32;      // rows per tile
+constexpr int kPulseRows = 64;      // rows per tile
 constexpr int kMaxCh = 8;
 constexpr int kPulseNbw = 160;      // CTA shared bin window
 
@@ -52,6 +52,7 @@ struct PulseArgs {
     int tmod_m, tmod_p;                     // int(t_now * prf) mod n_m, n_p
     const int *ind0_m, *ind0_p;             // [ny][nx]
     const float *sinc;                      // [8*20 + 1]
+    double *rowtab;                         // per-pulse row table, see pulse_rows_kernel
     void *raw;                              // [npol*nch][az_steps][rg_samp] complex T
     long long raw_out_stride, raw_row;      // elements between outputs, offset of this pulse row
     int nbins;
@@ -108,8 +109,32 @@ OCS_D void block_atomic_sum(double v, double *dst, double *sred) {
     }
 }
 
+// Per-pulse row table (sar_raw_nompi.py:353-363, 485-493): for every facet row y,
+// rowtab[q*ny + y] holds az, sin_az = az/sr0, the ground-projected azimuth angle and its
+// cos / sin (q = 0..4), then rowtab[5*ny + 2*(y*nch + c)] the complex antenna-pattern x
+// ATI-phase factor of channel c.  float64, computed once per pulse for all tiles.
+__global__ void pulse_rows_kernel(const __grid_constant__ PulseArgs a) {
+    for (int y = blockIdx.x * blockDim.x + threadIdx.x; y < a.ny; y += gridDim.x * blockDim.x) {
+        const double az = dsub((double)a.y[y], a.az_now);
+        const double sin_az = ddiv(az, a.sr0);
+        const double azp = asin(az / a.gr0);
+        a.rowtab[y] = az;
+        a.rowtab[(long long)a.ny + y] = sin_az;
+        a.rowtab[2LL * a.ny + y] = azp;
+        a.rowtab[3LL * a.ny + y] = cos(azp);
+        a.rowtab[4LL * a.ny + y] = sin(azp);
+        const double bp = np_sinc(a.ltx_over_l * sin_az) * np_sinc(a.lrx_over_l * sin_az);
+        double *fac = a.rowtab + 5LL * a.ny + 2LL * y * a.nch;
+        for (int c = 0; c < a.nch; ++c) {
+            const c128 ati = cexpi((-a.k0 * a.b_ati[c]) * sin_az);
+            fac[2 * c] = bp * ati.re;
+            fac[2 * c + 1] = bp * ati.im;
+        }
+    }
+}
+
 template <typename T, int NOUT, int S>
-__global__ void __launch_bounds__(kPulseCols, sizeof(T) == 4 ? 4 : 2)
+__global__ void __launch_bounds__(kPulseCols, (sizeof(T) == 4 && NOUT < 4) ? 4 : 2)
 pulse_kernel(const __grid_constant__ PulseArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr int wlen = wtab_len<T, S>(kSincTaps, kSincOvs);
@@ -133,21 +158,15 @@ pulse_kernel(const __grid_constant__ PulseArgs a) {
     const int y0 = (tile / tiles_x) * kPulseRows;
     const int nrows = min(kPulseRows, a.ny - y0);
     __syncthreads();                    // previous tile's bins and row tables are consumed
-    // per-row quantities (sar_raw_nompi.py:353-363, 485-493)
-    for (int i = threadIdx.x; i < nrows; i += blockDim.x) {
-        const double az = dsub((double)a.y[y0 + i], a.az_now);
-        const double sin_az = ddiv(az, a.sr0);
-        const double azp = asin(az / a.gr0);
-        r_az[i] = az;
-        r_sinaz[i] = sin_az;
-        r_azp[i] = azp;
-        r_cazp[i] = cos(azp);
-        r_sazp[i] = sin(azp);
-        const double bp = np_sinc(a.ltx_over_l * sin_az) * np_sinc(a.lrx_over_l * sin_az);
-        for (int c = 0; c < a.nch; ++c) {
-            const c128 ati = cexpi((-a.k0 * a.b_ati[c]) * sin_az);
-            r_fac[i * a.nch + c] = {(T)(bp * ati.re), (T)(bp * ati.im)};
-        }
+    // this tile's rows of the per-pulse row table (pulse_rows_kernel)
+    for (int i = threadIdx.x; i < nrows * 5; i += blockDim.x) {
+        const int q = i / nrows, k = i - q * nrows;
+        r_az[q * kPulseRows + k] = a.rowtab[(long long)q * a.ny + y0 + k];
+    }
+    {
+        const double *fac = a.rowtab + 5LL * a.ny + 2LL * y0 * a.nch;
+        for (int i = threadIdx.x; i < nrows * a.nch; i += blockDim.x)
+            r_fac[i] = {(T)fac[2 * i], (T)fac[2 * i + 1]};
     }
 
     CtaBins<T, NOUT> cb;
@@ -339,7 +358,7 @@ static int fill_pulse_args(const ocs_pulse_desc *d, PulseArgs &a) {
                         !d->spec_s_d || d->spec_n < 2 || !d->nrcs_bragg_d))
         return OCS_ERR_ARG;
     if (d->do_bragg && d->use_hmtf && !d->hmtf_d) return OCS_ERR_ARG;
-    if (d->az_step < 0 || d->az_step >= d->az_steps || d->nbins < 1) return OCS_ERR_ARG;
+    if (d->az_step < 0 || d->az_step >= d->az_steps || d->nbins < 1 || !d->rowtab_d) return OCS_ERR_ARG;
     if ((d->npol == 2) != (d->pol == POL_DP)) return OCS_ERR_ARG;
     a.nx = d->nx; a.ny = d->ny; a.npol = d->npol; a.nch = d->nch;
     a.dx_f = d->dx_d; a.dy_f = d->dy_d; a.dz_f = d->dz_d;
@@ -381,11 +400,17 @@ static int fill_pulse_args(const ocs_pulse_desc *d, PulseArgs &a) {
     a.ind0_m = d->ind0_m_d; a.ind0_p = d->ind0_p_d;
     a.sinc = d->sinc_d;
     a.raw = d->raw_d;
+    a.rowtab = (double *)d->rowtab_d;
     a.nbins = d->nbins;
     a.raw_out_stride = (long long)d->az_steps * d->nbins;
     a.raw_row = (long long)d->az_step * d->nbins;
     a.nrcs_spec = d->nrcs_spec_d; a.nrcs_bragg = d->nrcs_bragg_d; a.az_steps = d->az_steps;
     return OCS_OK;
+}
+
+extern "C" int64_t ocs_pulse_workspace_bytes(int32_t ny, int32_t nch) {
+    if (ny < 1 || nch < 1 || nch > kMaxCh) return -1;
+    return (int64_t)ny * (5 + 2 * nch) * (int64_t)sizeof(double);
 }
 
 extern "C" int ocs_pulse(const ocs_pulse_desc *d, int precision, void *stream) {
@@ -394,6 +419,8 @@ extern "C" int ocs_pulse(const ocs_pulse_desc *d, int precision, void *stream) {
     if (st != OCS_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
     const int nout = d->npol * d->nch;
+    pulse_rows_kernel<<<(d->ny + 127) / 128, 128, 0, s>>>(a);
+    if (cudaGetLastError() != cudaSuccess) return OCS_ERR_CUDA;
     if (precision == OCS_PREC_F64) {
         for (int o = 0; o < nout; o += 2) {
             a.out0 = o;
@@ -408,8 +435,8 @@ extern "C" int ocs_pulse(const ocs_pulse_desc *d, int precision, void *stream) {
         for (int o = 0; o < nout; o += 4) {
             a.out0 = o;
             a.nout = nout - o < 4 ? nout - o : 4;
-            if (a.nout == 1) st = launch_pulse<float, 1, 16>(a, s);
-            else if (a.nout == 2) st = launch_pulse<float, 2, 16>(a, s);
+            if (a.nout == 1) st = launch_pulse<float, 1, 12>(a, s);
+            else if (a.nout == 2) st = launch_pulse<float, 2, 12>(a, s);
             else st = launch_pulse<float, 4, 12>(a, s);
             if (st != OCS_OK) return st;
             a.refresh = 0;

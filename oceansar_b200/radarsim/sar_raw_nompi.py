@@ -221,6 +221,9 @@ class RawGenerator(object):
         d.nbins = self.rg_samp
         d.nrcs_spec_d = self.nrcs_spec_d.data_ptr()
         d.nrcs_bragg_d = self.nrcs_bragg_d.data_ptr()
+        nb = _capi.load().ocs_pulse_workspace_bytes(s.Ny, self.num_ch)
+        self._rowtab = torch.empty(int(nb), dtype=torch.uint8, device=_device.device())
+        d.rowtab_d = self._rowtab.data_ptr()
         self._refreshes = []
 
     # ------------------------------------------------------------------------------------
@@ -290,7 +293,7 @@ class RawGenerator(object):
         surf = 2 + (1 if self.surface._aux else 0)
         nout = self.npol * self.num_ch
         group = 2 if self.precision == 'f64' else 4
-        pulse = (nout + group - 1) // group
+        pulse = 1 + (nout + group - 1) // group          # row table + pulse kernel(s)
         return self.az_steps * (surf + pulse)
 
     def time_stages(self, steps):
