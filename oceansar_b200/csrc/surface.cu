@@ -158,10 +158,106 @@ struct ColStore {
     }
 };
 
+// Compile-time field programs of the row pass.  Program 1 is the field set of sar_raw
+// with the specular model (Dx Dy | Dz Diffx | Diffy Diffxx | Diffyy Diffxy), program 2
+// the one without it (Dx Dy | Dz Diffx | Diffy -); any other list runs program 0, which
+// evaluates the MultDesc recipes at run time.
+constexpr int kNone = -2;       // no second field in the pair
+constexpr int kRuntime = -1;    // recipe read from SurfaceArgs::mult
+
+template <int CODE> __host__ __device__ constexpr bool needs_kinv() {
+    return CODE == kRuntime || CODE == OCS_FIELD_DX || CODE == OCS_FIELD_DY || CODE == OCS_FIELD_VX ||
+           CODE == OCS_FIELD_VY || CODE == OCS_FIELD_AX || CODE == OCS_FIELD_AY || CODE == OCS_FIELD_HMTF ||
+           CODE >= OCS_FIELD_AUX_XX;
+}
+
+// Multiplier of a compile-time field code (kRuntime: the run-time recipe m).
+template <int CODE>
+OCS_D float2 mult_ct(const MultDesc &m, float kx, float ky, float k, float kinv, float om) {
+    if constexpr (CODE == kRuntime) return field_mult(m, kx, ky, k, kinv, om);
+    else if constexpr (CODE == OCS_FIELD_DZ) return make_float2(1.f, 0.f);
+    else if constexpr (CODE == OCS_FIELD_DX) return make_float2(0.f, kx * kinv);
+    else if constexpr (CODE == OCS_FIELD_DY) return make_float2(0.f, ky * kinv);
+    else if constexpr (CODE == OCS_FIELD_DIFFX) return make_float2(0.f, kx);
+    else if constexpr (CODE == OCS_FIELD_DIFFY) return make_float2(0.f, ky);
+    else if constexpr (CODE == OCS_FIELD_DIFFXX) return make_float2(-(kx * kx), 0.f);
+    else if constexpr (CODE == OCS_FIELD_DIFFYY) return make_float2(-(ky * ky), 0.f);
+    else if constexpr (CODE == OCS_FIELD_DIFFXY) return make_float2(-(kx * ky), 0.f);
+    else return field_mult(m, kx, ky, k, kinv, om);
+}
+
+// Packed spectra of transform p at the two mirror pairs of column x (pass 1):
+// (r, x) <-> (mr, nx-x) and (r, nx-x) <-> (mr, x).
+template <int CA, int CB>
+OCS_D void build_packed(const SurfaceArgs &a, int p, int x, int nx, float kyr, float kymr, const float2 *cA,
+                        const float2 *cB, const float *omA, const float *omB, float2 *rowA, float2 *rowB) {
+    const MultDesc ma = a.mult[2 * p], mb = a.mult[2 * p + 1];
+    const bool has_b = (CB == kRuntime) ? a.code[2 * p + 1] >= 0 : CB != kNone;
+    constexpr bool need_k = needs_kinv<CA>() || needs_kinv<CB>();
+    const int mx = (nx - x) % nx;
+    const float kxx = a.kx[x], kxm = a.kx[mx];
+#pragma unroll
+    for (int pr = 0; pr < 2; ++pr) {
+        const int xa = pr == 0 ? x : mx, xb = pr == 0 ? mx : x;   // columns of the pair
+        const float kxa = pr == 0 ? kxx : kxm, kxb = pr == 0 ? kxm : kxx;
+        const float2 c1 = cA[xa], c2 = cB[xb];
+        const bool om_needed = (CA == kRuntime || CB == kRuntime) && a.needs_omega;
+        const float o1 = om_needed ? omA[xa] : 0.f, o2 = om_needed ? omB[xb] : 0.f;
+        float k1 = 0.f, k2 = 0.f, ki1 = 0.f, ki2 = 0.f;
+        if constexpr (need_k) {
+            // |k| and 1/|k| from one reciprocal square root (1/|k| is 0 where |k| does not
+            // exceed min(kx_res, ky_res)/2, ocean.py:142-148)
+            const float q1 = fadd(fmul(kxa, kxa), fmul(kyr, kyr));
+            const float q2 = fadd(fmul(kxb, kxb), fmul(kymr, kymr));
+            const float r1 = q1 > 0.f ? rsqrtf(q1) : 0.f, r2 = q2 > 0.f ? rsqrtf(q2) : 0.f;
+            k1 = q1 * r1;
+            k2 = q2 * r2;
+            ki1 = k1 > a.kmin_half ? r1 : 0.f;
+            ki2 = k2 > a.kmin_half ? r2 : 0.f;
+        }
+        const float2 xa1 = c_mul(mult_ct<CA>(ma, kxa, kyr, k1, ki1, o1), c1);
+        const float2 xa2 = c_mul(mult_ct<CA>(ma, kxb, kymr, k2, ki2, o2), c2);
+        float2 xb1 = make_float2(0.f, 0.f), xb2 = make_float2(0.f, 0.f);
+        if (has_b) {
+            xb1 = c_mul(mult_ct<CB>(mb, kxa, kyr, k1, ki1, o1), c1);
+            xb2 = c_mul(mult_ct<CB>(mb, kxb, kymr, k2, ki2, o2), c2);
+        }
+        // Z(p) = (XA(p) + conj XA(-p)) / 2 + i (XB(p) + conj XB(-p)) / 2
+        rowA[pad_idx(xa)] = make_float2(0.5f * (xa1.x + xa2.x) - 0.5f * (xb1.y - xb2.y),
+                                        0.5f * (xa1.y - xa2.y) + 0.5f * (xb1.x + xb2.x));
+        rowB[pad_idx(xb)] = make_float2(0.5f * (xa2.x + xa1.x) - 0.5f * (xb2.y - xb1.y),
+                                        0.5f * (xa2.y - xa1.y) + 0.5f * (xb2.x + xb1.x));
+    }
+}
+
+// One packed transform of the row pass: build, transform, store.
+template <int N, int CA, int CB>
+OCS_D void row_transform(const SurfaceArgs &a, int p, int nx, int ny, int r, int mr, float kyr, float kymr,
+                         const float2 *cA, const float2 *cB, const float *omA, const float *omB,
+                         float2 *rowA, float2 *rowB, const float2 *stw, int vstride) {
+    const int nq = nx / 2 + 1;
+    for (int x = threadIdx.x; x < nq; x += blockDim.x)
+        build_packed<CA, CB>(a, p, x, nx, kyr, kymr, cA, cB, omA, omB, rowA, rowB);
+    __syncthreads();
+    if constexpr (N > 0) {
+        // the last stage writes straight into the scratch plane
+        const RowStore st{a.scratch + (size_t)p * ny * nx, nx, r, mr};
+        ifft_pow2<N, 2, rows_threads<N>(), false, true>(rowA, vstride, stw, NoLoad(), st);
+    } else {
+        const float2 *res = ifft_generic(rowA, rowB + vstride, vstride, 2, a.px);
+        float2 *outA = a.scratch + ((size_t)p * ny + r) * nx;
+        float2 *outB = a.scratch + ((size_t)p * ny + mr) * nx;
+        for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+            outA[x] = res[pad_idx(x)];
+            if (mr != r) outB[x] = res[vstride + pad_idx(x)];
+        }
+    }
+    __syncthreads();
+}
+
 // Pass 1.  Shared memory: c(t) of rows r and mr ([2][nx], unpadded), then the two padded
-// FFT rows (and, for non-power-of-two lengths, two more for the ping-pong).  Mirror pairs:
-// (r,x) <-> (mr,mx) and (r,mx) <-> (mr,x).
-template <int N>
+// FFT rows (and, for non-power-of-two lengths, two more for the ping-pong).
+template <int N, int PROG>
 __global__ void __launch_bounds__(rows_threads<N>(), rows_threads<N>() <= 512 ? 2 : 1)
 surface_rows_kernel(const __grid_constant__ SurfaceArgs a) {
     extern __shared__ __align__(16) float2 sbuf[];
@@ -184,60 +280,21 @@ surface_rows_kernel(const __grid_constant__ SurfaceArgs a) {
     }
     __syncthreads();
 
-    const int nq = nx / 2 + 1;
-    for (int p = 0; p < a.npair; ++p) {
-        const MultDesc ca = a.mult[2 * p], cb = a.mult[2 * p + 1];
-        const bool has_b = a.code[2 * p + 1] >= 0;
-        for (int x = threadIdx.x; x < nq; x += blockDim.x) {
-            const int mx = (nx - x) % nx;
-            const float kxx = a.kx[x], kxm = a.kx[mx];
-            // mirror pairs: (r, x) <-> (mr, mx) and (r, mx) <-> (mr, x)
-#pragma unroll
-            for (int pr = 0; pr < 2; ++pr) {
-                const int xa = pr == 0 ? x : mx, xb = pr == 0 ? mx : x;   // columns of the pair
-                const float kxa = pr == 0 ? kxx : kxm, kxb = pr == 0 ? kxm : kxx;
-                const float2 c1 = cA[xa], c2 = cB[xb];
-                const float o1 = a.needs_omega ? omA[xa] : 0.f, o2 = a.needs_omega ? omB[xb] : 0.f;
-                // |k| and 1/|k| from one reciprocal square root (1/|k| is 0 where |k| does not
-                // exceed min(kx_res, ky_res)/2, ocean.py:142-148)
-                const float q1 = fadd(fmul(kxa, kxa), fmul(kyr, kyr));
-                const float q2 = fadd(fmul(kxb, kxb), fmul(kymr, kymr));
-                const float r1 = q1 > 0.f ? rsqrtf(q1) : 0.f, r2 = q2 > 0.f ? rsqrtf(q2) : 0.f;
-                const float k1 = q1 * r1, k2 = q2 * r2;
-                const float ki1 = k1 > a.kmin_half ? r1 : 0.f;
-                const float ki2 = k2 > a.kmin_half ? r2 : 0.f;
-                const float2 xa1 = c_mul(field_mult(ca, kxa, kyr, k1, ki1, o1), c1);
-                const float2 xa2 = c_mul(field_mult(ca, kxb, kymr, k2, ki2, o2), c2);
-                float2 xb1 = make_float2(0.f, 0.f), xb2 = make_float2(0.f, 0.f);
-                if (has_b) {
-                    xb1 = c_mul(field_mult(cb, kxa, kyr, k1, ki1, o1), c1);
-                    xb2 = c_mul(field_mult(cb, kxb, kymr, k2, ki2, o2), c2);
-                }
-                // Z(p) = (XA(p) + conj XA(-p)) / 2 + i (XB(p) + conj XB(-p)) / 2
-                const float2 z1 = make_float2(0.5f * (xa1.x + xa2.x) - 0.5f * (xb1.y - xb2.y),
-                                              0.5f * (xa1.y - xa2.y) + 0.5f * (xb1.x + xb2.x));
-                const float2 z2 = make_float2(0.5f * (xa2.x + xa1.x) - 0.5f * (xb2.y - xb1.y),
-                                              0.5f * (xa2.y - xa1.y) + 0.5f * (xb2.x + xb1.x));
-                rowA[pad_idx(xa)] = z1;
-                rowB[pad_idx(xb)] = z2;
-            }
-        }
-        __syncthreads();
-        if constexpr (N > 0) {
-            // the last stage writes straight into the scratch plane
-            const RowStore st{a.scratch + (size_t)p * ny * nx, nx, r, mr};
-            ifft_pow2<N, 2, rows_threads<N>(), false, true>(rowA, vstride, stw, NoLoad(), st);
-        } else {
-            const float2 *res = ifft_generic(rowA, rowB + vstride, vstride, 2, a.px);
-            float2 *outA = a.scratch + ((size_t)p * ny + r) * nx;
-            float2 *outB = a.scratch + ((size_t)p * ny + mr) * nx;
-            for (int x = threadIdx.x; x < nx; x += blockDim.x) {
-                outA[x] = res[pad_idx(x)];
-                if (mr != r) outB[x] = res[vstride + pad_idx(x)];
-            }
-        }
-        __syncthreads();
+#define OCS_ROW_T(P, CA, CB) \
+    row_transform<N, CA, CB>(a, P, nx, ny, r, mr, kyr, kymr, cA, cB, omA, omB, rowA, rowB, stw, vstride)
+    if constexpr (PROG == 1) {
+        OCS_ROW_T(0, OCS_FIELD_DX, OCS_FIELD_DY);
+        OCS_ROW_T(1, OCS_FIELD_DZ, OCS_FIELD_DIFFX);
+        OCS_ROW_T(2, OCS_FIELD_DIFFY, OCS_FIELD_DIFFXX);
+        OCS_ROW_T(3, OCS_FIELD_DIFFYY, OCS_FIELD_DIFFXY);
+    } else if constexpr (PROG == 2) {
+        OCS_ROW_T(0, OCS_FIELD_DX, OCS_FIELD_DY);
+        OCS_ROW_T(1, OCS_FIELD_DZ, OCS_FIELD_DIFFX);
+        OCS_ROW_T(2, OCS_FIELD_DIFFY, kNone);
+    } else {
+        for (int p = 0; p < a.npair; ++p) OCS_ROW_T(p, kRuntime, kRuntime);
     }
+#undef OCS_ROW_T
 }
 
 // Pass 2.  One CTA per (transform p, tile of TILE columns).  Power-of-two lengths read
@@ -366,16 +423,36 @@ static size_t ws_sty(int nx, int ny) { return ws_stx(nx, ny) + align256((size_t)
 static size_t ws_scratch(int nx, int ny) { return ws_sty(nx, ny) + align256((size_t)ny * sizeof(float2)); }
 static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 
-template <int N>
-static cudaError_t launch_rows_n(const SurfaceArgs &a, cudaStream_t st) {
+template <int N, int PROG>
+static cudaError_t launch_rows_prog(const SurfaceArgs &a, cudaStream_t st) {
     const int nx = a.nx;
     size_t smem = (N > 0) ? (3 * (size_t)nx + 2 * (size_t)pow2_vstride(nx, 2)) * sizeof(float2)
                           : (2 * (size_t)nx + 4 * (size_t)padded_len(nx)) * sizeof(float2);
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
-    cudaError_t e = ensure_smem((const void *)surface_rows_kernel<N>, smem);
+    cudaError_t e = ensure_smem((const void *)surface_rows_kernel<N, PROG>, smem);
     if (e != cudaSuccess) return e;
-    surface_rows_kernel<N><<<a.ny / 2 + 1, rows_threads<N>(), smem, st>>>(a);
+    surface_rows_kernel<N, PROG><<<a.ny / 2 + 1, rows_threads<N>(), smem, st>>>(a);
     return cudaGetLastError();
+}
+
+// Field program of a packed code list (see surface_rows_kernel).
+static int field_program(const SurfaceArgs &a) {
+    static const int std8[8] = {OCS_FIELD_DX, OCS_FIELD_DY, OCS_FIELD_DZ, OCS_FIELD_DIFFX,
+                                OCS_FIELD_DIFFY, OCS_FIELD_DIFFXX, OCS_FIELD_DIFFYY, OCS_FIELD_DIFFXY};
+    static const int std5[6] = {OCS_FIELD_DX, OCS_FIELD_DY, OCS_FIELD_DZ, OCS_FIELD_DIFFX, OCS_FIELD_DIFFY, -1};
+    bool is8 = a.npair == 4, is5 = a.npair == 3;
+    for (int i = 0; i < 8 && is8; ++i) is8 = a.code[i] == std8[i];
+    for (int i = 0; i < 6 && is5; ++i) is5 = a.code[i] == std5[i];
+    return is8 ? 1 : (is5 ? 2 : 0);
+}
+
+template <int N>
+static cudaError_t launch_rows_n(const SurfaceArgs &a, cudaStream_t st) {
+    switch (field_program(a)) {
+        case 1: return launch_rows_prog<N, 1>(a, st);
+        case 2: return launch_rows_prog<N, 2>(a, st);
+        default: return launch_rows_prog<N, 0>(a, st);
+    }
 }
 
 template <int N, int TILE>
