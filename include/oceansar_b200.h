@@ -112,6 +112,13 @@ int ocs_surface_prepare(int32_t nx, int32_t ny, void *workspace_d, void *stream)
 /* Synthesize the requested fields at time t (float32, as ocean.py:424 casts it). */
 int ocs_surface_update(const ocs_surface_desc *desc, float t, void *stream);
 
+/* One or both passes of ocs_surface_update: passes = 1 runs the row pass (phase evolution,
+ * spectral multipliers, row transforms into the workspace), 2 the column pass (column
+ * transforms, field store), 3 both (= ocs_surface_update).  Pass 2 reads what pass 1 of
+ * the same descriptor and t left in the workspace.  Lets a caller time or schedule the two
+ * kernels separately; same reference interface as ocs_surface_update. */
+int ocs_surface_update_passes(const ocs_surface_desc *desc, float t, int passes, void *stream);
+
 typedef struct {
     int64_t n;                                       /* ny*nx                               */
     const float *ax_d, *ay_d, *axx_d, *ayy_d;        /* Re ifft2 of i kx c, i ky c, -kx^2/k c, -ky^2/k c */

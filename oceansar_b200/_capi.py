@@ -36,6 +36,7 @@ SIGNATURES = {
     "ocs_surface_workspace_bytes": [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32],
     "ocs_surface_prepare": [ctypes.c_int32, ctypes.c_int32, c_ptr, c_ptr],
     "ocs_surface_update": [c_ptr, c_flt, c_ptr],
+    "ocs_surface_update_passes": [c_ptr, c_flt, c_int, c_ptr],
     "ocs_surface_choppy": [c_ptr, c_ptr],
     "ocs_surface_update_noalloc": [c_ptr, c_flt, c_ptr],
     "ocs_pulse": [c_ptr, c_int, c_ptr],

@@ -519,7 +519,8 @@ extern "C" int ocs_surface_prepare(int32_t nx, int32_t ny, void *workspace, void
     return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
 }
 
-extern "C" int ocs_surface_update(const ocs_surface_desc *d, float t, void *stream) {
+extern "C" int ocs_surface_update_passes(const ocs_surface_desc *d, float t, int passes, void *stream) {
+    if (passes < 1 || passes > 3) return OCS_ERR_ARG;
     if (!d || !d->coefs_d || !d->omega_d || !d->kx_d || !d->ky_d || !d->workspace_d) return OCS_ERR_ARG;
     const int nx = d->nx, ny = d->ny;
     if (nx < 2 || ny < 2 || d->nfields < 1 || d->nfields > 2 * kMaxPacked) return OCS_ERR_ARG;
@@ -562,11 +563,15 @@ extern "C" int ocs_surface_update(const ocs_surface_desc *d, float t, void *stre
     a.scratch = (float2 *)(ws + ws_scratch(nx, ny));
     cudaStream_t st = (cudaStream_t)stream;
 
-    cudaError_t e = launch_rows(a, st);
+    cudaError_t e = (passes & 1) ? launch_rows(a, st) : cudaSuccess;
     if (e != cudaSuccess) return e == cudaErrorInvalidValue ? OCS_ERR_SIZE : OCS_ERR_CUDA;
-    e = launch_cols(a, st);
+    e = (passes & 2) ? launch_cols(a, st) : cudaSuccess;
     if (e != cudaSuccess) return e == cudaErrorInvalidValue ? OCS_ERR_SIZE : OCS_ERR_CUDA;
     return OCS_OK;
+}
+
+extern "C" int ocs_surface_update(const ocs_surface_desc *d, float t, void *stream) {
+    return ocs_surface_update_passes(d, t, 3, stream);
 }
 
 extern "C" int ocs_surface_choppy(const ocs_choppy_desc *d, void *stream) {

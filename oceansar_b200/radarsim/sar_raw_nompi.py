@@ -299,22 +299,31 @@ class RawGenerator(object):
     def time_stages(self, steps):
         """Average device time [ms] of the surface update and of the pulse kernel(s) over
         ``steps`` pulses, from CUDA events on the launching stream."""
+        t = self.time_kernels(steps)
+        return t['surface_rows'] + t['surface_cols'], t['pulse'], None, None
+
+    def time_kernels(self, steps):
+        """Average device time [ms] per pulse of each kernel of the scene loop over ``steps``
+        pulses: 'surface_rows' (row pass), 'surface_cols' (column pass) and 'pulse' (the
+        per-pulse row table and the fused NRCS / scene / accumulation kernel(s)), each from
+        CUDA events recorded on the launching stream around that launch alone."""
         st = torch.cuda.current_stream()
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
-               torch.cuda.Event(enable_timing=True)) for _ in steps]
+        mk = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
+        ev = [[mk() for _ in range(4)] for _ in steps]
         saved_last = self.t_last_rcs_bragg
-        for (e0, e1, e2), a in zip(ev, steps):
+        for e, a in zip(ev, steps):
             t_now = a * self.t_step
-            e0.record(st)
-            self.surface.set_t(t_now)
-            e1.record(st)
+            e[0].record(st)
+            self.surface.set_t(t_now, passes=1)
+            e[1].record(st)
+            self.surface.set_t(t_now, passes=2)
+            e[2].record(st)
             self.pulse(a, update_surface=False)
-            e2.record(st)
+            e[3].record(st)
         torch.cuda.synchronize()
         self.t_last_rcs_bragg = saved_last
-        surf = [e0.elapsed_time(e1) for e0, e1, _ in ev]
-        puls = [e1.elapsed_time(e2) for _, e1, e2 in ev]
-        return float(np.mean(surf)), float(np.mean(puls)), surf, puls
+        names = ('surface_rows', 'surface_cols', 'pulse')
+        return {n: float(np.mean([e[i].elapsed_time(e[i + 1]) for e in ev])) for i, n in enumerate(names)}
 
     # ------------------------------------------------------------------------------------
     def nrcs_avg(self):

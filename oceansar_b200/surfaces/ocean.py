@@ -349,8 +349,11 @@ class OceanSurface(object):
     def t(self, value):
         self.set_t(value)
 
-    def set_t(self, value, stream=None):
-        """Propagate to time ``value`` and synthesise every requested field on the GPU."""
+    def set_t(self, value, stream=None, passes=3):
+        """Propagate to time ``value`` and synthesise every requested field on the GPU.
+
+        ``passes`` selects the row pass (1), the column pass (2) or both (3, the default);
+        the column pass consumes what the row pass of the same time left in the workspace."""
         if not self.initialized:
             raise Exception('Surface not initialized')
         self._t = np.float32(value)
@@ -377,8 +380,12 @@ class OceanSurface(object):
                            self._swell_d.data_ptr() if self._swell_d is not None else None,
                            float(np.real(rot)), float(np.imag(rot)), self._ws.data_ptr())
         sp = _device.stream_ptr(stream)
-        _capi.call("ocs_surface_update", ctypes.addressof(desc), ctypes.c_float(float(self._t)), sp)
-        if self._aux:
+        if passes == 3:
+            _capi.call("ocs_surface_update", ctypes.addressof(desc), ctypes.c_float(float(self._t)), sp)
+        else:
+            _capi.call("ocs_surface_update_passes", ctypes.addressof(desc), ctypes.c_float(float(self._t)),
+                       int(passes), sp)
+        if self._aux and passes & 2:
             self._choppy(rot, sp)
 
     def _choppy(self, rot, sp):
