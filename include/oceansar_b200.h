@@ -247,6 +247,48 @@ typedef struct {
 
 int ocs_field_kodis(const ocs_kodis_desc *desc, void *stream);
 
+/* ---- Scene batch ----------------------------------------------------------------------
+ * Many independent scenes (any mix of grid sizes, geometries and channel counts) advanced
+ * together, one pulse of every scene per step, by persistent kernels that find their work
+ * in a device-resident slot table.  Each step is a fixed launch sequence needing no host
+ * arguments, so it can be recorded once into a CUDA graph and replayed while scenes enter
+ * and leave the slots (as long as the set of grid sizes and output widths in use stays
+ * the same).  No counterpart in the reference: its sar_raw
+ * (oceansar/radarsim/sar_raw_nompi.py:32-641) runs the same per-pulse body for one scene
+ * per call; a slot runs exactly that body (ocs_surface_update + ocs_pulse) at each pulse. */
+typedef struct {
+    const ocs_surface_desc *surface;   /* as for ocs_surface_update; t, add and swell_rot are
+                                          taken per pulse from the tables below           */
+    const ocs_pulse_desc *pulse;       /* as for ocs_pulse (az_step = 0); az_step, az_now,
+                                          tind and refresh are taken from the tables below */
+    int32_t tile_rows;                 /* facet rows per pulse-kernel tile, 1..128 (0: 64) */
+    const float *t_d;                  /* [az_steps] float32 surface time of each pulse     */
+    const float *add_d;                /* [az_steps][surface->nfields] additive terms       */
+    const float *swell_rot_d;          /* [az_steps][2] exp(-i w_s t), or NULL              */
+    const double *az_now_d;            /* [az_steps] platform azimuth position              */
+    const int32_t *flags_d;            /* [az_steps] 1: synthesise the surface, 2: refresh
+                                          the Bragg RCS at this pulse                       */
+    const int32_t *tmod_d;             /* [az_steps][2] int(t prf) mod N_m, mod N_p         */
+} ocs_scene_desc;
+
+typedef struct ocs_batch ocs_batch;    /* opaque engine handle                              */
+
+/* Engine with max_slots (1..256) scene slots for one precision (OCS_PREC_*). */
+int ocs_batch_create(int32_t max_slots, int32_t precision, ocs_batch **out);
+int ocs_batch_destroy(ocs_batch *batch);
+/* Put a scene in a slot with its pulse counter at 0 (the caller zeroes its raw cube and
+ * NRCS accumulators).  Synchronous with respect to the stream. */
+int ocs_batch_set(ocs_batch *batch, int32_t slot, const ocs_scene_desc *scene, void *stream);
+/* Take the scene out of a slot.  Synchronous with respect to the stream. */
+int ocs_batch_clear(ocs_batch *batch, int32_t slot, void *stream);
+/* Enqueue `pulses` steps: every slot whose counter is below its az_steps runs one pulse per
+ * step; finished and empty slots cost nothing. */
+int ocs_batch_step(ocs_batch *batch, int32_t pulses, void *stream);
+/* Kernel launches one step enqueues for the slots in use. */
+int ocs_batch_launches_per_step(const ocs_batch *batch);
+/* Pulse counter of every slot (-1 for empty slots) into out[max_slots]; synchronous. */
+int ocs_batch_counters(const ocs_batch *batch, int32_t *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

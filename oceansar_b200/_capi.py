@@ -43,6 +43,13 @@ SIGNATURES = {
     "ocs_pulse_workspace_bytes": [ctypes.c_int32, ctypes.c_int32],
     "ocs_rcs_romeiser": [c_ptr, c_ptr],
     "ocs_field_kodis": [c_ptr, c_ptr],
+    "ocs_batch_create": [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(c_ptr)],
+    "ocs_batch_destroy": [c_ptr],
+    "ocs_batch_set": [c_ptr, ctypes.c_int32, c_ptr, c_ptr],
+    "ocs_batch_clear": [c_ptr, ctypes.c_int32, c_ptr],
+    "ocs_batch_step": [c_ptr, ctypes.c_int32, c_ptr],
+    "ocs_batch_launches_per_step": [c_ptr],
+    "ocs_batch_counters": [c_ptr, c_ptr, c_ptr],
 }
 _RESTYPE = {"ocs_version": ctypes.c_char_p, "ocs_surface_workspace_bytes": ctypes.c_int64,
             "ocs_pulse_workspace_bytes": ctypes.c_int64}

@@ -56,3 +56,10 @@ class KodisDesc(ctypes.Structure):
                 ("diffx_d", P), ("diffy_d", P), ("diffxx_d", P), ("diffyy_d", P), ("diffxy_d", P),
                 ("k0", F64), ("R_re", F64), ("R_im", F64), ("dx", F64), ("dy", F64),
                 ("out_d", P)]
+
+
+class SceneDesc(ctypes.Structure):
+    """``ocs_scene_desc``: one scene of the scene batch."""
+    _fields_ = [("surface", ctypes.c_void_p), ("pulse", ctypes.c_void_p), ("tile_rows", ctypes.c_int32),
+                ("t_d", ctypes.c_void_p), ("add_d", ctypes.c_void_p), ("swell_rot_d", ctypes.c_void_p),
+                ("az_now_d", ctypes.c_void_p), ("flags_d", ctypes.c_void_p), ("tmod_d", ctypes.c_void_p)]

@@ -22,12 +22,14 @@
 #include <string.h>
 
 #include "accum.cuh"
+#include "batch.cuh"
 #include "physics.cuh"
 
 namespace ocs {
 
 constexpr int kPulseCols = 128;     // columns (threads) per CTA
-constexpr int kPulseRows = 64;      // rows per tile
+constexpr int kPulseRows = 64;      // rows per tile (single-scene launches)
+constexpr int kPulseRowsMax = 128;  // largest rows per tile (shared row tables)
 constexpr int kMaxCh = 8;
 constexpr int kPulseNbw = 160;      // CTA shared bin window
 
@@ -113,64 +115,80 @@ OCS_D void block_atomic_sum(double v, double *dst, double *sred) {
 // rowtab[q*ny + y] holds az, sin_az = az/sr0, the ground-projected azimuth angle and its
 // cos / sin (q = 0..4), then rowtab[5*ny + 2*(y*nch + c)] the complex antenna-pattern x
 // ATI-phase factor of channel c.  float64, computed once per pulse for all tiles.
-__global__ void pulse_rows_kernel(const __grid_constant__ PulseArgs a) {
-    for (int y = blockIdx.x * blockDim.x + threadIdx.x; y < a.ny; y += gridDim.x * blockDim.x) {
-        const double az = dsub((double)a.y[y], a.az_now);
-        const double sin_az = ddiv(az, a.sr0);
-        const double azp = asin(az / a.gr0);
-        a.rowtab[y] = az;
-        a.rowtab[(long long)a.ny + y] = sin_az;
-        a.rowtab[2LL * a.ny + y] = azp;
-        a.rowtab[3LL * a.ny + y] = cos(azp);
-        a.rowtab[4LL * a.ny + y] = sin(azp);
-        const double bp = np_sinc(a.ltx_over_l * sin_az) * np_sinc(a.lrx_over_l * sin_az);
-        double *fac = a.rowtab + 5LL * a.ny + 2LL * y * a.nch;
-        for (int c = 0; c < a.nch; ++c) {
-            const c128 ati = cexpi((-a.k0 * a.b_ati[c]) * sin_az);
-            fac[2 * c] = bp * ati.re;
-            fac[2 * c + 1] = bp * ati.im;
-        }
+OCS_D void pulse_row(const PulseArgs &a, double az_now, int y) {
+    const double az = dsub((double)a.y[y], az_now);
+    const double sin_az = ddiv(az, a.sr0);
+    const double azp = asin(az / a.gr0);
+    a.rowtab[y] = az;
+    a.rowtab[(long long)a.ny + y] = sin_az;
+    a.rowtab[2LL * a.ny + y] = azp;
+    a.rowtab[3LL * a.ny + y] = cos(azp);
+    a.rowtab[4LL * a.ny + y] = sin(azp);
+    const double bp = np_sinc(a.ltx_over_l * sin_az) * np_sinc(a.lrx_over_l * sin_az);
+    double *fac = a.rowtab + 5LL * a.ny + 2LL * y * a.nch;
+    for (int c = 0; c < a.nch; ++c) {
+        const c128 ati = cexpi((-a.k0 * a.b_ati[c]) * sin_az);
+        fac[2 * c] = bp * ati.re;
+        fac[2 * c + 1] = bp * ati.im;
     }
 }
 
-template <typename T, int NOUT, int S>
-__global__ void __launch_bounds__(kPulseCols, (sizeof(T) == 4 && NOUT < 4) ? 4 : 2)
-pulse_kernel(const __grid_constant__ PulseArgs a) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    constexpr int wlen = wtab_len<T, S>(kSincTaps, kSincOvs);
-    T *wtab = reinterpret_cast<T *>(smem);
-    T *bins = wtab + wlen;                                            // [NOUT][nbw][2]
-    double *r_az = reinterpret_cast<double *>(bins + NOUT * kPulseNbw * 2);
-    double *r_sinaz = r_az + kPulseRows;
-    double *r_azp = r_sinaz + kPulseRows;
-    double *r_cazp = r_azp + kPulseRows;
-    double *r_sazp = r_cazp + kPulseRows;
-    cplx<T> *r_fac = reinterpret_cast<cplx<T> *>(r_sazp + kPulseRows);   // [rows][nch]
-    double *sred = reinterpret_cast<double *>(r_fac + kPulseRows * a.nch);
+__global__ void pulse_rows_kernel(const __grid_constant__ PulseArgs a) {
+    for (int y = blockIdx.x * blockDim.x + threadIdx.x; y < a.ny; y += gridDim.x * blockDim.x)
+        pulse_row(a, a.az_now, y);
+}
 
-    build_wtab<T, S>(wtab, a.sinc, kSincTaps, kSincOvs);
+// Shared memory of the pulse kernel: pre-shifted weight table, CTA bin window, the tile's
+// rows of the per-pulse row table ([5][kPulseRowsMax] float64 + [rows][nch] complex), and
+// the block-reduction scratch.
+template <typename T> struct PulseSmem {
+    T *wtab, *bins;
+    double *r_az;
+    cplx<T> *r_fac;
+    double *sred;
+};
+
+template <typename T, int NOUT, int S>
+OCS_HD constexpr size_t pulse_smem_bytes(int nch) {
+    return (size_t)wtab_len<T, S>(kSincTaps, kSincOvs) * sizeof(T) + (size_t)NOUT * kPulseNbw * 2 * sizeof(T) +
+           5 * kPulseRowsMax * sizeof(double) + (size_t)kPulseRowsMax * nch * sizeof(cplx<T>) + 32 * sizeof(double);
+}
+
+template <typename T, int NOUT, int S>
+OCS_D PulseSmem<T> pulse_smem(unsigned char *smem, int nch) {
+    PulseSmem<T> sm;
+    sm.wtab = reinterpret_cast<T *>(smem);
+    sm.bins = sm.wtab + wtab_len<T, S>(kSincTaps, kSincOvs);             // [NOUT][nbw][2]
+    sm.r_az = reinterpret_cast<double *>(sm.bins + NOUT * kPulseNbw * 2);
+    sm.r_fac = reinterpret_cast<cplx<T> *>(sm.r_az + 5 * kPulseRowsMax);   // [rows][nch]
+    sm.sred = reinterpret_cast<double *>(sm.r_fac + kPulseRowsMax * nch);
+    return sm;
+}
+
+// One tile of kPulseCols columns x tile_rows rows: NRCS, scene and accumulation of every
+// facet into this pulse's raw rows; the tile's NRCS sums are added to spec_sum and
+// bragg_sum.
+template <typename T, int NOUT, int S>
+OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSmem<T> &sm, double &spec_sum,
+                      double (&bragg_sum)[2]) {
     const int tiles_x = (a.nx + kPulseCols - 1) / kPulseCols;
-    const int tiles = tiles_x * ((a.ny + kPulseRows - 1) / kPulseRows);
-    double spec_sum = 0.0, bragg_sum[2] = {0.0, 0.0};
-    // persistent CTAs: each walks tiles of kPulseCols columns x kPulseRows rows
-    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
     const int x = (tile % tiles_x) * kPulseCols + threadIdx.x;
-    const int y0 = (tile / tiles_x) * kPulseRows;
-    const int nrows = min(kPulseRows, a.ny - y0);
+    const int y0 = (tile / tiles_x) * tile_rows;
+    const int nrows = min(tile_rows, a.ny - y0);
     __syncthreads();                    // previous tile's bins and row tables are consumed
     // this tile's rows of the per-pulse row table (pulse_rows_kernel)
     for (int i = threadIdx.x; i < nrows * 5; i += blockDim.x) {
         const int q = i / nrows, k = i - q * nrows;
-        r_az[q * kPulseRows + k] = a.rowtab[(long long)q * a.ny + y0 + k];
+        sm.r_az[q * kPulseRowsMax + k] = a.rowtab[(long long)q * a.ny + y0 + k];
     }
     {
         const double *fac = a.rowtab + 5LL * a.ny + 2LL * y0 * a.nch;
         for (int i = threadIdx.x; i < nrows * a.nch; i += blockDim.x)
-            r_fac[i] = {(T)fac[2 * i], (T)fac[2 * i + 1]};
+            sm.r_fac[i] = {(T)fac[2 * i], (T)fac[2 * i + 1]};
     }
 
     CtaBins<T, NOUT> cb;
-    cb.acc = bins;
+    cb.acc = sm.bins;
     cb.nbw = kPulseNbw;
     cb.nout = a.nout;
     cb.nbins = a.nbins;
@@ -205,7 +223,7 @@ pulse_kernel(const __grid_constant__ PulseArgs a) {
         for (int i = 0; i < nrows; ++i) {
             const long long idx = (long long)(y0 + i) * a.nx + x;
             if (i + 1 < nrows) nxt.load(a, idx + a.nx, npix, scat, load_scat);
-            const double az = r_az[i], sin_az = r_sinaz[i];
+            const double az = sm.r_az[i], sin_az = sm.r_az[kPulseRowsMax + i];
             // slant range: sr - cos_inc*Dz + az/2*sin_az + Dx*sin_inc + Dy*sin_az, float64,
             // left to right, no fused multiply-adds (bit-identical with numpy)
             double srs = dsub(sr_c, dmul(cos_i, (double)cur.dz));
@@ -218,7 +236,7 @@ pulse_kernel(const __grid_constant__ PulseArgs a) {
 
             cplx<T> scene[2] = {{(T)0, (T)0}, {(T)0, (T)0}};      // per polarisation
             if (a.do_kodis) {
-                const cplx<T> e = kodis_facet<T>(a.kodis, srs, sin_i, cos_i, tan_i, r_cazp[i], r_sazp[i],
+                const cplx<T> e = kodis_facet<T>(a.kodis, srs, sin_i, cos_i, tan_i, sm.r_az[3 * kPulseRowsMax + i], sm.r_az[4 * kPulseRowsMax + i],
                                                  cur.diffx, cur.diffy, cur.diffxx, cur.diffyy, cur.diffxy);
                 const T s4 = (T)3.5449077018110318;                 // sqrt(4 pi)
                 const cplx<T> es = {e.re * s4, e.im * s4};
@@ -230,7 +248,7 @@ pulse_kernel(const __grid_constant__ PulseArgs a) {
                 T sc[2][2];                                            // [pol][line]
                 if (a.refresh) {
                     T hh[2], vv[2];
-                    romeiser_facet<T>(a.rom, (T)inc_c, (T)r_azp[i], (T)r_cazp[i], (T)r_sazp[i],
+                    romeiser_facet<T>(a.rom, (T)inc_c, (T)sm.r_az[2 * kPulseRowsMax + i], (T)sm.r_az[3 * kPulseRowsMax + i], (T)sm.r_az[4 * kPulseRowsMax + i],
                                       (T)cur.diffx, (T)cur.diffy, hh, vv);
                     if (a.use_hmtf) {
                         float hm = a.hmtf[idx];
@@ -246,8 +264,10 @@ pulse_kernel(const __grid_constant__ PulseArgs a) {
                             bragg_sum[p] += (double)r0 + (double)r1;
                             sc[p][0] = tsqrt(r0);
                             sc[p][1] = tsqrt(r1);
-                            scat[(2 * p) * npix + idx] = sc[p][0];
-                            scat[(2 * p + 1) * npix + idx] = sc[p][1];
+                            if (a.out0 == 0) {          // one output group stores the RCS
+                                scat[(2 * p) * npix + idx] = sc[p][0];
+                                scat[(2 * p + 1) * npix + idx] = sc[p][1];
+                            }
                         }
                     }
                 } else {
@@ -294,7 +314,7 @@ pulse_kernel(const __grid_constant__ PulseArgs a) {
                 if (k < a.nout) {
                     const int o = a.out0 + k;
                     const int p = o / a.nch, c = o - p * a.nch;
-                    cplx<T> v = cmul(p == 0 ? scene[0] : scene[1], r_fac[i * a.nch + c]);
+                    cplx<T> v = cmul(p == 0 ? scene[0] : scene[1], sm.r_fac[i * a.nch + c]);
                     if (a.b_xti[c] != 0.0) {
                         const double ph = (-a.k0 * a.b_xti[c]) * (dinc0 + wave_dinc);
                         v = cmul(v, cexp_phase<T>(ph));
@@ -305,29 +325,128 @@ pulse_kernel(const __grid_constant__ PulseArgs a) {
                 }
             }
             if (bin_d > -(1 << 29))
-                win.add(bin_d - kSincTaps / 2, lut, coef, wtab, a.sinc, kSincTaps, kSincOvs, cb);
+                win.add(bin_d - kSincTaps / 2, lut, coef, sm.wtab, a.sinc, kSincTaps, kSincOvs, cb);
             cur = nxt;
         }
     }
     win.flush(cb);
     __syncthreads();
     cb.flush_to_global();
-    }
-    // NRCS bookkeeping (only the first output group accumulates it)
+}
+
+// NRCS bookkeeping of a CTA (only the first output group accumulates it).
+template <typename T>
+OCS_D void pulse_nrcs(const PulseArgs &a, const PulseSmem<T> &sm, double spec_sum, const double (&bragg_sum)[2]) {
     if (a.out0 == 0) {
-        if (a.do_kodis) block_atomic_sum(spec_sum, &a.nrcs_spec[a.az_step], sred);
+        if (a.do_kodis) block_atomic_sum(spec_sum, &a.nrcs_spec[a.az_step], sm.sred);
         if (a.do_bragg && a.refresh)
             for (int p = 0; p < a.npol; ++p)
-                block_atomic_sum(bragg_sum[p], &a.nrcs_bragg[(long long)p * a.az_steps + a.az_step], sred);
+                block_atomic_sum(bragg_sum[p], &a.nrcs_bragg[(long long)p * a.az_steps + a.az_step], sm.sred);
     }
 }
 
 template <typename T, int NOUT, int S>
+__global__ void __launch_bounds__(kPulseCols, (sizeof(T) == 4 && NOUT < 4) ? 4 : 2)
+pulse_kernel(const __grid_constant__ PulseArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const PulseSmem<T> sm = pulse_smem<T, NOUT, S>(smem, a.nch);
+    build_wtab<T, S>(sm.wtab, a.sinc, kSincTaps, kSincOvs);
+    const int tiles = ((a.nx + kPulseCols - 1) / kPulseCols) * ((a.ny + kPulseRows - 1) / kPulseRows);
+    double spec_sum = 0.0, bragg_sum[2] = {0.0, 0.0};
+    // persistent CTAs: each walks tiles of kPulseCols columns x kPulseRows rows
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x)
+        pulse_tile<T, NOUT, S>(a, tile, kPulseRows, sm, spec_sum, bragg_sum);
+    pulse_nrcs<T>(a, sm, spec_sum, bragg_sum);
+}
+
+// ---------------------------------------------------------------------------------------
+// Scene batch (batch.cuh).  Output groups: a slot's npol*nch outputs are taken G at a time
+// (G = 4 in the mixed form, 2 in FP64); a group of w outputs runs in the kernel of width
+// class 1 (w = 1), 2 (w = 2) or 4 (w = 3, 4).  On refresh pulses every group evaluates the
+// Romeiser model and only the first group stores sqrt(RCS), so groups need no ordering.
+OCS_HD constexpr int width_class(int w) { return w <= 1 ? 1 : (w == 2 ? 2 : 4); }
+
+// Number of groups of width class K among nout outputs; out0 / width of the j-th one.
+OCS_D int groups_of_class(int nout, int G, int K, int j, int &out0, int &width) {
+    int n = 0;
+    for (int o = 0; o < nout; o += G) {
+        const int w = nout - o < G ? nout - o : G;
+        if (width_class(w) == K) {
+            if (n == j) { out0 = o; width = w; }
+            ++n;
+        }
+    }
+    return n;
+}
+
+OCS_D int slot_pulse_tiles(const SlotState &g) {
+    return ((g.nx + kPulseCols - 1) / kPulseCols) * ((g.ny + g.tile_rows - 1) / g.tile_rows);
+}
+
+__global__ void batch_pulse_rows_kernel(const __grid_constant__ BatchRef b) {
+    __shared__ int pref[kMaxSlots + 1];
+    const int total = scan_slots(b, pref, [](const SlotState &g) {
+        return slot_live(g) ? (g.ny + (int)blockDim.x - 1) / (int)blockDim.x : 0;
+    });
+    for (int item = blockIdx.x; item < total; item += gridDim.x) {
+        const int s = find_slot(pref, b.nslots, item);
+        const SlotState &g = b.slots[s];
+        const PulseArgs &a = *static_cast<const PulseArgs *>(g.pargs);
+        const int y = (item - pref[s]) * blockDim.x + threadIdx.x;
+        if (y < a.ny) pulse_row(a, g.aznow_tab[g.counter], y);
+    }
+}
+
+// One launch covers every live slot's groups of width class NOUT; the host sizes the grid
+// for all slots in use and each CTA takes one (slot, group, tile) item.
+template <typename T, int NOUT, int S>
+__global__ void __launch_bounds__(kPulseCols, (sizeof(T) == 4 && NOUT < 4) ? 4 : 2)
+batch_pulse_kernel(const __grid_constant__ BatchRef b) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ PulseArgs pa;
+    __shared__ int pref[kMaxSlots + 1];
+    constexpr int G = sizeof(T) == 4 ? 4 : 2;
+    const int total = scan_slots(b, pref, [](const SlotState &g) {
+        int o, w;
+        return slot_live(g) ? groups_of_class(g.nout, G, NOUT, -1, o, w) * slot_pulse_tiles(g) : 0;
+    });
+    const int item = blockIdx.x;
+    if (item >= total) return;
+    const int s = find_slot(pref, b.nslots, item);
+    const SlotState &g = b.slots[s];
+    const int tiles = slot_pulse_tiles(g);
+    const int j = item - pref[s];
+    const int grp = j / tiles, tile = j - grp * tiles;
+    {
+        const int *src = static_cast<const int *>(g.pargs);
+        int *dst = reinterpret_cast<int *>(&pa);
+        for (int i = threadIdx.x; i < (int)(sizeof(PulseArgs) / 4); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int c = g.counter;
+        int o = 0, w = 0;
+        groups_of_class(g.nout, G, NOUT, grp, o, w);
+        pa.out0 = o;
+        pa.nout = w;
+        pa.az_step = c;
+        pa.az_now = g.aznow_tab[c];
+        pa.refresh = (g.flags_tab[c] & kFlagRefresh) ? 1 : 0;
+        pa.tmod_m = g.tmod_tab[2 * c];
+        pa.tmod_p = g.tmod_tab[2 * c + 1];
+        pa.raw_row = (long long)c * pa.nbins;
+    }
+    __syncthreads();
+    const PulseSmem<T> sm = pulse_smem<T, NOUT, S>(smem, kMaxCh);
+    build_wtab<T, S>(sm.wtab, pa.sinc, kSincTaps, kSincOvs);
+    double spec_sum = 0.0, bragg_sum[2] = {0.0, 0.0};
+    pulse_tile<T, NOUT, S>(pa, tile, g.tile_rows, sm, spec_sum, bragg_sum);
+    pulse_nrcs<T>(pa, sm, spec_sum, bragg_sum);
+}
+
+template <typename T, int NOUT, int S>
 static int launch_pulse(const PulseArgs &a, cudaStream_t st) {
-    constexpr int wlen = wtab_len<T, S>(kSincTaps, kSincOvs);
-    size_t smem = (size_t)wlen * sizeof(T) + (size_t)NOUT * kPulseNbw * 2 * sizeof(T) +
-                  5 * kPulseRows * sizeof(double) + (size_t)kPulseRows * a.nch * sizeof(cplx<T>) +
-                  32 * sizeof(double);
+    const size_t smem = pulse_smem_bytes<T, NOUT, S>(a.nch);
     auto k = pulse_kernel<T, NOUT, S>;
     if (ensure_smem((const void *)k, smem) != cudaSuccess)
         return OCS_ERR_CUDA;
@@ -407,6 +526,60 @@ static int fill_pulse_args(const ocs_pulse_desc *d, PulseArgs &a) {
     a.nrcs_spec = d->nrcs_spec_d; a.nrcs_bragg = d->nrcs_bragg_d; a.az_steps = d->az_steps;
     return OCS_OK;
 }
+
+namespace ocs {
+
+size_t pulse_args_bytes() { return sizeof(PulseArgs); }
+
+int pulse_args_fill(const ocs_pulse_desc *d, void *out) {
+    PulseArgs a;
+    const int st = fill_pulse_args(d, a);
+    if (st == OCS_OK) memcpy(out, &a, sizeof(a));
+    return st;
+}
+
+int batch_launch_pulse_rows(const BatchRef &b, cudaStream_t st) {
+    int sms = 0, dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return OCS_ERR_CUDA;
+    batch_pulse_rows_kernel<<<sms * 4, 128, 0, st>>>(b);
+    return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
+}
+
+template <typename T, int NOUT, int S>
+static int batch_pulse_n(const BatchRef &b, int grid, cudaStream_t st) {
+    const size_t smem = pulse_smem_bytes<T, NOUT, S>(kMaxCh);
+    auto k = batch_pulse_kernel<T, NOUT, S>;
+    if (ensure_smem((const void *)k, smem) != cudaSuccess) return OCS_ERR_CUDA;
+    k<<<grid, kPulseCols, smem, st>>>(b);
+    return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
+}
+
+int batch_pulse_items(int nx, int ny, int tile_rows, int nout, int precision, int width) {
+    const int G = precision == OCS_PREC_F64 ? 2 : 4;
+    int groups = 0;
+    for (int o = 0; o < nout; o += G) groups += width_class(nout - o < G ? nout - o : G) == width;
+    return groups * ((nx + kPulseCols - 1) / kPulseCols) * ((ny + tile_rows - 1) / tile_rows);
+}
+
+int batch_launch_pulse(const BatchRef &b, int precision, int width, int grid, cudaStream_t st) {
+    if (grid < 1) return OCS_OK;
+    if (precision == OCS_PREC_F64) {
+        if (width == 1) return batch_pulse_n<double, 1, 12>(b, grid, st);
+        if (width == 2) return batch_pulse_n<double, 2, 12>(b, grid, st);
+        return OCS_ERR_ARG;
+    }
+    if (precision == OCS_PREC_MIXED) {
+        if (width == 1) return batch_pulse_n<float, 1, 12>(b, grid, st);
+        if (width == 2) return batch_pulse_n<float, 2, 12>(b, grid, st);
+        if (width == 4) return batch_pulse_n<float, 4, 12>(b, grid, st);
+        return OCS_ERR_ARG;
+    }
+    return OCS_ERR_ARG;
+}
+
+}  // namespace ocs
 
 extern "C" int64_t ocs_pulse_workspace_bytes(int32_t ny, int32_t nch) {
     if (ny < 1 || nch < 1 || nch > kMaxCh) return -1;

@@ -18,6 +18,7 @@
 #include <math.h>
 #include <string.h>
 
+#include "batch.cuh"
 #include "fft.cuh"
 
 namespace ocs {
@@ -38,6 +39,7 @@ struct SurfaceArgs {
     float t;
     float inv_n;
     int npair;
+    int prog;                         // field program of the row pass (surface_rows_kernel)
     int needs_omega;                  // some field's multiplier involves omega
     int code[2 * kMaxPacked];
     MultDesc mult[2 * kMaxPacked];
@@ -255,21 +257,20 @@ OCS_D void row_transform(const SurfaceArgs &a, int p, int nx, int ny, int r, int
     __syncthreads();
 }
 
-// Pass 1.  Shared memory: c(t) of rows r and mr ([2][nx], unpadded), then the two padded
-// FFT rows (and, for non-power-of-two lengths, two more for the ping-pong).
+// Pass 1, one item = the mirror row pair (r, ny - r).  Shared memory: c(t) of rows r and
+// mr ([2][nx], unpadded), then the two padded FFT rows (and, for non-power-of-two lengths,
+// two more for the ping-pong), then (power-of-two lengths) the stage-major twiddles, which
+// are only (re)loaded when load_tw is set.
 template <int N, int PROG>
-__global__ void __launch_bounds__(rows_threads<N>(), rows_threads<N>() <= 512 ? 2 : 1)
-surface_rows_kernel(const __grid_constant__ SurfaceArgs a) {
-    extern __shared__ __align__(16) float2 sbuf[];
+OCS_D void rows_item(const SurfaceArgs &a, int r, float2 *sbuf, bool load_tw) {
     const int nx = (N > 0) ? N : a.nx;
     const int ny = a.ny;
-    const int r = blockIdx.x;
     const int mr = (ny - r) % ny;
     const int vstride = (N > 0) ? pow2_vstride(nx, 2) : padded_len(nx);
     float2 *cA = sbuf, *cB = sbuf + nx;
     float2 *rowA = sbuf + 2 * nx, *rowB = rowA + vstride;
     float2 *stw = rowB + vstride;                 // power-of-two lengths: twiddles in smem
-    if (N > 0)
+    if (N > 0 && load_tw)
         for (int i = threadIdx.x; i < nx; i += blockDim.x) stw[i] = a.stw_x[i];
     const float kyr = a.ky[r], kymr = a.ky[mr];
     const float *omA = a.omega + (size_t)r * nx, *omB = a.omega + (size_t)mr * nx;
@@ -297,23 +298,27 @@ surface_rows_kernel(const __grid_constant__ SurfaceArgs a) {
 #undef OCS_ROW_T
 }
 
-// Pass 2.  One CTA per (transform p, tile of TILE columns).  Power-of-two lengths read
-// the tile inside the first FFT stage and unpack the fields inside the last one.
-template <int N, int TILE>
-__global__ void __launch_bounds__(cols_threads<N, TILE>(), cols_threads<N, TILE>() <= 512 ? 2 : 1)
-surface_cols_kernel(const __grid_constant__ SurfaceArgs a) {
+template <int N, int PROG>
+__global__ void __launch_bounds__(rows_threads<N>(), rows_threads<N>() <= 512 ? 2 : 1)
+surface_rows_kernel(const __grid_constant__ SurfaceArgs a) {
     extern __shared__ __align__(16) float2 sbuf[];
+    rows_item<N, PROG>(a, blockIdx.x, sbuf, true);
+}
+
+// Pass 2, one item = (transform p, tile of TILE columns starting at x0).  Power-of-two
+// lengths read the tile inside the first FFT stage and unpack the fields inside the last.
+template <int N, int TILE>
+OCS_D void cols_item(const SurfaceArgs &a, int p, int x0, float2 *sbuf, bool load_tw) {
     const int nx = a.nx;
     const int ny = (N > 0) ? N : a.ny;
-    const int p = blockIdx.y;
-    const int x0 = blockIdx.x * TILE;
     const int vstride = (N > 0) ? pow2_vstride(ny, TILE) : padded_len(ny);
     const float2 *src = a.scratch + (size_t)p * ny * nx;
     const ColStore st{a.dst[2 * p], a.dst[2 * p + 1], a.swell_exp, a.swell_rot, a.swm[2 * p],
                       a.swm[2 * p + 1], a.inv_n, a.add[2 * p], a.add[2 * p + 1], nx, x0};
     if constexpr (N > 0) {
         float2 *stw = sbuf + TILE * vstride;      // twiddles in smem (first used in stage 2)
-        for (int i = threadIdx.x; i < ny; i += blockDim.x) stw[i] = a.stw_y[i];
+        if (load_tw)
+            for (int i = threadIdx.x; i < ny; i += blockDim.x) stw[i] = a.stw_y[i];
         ifft_pow2<N, TILE, cols_threads<N, TILE>(), true, true>(sbuf, vstride, stw, ColLoad{src, nx, x0}, st);
     } else {
         for (int i = threadIdx.x; i < ny * TILE; i += blockDim.x) {
@@ -328,6 +333,13 @@ surface_cols_kernel(const __grid_constant__ SurfaceArgs a) {
             st(w, y, res[w * vstride + pad_idx(y)]);
         }
     }
+}
+
+template <int N, int TILE>
+__global__ void __launch_bounds__(cols_threads<N, TILE>(), cols_threads<N, TILE>() <= 512 ? 2 : 1)
+surface_cols_kernel(const __grid_constant__ SurfaceArgs a) {
+    extern __shared__ __align__(16) float2 sbuf[];
+    cols_item<N, TILE>(a, blockIdx.y, blockIdx.x * TILE, sbuf, true);
 }
 
 // Choppy-wave slopes and curvatures from the auxiliary fields (ocean.py:451-456, 468-482).
@@ -423,12 +435,22 @@ static size_t ws_sty(int nx, int ny) { return ws_stx(nx, ny) + align256((size_t)
 static size_t ws_scratch(int nx, int ny) { return ws_sty(nx, ny) + align256((size_t)ny * sizeof(float2)); }
 static bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 
+// Dynamic shared memory of a row item / column item.
+static size_t rows_smem_bytes(int key, int nx) {
+    return (key > 0) ? (3 * (size_t)nx + 2 * (size_t)pow2_vstride(nx, 2)) * sizeof(float2)
+                     : (2 * (size_t)nx + 4 * (size_t)padded_len(nx)) * sizeof(float2);
+}
+static size_t cols_smem_bytes(int key, int tile, int ny) {
+    return (key > 0) ? ((size_t)tile * pow2_vstride(ny, tile) + ny) * sizeof(float2)
+                     : 2 * (size_t)tile * padded_len(ny) * sizeof(float2);
+}
+constexpr size_t kSmemLimit = 227 * 1024;
+constexpr size_t kBatchStatic = 4096;     // static smem of the batch kernels (args + prefix)
+
 template <int N, int PROG>
 static cudaError_t launch_rows_prog(const SurfaceArgs &a, cudaStream_t st) {
-    const int nx = a.nx;
-    size_t smem = (N > 0) ? (3 * (size_t)nx + 2 * (size_t)pow2_vstride(nx, 2)) * sizeof(float2)
-                          : (2 * (size_t)nx + 4 * (size_t)padded_len(nx)) * sizeof(float2);
-    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+    const size_t smem = rows_smem_bytes(N, a.nx);
+    if (smem > kSmemLimit) return cudaErrorInvalidValue;
     cudaError_t e = ensure_smem((const void *)surface_rows_kernel<N, PROG>, smem);
     if (e != cudaSuccess) return e;
     surface_rows_kernel<N, PROG><<<a.ny / 2 + 1, rows_threads<N>(), smem, st>>>(a);
@@ -448,7 +470,7 @@ static int field_program(const SurfaceArgs &a) {
 
 template <int N>
 static cudaError_t launch_rows_n(const SurfaceArgs &a, cudaStream_t st) {
-    switch (field_program(a)) {
+    switch (a.prog) {
         case 1: return launch_rows_prog<N, 1>(a, st);
         case 2: return launch_rows_prog<N, 2>(a, st);
         default: return launch_rows_prog<N, 0>(a, st);
@@ -457,10 +479,8 @@ static cudaError_t launch_rows_n(const SurfaceArgs &a, cudaStream_t st) {
 
 template <int N, int TILE>
 static cudaError_t launch_cols_n(const SurfaceArgs &a, cudaStream_t st) {
-    const int ny = a.ny;
-    size_t smem = (N > 0) ? ((size_t)TILE * pow2_vstride(ny, TILE) + ny) * sizeof(float2)
-                          : 2 * (size_t)TILE * padded_len(ny) * sizeof(float2);
-    if (smem > 227 * 1024) return cudaErrorInvalidValue;
+    const size_t smem = cols_smem_bytes(N, TILE, a.ny);
+    if (smem > kSmemLimit) return cudaErrorInvalidValue;
     cudaError_t e = ensure_smem((const void *)surface_cols_kernel<N, TILE>, smem);
     if (e != cudaSuccess) return e;
     dim3 grid((a.nx + TILE - 1) / TILE, a.npair);
@@ -496,6 +516,152 @@ static cudaError_t launch_cols(const SurfaceArgs &a, cudaStream_t st) {
     }
 }
 
+
+// ---------------------------------------------------------------------------------------
+// Scene batch (batch.cuh): one launch of the row (column) pass covers every live slot whose
+// transform length is N.  The host sizes the grid for all slots in use; CTAs enumerate
+// the live slots' items over the slot table and take one item each (a CTA that loops over
+// several items makes the compiler keep the FFT's loop-invariant shared-memory addressing
+// in registers across items, which spills).
+
+// Copy a slot's SurfaceArgs into shared memory and set this pulse's time, additive terms
+// and swell rotation from the slot's per-pulse tables.
+OCS_D void load_slot_surface(const SlotState &g, SurfaceArgs &sa) {
+    const int *src = static_cast<const int *>(g.sargs);
+    int *dst = reinterpret_cast<int *>(&sa);
+    for (int i = threadIdx.x; i < (int)(sizeof(SurfaceArgs) / 4); i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int c = g.counter;
+        sa.t = g.t_tab[c];
+        for (int f = 0; f < g.nfields; ++f) sa.add[f] = g.add_tab[(size_t)c * g.nfields + f];
+        if (g.swrot_tab) sa.swell_rot = g.swrot_tab[c];
+    }
+    __syncthreads();
+}
+
+OCS_D bool slot_surface_live(const SlotState &g) {
+    return slot_live(g) && (g.flags_tab[g.counter] & kFlagSurface);
+}
+
+template <int N, int PROG>
+__global__ void __launch_bounds__(rows_threads<N>(), rows_threads<N>() <= 512 ? 2 : 1)
+batch_rows_kernel(const __grid_constant__ BatchRef b) {
+    extern __shared__ __align__(16) float2 sbuf[];
+    __shared__ SurfaceArgs sa;
+    __shared__ int pref[kMaxSlots + 1];
+    const int total = scan_slots(b, pref, [](const SlotState &g) {
+        return (g.rows_key == N && g.prog == PROG && slot_surface_live(g)) ? g.ny / 2 + 1 : 0;
+    });
+    const int item = blockIdx.x;
+    if (item >= total) return;
+    const int s = find_slot(pref, b.nslots, item);
+    load_slot_surface(b.slots[s], sa);
+    rows_item<N, PROG>(sa, item - pref[s], sbuf, true);
+}
+
+template <int N, int TILE>
+__global__ void __launch_bounds__(cols_threads<N, TILE>(), cols_threads<N, TILE>() <= 512 ? 2 : 1)
+batch_cols_kernel(const __grid_constant__ BatchRef b) {
+    extern __shared__ __align__(16) float2 sbuf[];
+    __shared__ SurfaceArgs sa;
+    __shared__ int pref[kMaxSlots + 1];
+    const int total = scan_slots(b, pref, [](const SlotState &g) {
+        return (g.cols_key == N && slot_surface_live(g)) ? g.npair * ((g.nx + TILE - 1) / TILE) : 0;
+    });
+    const int item = blockIdx.x;
+    if (item >= total) return;
+    const int s = find_slot(pref, b.nslots, item);
+    load_slot_surface(b.slots[s], sa);
+    const int j = item - pref[s];
+    const int ntile = (sa.nx + TILE - 1) / TILE;
+    const int p = j / ntile;
+    cols_item<N, TILE>(sa, p, (j - p * ntile) * TILE, sbuf, true);
+}
+
+template <int N, int PROG>
+static int batch_rows_prog(const BatchRef &b, int grid, size_t smem, cudaStream_t st) {
+    auto k = batch_rows_kernel<N, PROG>;
+    if (smem + kBatchStatic > kSmemLimit) return OCS_ERR_SIZE;
+    if (ensure_smem((const void *)k, smem) != cudaSuccess) return OCS_ERR_CUDA;
+    k<<<grid, rows_threads<N>(), smem, st>>>(b);
+    return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
+}
+
+template <int N, int TILE>
+static int batch_cols_n(const BatchRef &b, int grid, size_t smem, cudaStream_t st) {
+    auto k = batch_cols_kernel<N, TILE>;
+    if (smem + kBatchStatic > kSmemLimit) return OCS_ERR_SIZE;
+    if (ensure_smem((const void *)k, smem) != cudaSuccess) return OCS_ERR_CUDA;
+    k<<<grid, cols_threads<N, TILE>(), smem, st>>>(b);
+    return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
+}
+
+template <int N>
+static int batch_rows_n(const BatchRef &b, int prog, int grid, size_t smem, cudaStream_t st) {
+    switch (prog) {
+        case 1: return batch_rows_prog<N, 1>(b, grid, smem, st);
+        case 2: return batch_rows_prog<N, 2>(b, grid, smem, st);
+        default: return batch_rows_prog<N, 0>(b, grid, smem, st);
+    }
+}
+
+size_t surface_args_bytes() { return sizeof(SurfaceArgs); }
+
+int surface_key(int n) {
+    switch (n) {
+        case 64: case 128: case 256: case 512: case 1024: case 2048: case 4096: case 8192: return n;
+        default: {
+            FftPlan pl;
+            return (n >= 2 && n <= 8192 && make_plan(n, pl)) ? 0 : -1;
+        }
+    }
+}
+
+int surface_cols_tile(int key) { return key == 8192 ? 2 : 4; }
+
+long long surface_rows_smem(int key, int nx) {
+    const size_t b = rows_smem_bytes(key, nx);
+    return b + kBatchStatic > kSmemLimit ? -1 : (long long)b;
+}
+
+long long surface_cols_smem(int key, int ny) {
+    const size_t b = cols_smem_bytes(key, surface_cols_tile(key), ny);
+    return b + kBatchStatic > kSmemLimit ? -1 : (long long)b;
+}
+
+int batch_launch_rows(const BatchRef &b, int key, int prog, int grid, size_t smem, cudaStream_t st) {
+    if (grid < 1) return OCS_OK;
+    switch (key) {
+        case 64: return batch_rows_n<64>(b, prog, grid, smem, st);
+        case 128: return batch_rows_n<128>(b, prog, grid, smem, st);
+        case 256: return batch_rows_n<256>(b, prog, grid, smem, st);
+        case 512: return batch_rows_n<512>(b, prog, grid, smem, st);
+        case 1024: return batch_rows_n<1024>(b, prog, grid, smem, st);
+        case 2048: return batch_rows_n<2048>(b, prog, grid, smem, st);
+        case 4096: return batch_rows_n<4096>(b, prog, grid, smem, st);
+        case 8192: return batch_rows_n<8192>(b, prog, grid, smem, st);
+        case 0: return batch_rows_n<0>(b, prog, grid, smem, st);
+        default: return OCS_ERR_ARG;
+    }
+}
+
+int batch_launch_cols(const BatchRef &b, int key, int grid, size_t smem, cudaStream_t st) {
+    if (grid < 1) return OCS_OK;
+    switch (key) {
+        case 64: return batch_cols_n<64, 4>(b, grid, smem, st);
+        case 128: return batch_cols_n<128, 4>(b, grid, smem, st);
+        case 256: return batch_cols_n<256, 4>(b, grid, smem, st);
+        case 512: return batch_cols_n<512, 4>(b, grid, smem, st);
+        case 1024: return batch_cols_n<1024, 4>(b, grid, smem, st);
+        case 2048: return batch_cols_n<2048, 4>(b, grid, smem, st);
+        case 4096: return batch_cols_n<4096, 4>(b, grid, smem, st);
+        case 8192: return batch_cols_n<8192, 2>(b, grid, smem, st);
+        case 0: return batch_cols_n<0, 4>(b, grid, smem, st);
+        default: return OCS_ERR_ARG;
+    }
+}
+
 }  // namespace ocs
 
 using namespace ocs;
@@ -519,13 +685,13 @@ extern "C" int ocs_surface_prepare(int32_t nx, int32_t ny, void *workspace, void
     return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
 }
 
-extern "C" int ocs_surface_update_passes(const ocs_surface_desc *d, float t, int passes, void *stream) {
-    if (passes < 1 || passes > 3) return OCS_ERR_ARG;
+// Launch arguments of a surface descriptor at time t (shared by the single-scene entry
+// points and the scene batch).
+int fill_surface_args(const ocs_surface_desc *d, float t, SurfaceArgs &a) {
     if (!d || !d->coefs_d || !d->omega_d || !d->kx_d || !d->ky_d || !d->workspace_d) return OCS_ERR_ARG;
     const int nx = d->nx, ny = d->ny;
     if (nx < 2 || ny < 2 || d->nfields < 1 || d->nfields > 2 * kMaxPacked) return OCS_ERR_ARG;
     if (nx > 8192 || ny > 8192) return OCS_ERR_SIZE;
-    SurfaceArgs a;
     memset(&a, 0, sizeof(a));
     a.nx = nx;
     a.ny = ny;
@@ -561,6 +727,27 @@ extern "C" int ocs_surface_update_passes(const ocs_surface_desc *d, float t, int
     a.stw_x = (const float2 *)(ws + ws_stx(nx, ny));
     a.stw_y = (const float2 *)(ws + ws_sty(nx, ny));
     a.scratch = (float2 *)(ws + ws_scratch(nx, ny));
+    a.prog = field_program(a);
+    return OCS_OK;
+}
+
+namespace ocs {
+int surface_args_fill(const ocs_surface_desc *d, void *out, int *prog) {
+    SurfaceArgs a;
+    const int st = fill_surface_args(d, 0.f, a);
+    if (st == OCS_OK) {
+        memcpy(out, &a, sizeof(a));
+        *prog = a.prog;
+    }
+    return st;
+}
+}  // namespace ocs
+
+extern "C" int ocs_surface_update_passes(const ocs_surface_desc *d, float t, int passes, void *stream) {
+    if (passes < 1 || passes > 3) return OCS_ERR_ARG;
+    SurfaceArgs a;
+    const int fst = fill_surface_args(d, t, a);
+    if (fst != OCS_OK) return fst;
     cudaStream_t st = (cudaStream_t)stream;
 
     cudaError_t e = (passes & 1) ? launch_rows(a, st) : cudaSuccess;

@@ -250,6 +250,42 @@ class RawGenerator(object):
         _capi.call("ocs_pulse", ctypes.addressof(d), PRECISIONS[self.precision],
                    _device.stream_ptr(self.stream))
 
+    def pulse_schedule(self):
+        """Per-pulse inputs of the whole scene, computed as ``pulse`` computes them pulse
+        by pulse (same float32 time, additive terms, swell rotation, azimuth position,
+        surface-update and Bragg-refresh decisions and scatterer offsets), for the scene
+        batch.  Returns (tables, refresh pulses, time of the last refresh)."""
+        s = self.surface
+        n = self.az_steps
+        nf = max(1, len(s._raw))
+        t32 = np.zeros(n, np.float32)
+        add = np.zeros((n, nf), np.float32)
+        rot = np.zeros((n, 2), np.float32)
+        az_now = np.zeros(n, np.float64)
+        flags = np.zeros(n, np.int32)
+        tmod = np.zeros((n, 2), np.int32)
+        t_last = -1.
+        refreshes = []
+        for a in range(n):
+            t_now = a * self.t_step
+            az_now[a] = (t_now - self.t_span / 2.) * self.v_ground
+            if (not self.frozen) or a == 0:
+                flags[a] |= 1
+            tt, ad, ro = s.time_terms(t_now)
+            t32[a] = tt
+            add[a, :len(ad)] = ad
+            rot[a] = (np.real(ro), np.imag(ro))
+            if self.scat_bragg_enable:
+                tind = self.rndscat_m.tind(t_now)
+                tmod[a] = (tind % int(self.rndscat_m.N), tind % int(self.rndscat_p.N))
+                if (t_now - t_last) > self.ocean_dt:
+                    flags[a] |= 2
+                    t_last = t_now
+                    refreshes.append(a)
+        tables = dict(t=t32, add=add, swell_rot=rot if s.swell_enable else None, az_now=az_now,
+                      flags=flags, tmod=tmod)
+        return tables, refreshes, t_last
+
     def run(self, steps=None):
         for a in (range(self.az_steps) if steps is None else steps):
             self.pulse(a)

@@ -360,25 +360,8 @@ class OceanSurface(object):
         self._host_cache = {}
         if not self._raw:
             return
-        n = len(self._raw)
-        add = (ctypes.c_float * n)()
-        for i, (_, _, key, _) in enumerate(self._raw):
-            if key == 'Dx':
-                add[i] = float(self.current[0] * self._t)
-            elif key == 'Dy':
-                add[i] = float(self.current[1] * self._t)
-            elif key == 'Vx':
-                add[i] = float(self.current[0])
-            elif key == 'Vy':
-                add[i] = float(self.current[1])
-        rot = np.complex64(0)
-        if self.swell_enable:
-            rot = np.exp(-1j * self.swell_omega * self._t)
-        desc = SurfaceDesc(self.Nx, self.Ny, self._coefs_d.data_ptr(), self._omega_d.data_ptr(),
-                           self._kx_d.data_ptr(), self._ky_d.data_ptr(), float(self.kmin_half), n,
-                           self._codes, self._dsts, add, self._swm,
-                           self._swell_d.data_ptr() if self._swell_d is not None else None,
-                           float(np.real(rot)), float(np.imag(rot)), self._ws.data_ptr())
+        _, add, rot = self.time_terms(value)
+        desc = self.update_desc(add, rot)
         sp = _device.stream_ptr(stream)
         if passes == 3:
             _capi.call("ocs_surface_update", ctypes.addressof(desc), ctypes.c_float(float(self._t)), sp)
@@ -387,6 +370,39 @@ class OceanSurface(object):
                        int(passes), sp)
         if self._aux and passes & 2:
             self._choppy(rot, sp)
+
+    def time_terms(self, value):
+        """(float32 t, additive term of every synthesised field, swell rotation) at time
+        ``value``: the per-call inputs of the surface update besides the spectrum."""
+        t = np.float32(value)
+        add = []
+        for _, _, key, _ in self._raw:
+            if key == 'Dx':
+                add.append(float(self.current[0] * t))
+            elif key == 'Dy':
+                add.append(float(self.current[1] * t))
+            elif key == 'Vx':
+                add.append(float(self.current[0]))
+            elif key == 'Vy':
+                add.append(float(self.current[1]))
+            else:
+                add.append(0.0)
+        rot = np.complex64(0)
+        if self.swell_enable:
+            rot = np.exp(-1j * self.swell_omega * t)
+        return t, add, rot
+
+    def update_desc(self, add=None, rot=np.complex64(0)):
+        """``ocs_surface_desc`` of this surface (the caller keeps it alive while in use)."""
+        n = len(self._raw)
+        add_c = (ctypes.c_float * n)(*(add if add is not None else [0.0] * n))
+        desc = SurfaceDesc(self.Nx, self.Ny, self._coefs_d.data_ptr(), self._omega_d.data_ptr(),
+                           self._kx_d.data_ptr(), self._ky_d.data_ptr(), float(self.kmin_half), n,
+                           self._codes, self._dsts, add_c, self._swm,
+                           self._swell_d.data_ptr() if self._swell_d is not None else None,
+                           float(np.real(rot)), float(np.imag(rot)), self._ws.data_ptr())
+        desc._keep = add_c
+        return desc
 
     def _choppy(self, rot, sp):
         a, f = self._aux, self._fields
