@@ -139,8 +139,8 @@ __global__ void pulse_rows_kernel(const __grid_constant__ PulseArgs a) {
 }
 
 // Shared memory of the pulse kernel: pre-shifted weight table, CTA bin window, the tile's
-// rows of the per-pulse row table ([5][kPulseRowsMax] float64 + [rows][nch] complex), and
-// the block-reduction scratch.
+// rows of the per-pulse row table ([5][RCAP] float64 + [RCAP][nch] complex, RCAP = the
+// largest tile height of the launch), and the block-reduction scratch.
 template <typename T> struct PulseSmem {
     T *wtab, *bins;
     double *r_az;
@@ -148,27 +148,27 @@ template <typename T> struct PulseSmem {
     double *sred;
 };
 
-template <typename T, int NOUT, int S>
+template <typename T, int NOUT, int S, int RCAP>
 OCS_HD constexpr size_t pulse_smem_bytes(int nch) {
     return (size_t)wtab_len<T, S>(kSincTaps, kSincOvs) * sizeof(T) + (size_t)NOUT * kPulseNbw * 2 * sizeof(T) +
-           5 * kPulseRowsMax * sizeof(double) + (size_t)kPulseRowsMax * nch * sizeof(cplx<T>) + 32 * sizeof(double);
+           5 * RCAP * sizeof(double) + (size_t)RCAP * nch * sizeof(cplx<T>) + 32 * sizeof(double);
 }
 
-template <typename T, int NOUT, int S>
+template <typename T, int NOUT, int S, int RCAP>
 OCS_D PulseSmem<T> pulse_smem(unsigned char *smem, int nch) {
     PulseSmem<T> sm;
     sm.wtab = reinterpret_cast<T *>(smem);
     sm.bins = sm.wtab + wtab_len<T, S>(kSincTaps, kSincOvs);             // [NOUT][nbw][2]
     sm.r_az = reinterpret_cast<double *>(sm.bins + NOUT * kPulseNbw * 2);
-    sm.r_fac = reinterpret_cast<cplx<T> *>(sm.r_az + 5 * kPulseRowsMax);   // [rows][nch]
-    sm.sred = reinterpret_cast<double *>(sm.r_fac + kPulseRowsMax * nch);
+    sm.r_fac = reinterpret_cast<cplx<T> *>(sm.r_az + 5 * RCAP);            // [rows][nch]
+    sm.sred = reinterpret_cast<double *>(sm.r_fac + RCAP * nch);
     return sm;
 }
 
 // One tile of kPulseCols columns x tile_rows rows: NRCS, scene and accumulation of every
 // facet into this pulse's raw rows; the tile's NRCS sums are added to spec_sum and
 // bragg_sum.
-template <typename T, int NOUT, int S>
+template <typename T, int NOUT, int S, int RCAP>
 OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSmem<T> &sm, double &spec_sum,
                       double (&bragg_sum)[2]) {
     const int tiles_x = (a.nx + kPulseCols - 1) / kPulseCols;
@@ -179,7 +179,7 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
     // this tile's rows of the per-pulse row table (pulse_rows_kernel)
     for (int i = threadIdx.x; i < nrows * 5; i += blockDim.x) {
         const int q = i / nrows, k = i - q * nrows;
-        sm.r_az[q * kPulseRowsMax + k] = a.rowtab[(long long)q * a.ny + y0 + k];
+        sm.r_az[q * RCAP + k] = a.rowtab[(long long)q * a.ny + y0 + k];
     }
     {
         const double *fac = a.rowtab + 5LL * a.ny + 2LL * y0 * a.nch;
@@ -223,7 +223,7 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
         for (int i = 0; i < nrows; ++i) {
             const long long idx = (long long)(y0 + i) * a.nx + x;
             if (i + 1 < nrows) nxt.load(a, idx + a.nx, npix, scat, load_scat);
-            const double az = sm.r_az[i], sin_az = sm.r_az[kPulseRowsMax + i];
+            const double az = sm.r_az[i], sin_az = sm.r_az[RCAP + i];
             // slant range: sr - cos_inc*Dz + az/2*sin_az + Dx*sin_inc + Dy*sin_az, float64,
             // left to right, no fused multiply-adds (bit-identical with numpy)
             double srs = dsub(sr_c, dmul(cos_i, (double)cur.dz));
@@ -236,7 +236,7 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
 
             cplx<T> scene[2] = {{(T)0, (T)0}, {(T)0, (T)0}};      // per polarisation
             if (a.do_kodis) {
-                const cplx<T> e = kodis_facet<T>(a.kodis, srs, sin_i, cos_i, tan_i, sm.r_az[3 * kPulseRowsMax + i], sm.r_az[4 * kPulseRowsMax + i],
+                const cplx<T> e = kodis_facet<T>(a.kodis, srs, sin_i, cos_i, tan_i, sm.r_az[3 * RCAP + i], sm.r_az[4 * RCAP + i],
                                                  cur.diffx, cur.diffy, cur.diffxx, cur.diffyy, cur.diffxy);
                 const T s4 = (T)3.5449077018110318;                 // sqrt(4 pi)
                 const cplx<T> es = {e.re * s4, e.im * s4};
@@ -248,7 +248,7 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
                 T sc[2][2];                                            // [pol][line]
                 if (a.refresh) {
                     T hh[2], vv[2];
-                    romeiser_facet<T>(a.rom, (T)inc_c, (T)sm.r_az[2 * kPulseRowsMax + i], (T)sm.r_az[3 * kPulseRowsMax + i], (T)sm.r_az[4 * kPulseRowsMax + i],
+                    romeiser_facet<T>(a.rom, (T)inc_c, (T)sm.r_az[2 * RCAP + i], (T)sm.r_az[3 * RCAP + i], (T)sm.r_az[4 * RCAP + i],
                                       (T)cur.diffx, (T)cur.diffy, hh, vv);
                     if (a.use_hmtf) {
                         float hm = a.hmtf[idx];
@@ -349,13 +349,13 @@ template <typename T, int NOUT, int S>
 __global__ void __launch_bounds__(kPulseCols, (sizeof(T) == 4 && NOUT < 4) ? 4 : 2)
 pulse_kernel(const __grid_constant__ PulseArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
-    const PulseSmem<T> sm = pulse_smem<T, NOUT, S>(smem, a.nch);
+    const PulseSmem<T> sm = pulse_smem<T, NOUT, S, kPulseRows>(smem, a.nch);
     build_wtab<T, S>(sm.wtab, a.sinc, kSincTaps, kSincOvs);
     const int tiles = ((a.nx + kPulseCols - 1) / kPulseCols) * ((a.ny + kPulseRows - 1) / kPulseRows);
     double spec_sum = 0.0, bragg_sum[2] = {0.0, 0.0};
     // persistent CTAs: each walks tiles of kPulseCols columns x kPulseRows rows
     for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x)
-        pulse_tile<T, NOUT, S>(a, tile, kPulseRows, sm, spec_sum, bragg_sum);
+        pulse_tile<T, NOUT, S, kPulseRows>(a, tile, kPulseRows, sm, spec_sum, bragg_sum);
     pulse_nrcs<T>(a, sm, spec_sum, bragg_sum);
 }
 
@@ -437,16 +437,16 @@ batch_pulse_kernel(const __grid_constant__ BatchRef b) {
         pa.raw_row = (long long)c * pa.nbins;
     }
     __syncthreads();
-    const PulseSmem<T> sm = pulse_smem<T, NOUT, S>(smem, kMaxCh);
+    const PulseSmem<T> sm = pulse_smem<T, NOUT, S, kPulseRowsMax>(smem, kMaxCh);
     build_wtab<T, S>(sm.wtab, pa.sinc, kSincTaps, kSincOvs);
     double spec_sum = 0.0, bragg_sum[2] = {0.0, 0.0};
-    pulse_tile<T, NOUT, S>(pa, tile, g.tile_rows, sm, spec_sum, bragg_sum);
+    pulse_tile<T, NOUT, S, kPulseRowsMax>(pa, tile, g.tile_rows, sm, spec_sum, bragg_sum);
     pulse_nrcs<T>(pa, sm, spec_sum, bragg_sum);
 }
 
 template <typename T, int NOUT, int S>
 static int launch_pulse(const PulseArgs &a, cudaStream_t st) {
-    const size_t smem = pulse_smem_bytes<T, NOUT, S>(a.nch);
+    const size_t smem = pulse_smem_bytes<T, NOUT, S, kPulseRows>(a.nch);
     auto k = pulse_kernel<T, NOUT, S>;
     if (ensure_smem((const void *)k, smem) != cudaSuccess)
         return OCS_ERR_CUDA;
@@ -549,7 +549,7 @@ int batch_launch_pulse_rows(const BatchRef &b, cudaStream_t st) {
 
 template <typename T, int NOUT, int S>
 static int batch_pulse_n(const BatchRef &b, int grid, cudaStream_t st) {
-    const size_t smem = pulse_smem_bytes<T, NOUT, S>(kMaxCh);
+    const size_t smem = pulse_smem_bytes<T, NOUT, S, kPulseRowsMax>(kMaxCh);
     auto k = batch_pulse_kernel<T, NOUT, S>;
     if (ensure_smem((const void *)k, smem) != cudaSuccess) return OCS_ERR_CUDA;
     k<<<grid, kPulseCols, smem, st>>>(b);

@@ -49,6 +49,7 @@ class SceneBatch(object):
         self._h = h
         self._slots = [None] * self.max_slots
         self._graphs = {}
+        self.max_graphs = 64
         self.steps_run = 0
 
     # ------------------------------------------------------------------------------------
@@ -91,10 +92,13 @@ class SceneBatch(object):
             slot = free[0]
         if self._slots[slot] is not None:
             raise ValueError('slot %d is occupied' % slot)
-        tables, refreshes, t_last = gen.pulse_schedule()
-        dev = {}
-        for k, v in tables.items():
-            dev[k] = None if v is None else _device.to_device(v, v.dtype)
+        gen.to_device()
+        sched = getattr(gen, '_batch_schedule', None)
+        if sched is None:
+            tables, refreshes, t_last = gen.pulse_schedule()
+            dev = {k: (None if v is None else _device.to_device(v, v.dtype)) for k, v in tables.items()}
+            sched = gen._batch_schedule = (dev, refreshes, t_last)
+        dev, refreshes, t_last = sched
         gen.reset()
         gen._refreshes = list(refreshes)
         d = gen.desc
@@ -112,6 +116,23 @@ class SceneBatch(object):
                  gen.npol * gen.num_ch, s.tile_rows)
         self._slots[slot] = s
         return slot
+
+    def restart(self, slot, tile_rows=None):
+        """Put a slot's scene back to pulse 0 (raw cube and NRCS cleared), optionally with
+        another pulse-kernel tile height (used by the autotuner)."""
+        s = self._slots[slot]
+        rows = s.tile_rows if tile_rows is None else int(tile_rows)
+        self._slots[slot] = None
+        _capi.call("ocs_batch_clear", self._h, int(slot), self._sp())
+        self.add(s.gen, slot=slot, tile_rows=rows)
+
+    def tile_rows(self, slot):
+        return self._slots[slot].tile_rows
+
+    def scene_class(self, slot):
+        """(Nx, Ny, outputs): scenes of one class share their launch shapes."""
+        g = self._slots[slot].gen
+        return (g.surface.Nx, g.surface.Ny, g.npol * g.num_ch)
 
     def remove(self, slot):
         """Free a slot (the scene's buffers stay with its RawGenerator)."""
@@ -175,6 +196,9 @@ class SceneBatch(object):
             with torch.cuda.graph(g, stream=side):
                 _capi.call("ocs_batch_step", self._h, int(pulses), ctypes.c_void_p(side.cuda_stream))
             cur.wait_stream(side)
+            if len(self._graphs) >= self.max_graphs:
+                for k in [k for k, v in self._graphs.items() if v is not None][:len(self._graphs) // 2]:
+                    del self._graphs[k]
             self._graphs[key] = g
             # recording enqueued nothing: the steps still have to run
         with torch.cuda.stream(self.stream) if self.stream is not None else _nullctx():

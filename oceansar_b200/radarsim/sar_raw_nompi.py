@@ -41,14 +41,33 @@ def sinc_bp(sin_angle, L, f0, field=False):
     return pattern if field else pattern ** 2
 
 
+def scene_device_bytes(nx, ny, nfields, npol, nch, az_steps, rg_samp, precision, bragg=True):
+    """Device memory a scene holds while it runs (bytes): spectrum, omega, surface fields and
+    FFT scratch, sqrt(RCS), scatterer index maps, raw cube and small tables.  Used to admit
+    scenes under a memory budget before they are allocated."""
+    nf = float(nx) * ny
+    npair = (nfields + 1) // 2
+    cb = 16 if precision == 'f64' else 8
+    b = nf * (8 + 4)                         # wave coefficients, omega
+    b += nf * 4 * nfields                    # fields
+    b += nf * 8 * npair                      # FFT scratch planes
+    if bragg:
+        b += nf * (8 if precision == 'f64' else 4) * 2 * npol + nf * 4 * 2
+    b += float(npol) * nch * az_steps * rg_samp * cb
+    b += az_steps * (8 + 8 * npol + 64) + ny * (5 + 2 * nch) * 8 + (nx + ny) * 64 + (1 << 20)
+    return int(b)
+
+
 class RawGenerator(object):
     """Device-resident state of one ``sar_raw`` scene; see the module docstring.
 
     ``overrides`` may fix ``az_steps`` / ``rg_samp`` / ``rg_samp_orig`` (the reference
-    derives them from the geometry, ``sar_raw_nompi.py:264-278``).
+    derives them from the geometry, ``sar_raw_nompi.py:264-278``).  ``device=False`` does
+    only the host set-up (no GPU touched; the object pickles), and ``to_device()`` then
+    uploads and allocates -- scene preparation in worker processes.
     """
 
-    def __init__(self, cfg, precision='f64', overrides=None, seed=None, stream=None):
+    def __init__(self, cfg, precision='f64', overrides=None, seed=None, stream=None, device=True):
         if precision not in PRECISIONS:
             raise ValueError('precision must be f64 or mixed')
         self.precision = precision
@@ -103,7 +122,7 @@ class RawGenerator(object):
                np.deg2rad(oc.current_dir), oc.dir_swell_dir, oc.freq_r, oc.sigf, oc.sigs, oc.Hs,
                oc.swell_dir_enable, oc.swell_enable, oc.swell_ampl, np.deg2rad(oc.swell_dir),
                oc.swell_wl, compute, oc.opt_res, oc.fft_max_prime, choppy_enable=oc.choppy_enable,
-               depth=oc.depth, dirspectrum_func=None, dir_swell_spec=dir_swell)
+               depth=oc.depth, dirspectrum_func=None, dir_swell_spec=dir_swell, device=device)
         self.frozen = bool(getattr(oc, 'frozen_ocean', False))
 
         # ---- geometry (:231-278) ----------------------------------------------------------
@@ -158,8 +177,24 @@ class RawGenerator(object):
                                                 srg.scat_bragg_spec, srg.scat_bragg_spread,
                                                 srg.scat_bragg_d, rmss_x=s.rmss_x, rmss_y=s.rmss_y,
                                                 use_lut=bool(srg.use_lut))
-        self._alloc()
+        self._on_device = False
+        if device:
+            self.to_device()
         self.t_last_rcs_bragg = -1.
+
+    def to_device(self):
+        """Upload the host set-up and allocate the device buffers (once)."""
+        if not self._on_device:
+            self.surface.to_device()
+            self._alloc()
+            self._on_device = True
+        return self
+
+    def device_bytes(self):
+        """Device memory of the scene's buffers (bytes), known before ``to_device``."""
+        nfields = 5 + (3 if self.scat_spec_enable else 0) + (1 if self.use_hmtf else 0)
+        return scene_device_bytes(self.surface.Nx, self.surface.Ny, nfields, self.npol, self.num_ch,
+                                  self.az_steps, self.rg_samp, self.precision, self.scat_bragg_enable)
 
     # ------------------------------------------------------------------------------------
     def _alloc(self):

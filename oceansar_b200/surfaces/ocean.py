@@ -86,7 +86,9 @@ class OceanSurface(object):
              wind_U, current_mag, current_dir, dir_swell_dir=0, freq_r=100, sigf=1, sigs=1, Hs=2,
              swell_dir_enable=False, swell_enable=False, swell_ampl=0., swell_dir=0., swell_wl=0.,
              compute=[], opt_res=True, fft_max_prime=2, choppy_enable=False, dirspectrum_func=None,
-             depth=None, dir_swell_spec=None):
+             depth=None, dir_swell_spec=None, device=True):
+        """``device=False`` stops after the host-side spectrum (no GPU touched); ``to_device()``
+        uploads it later (a scene prepared in another process)."""
         self.Lx, self.Ly, self.dx, self.dy = Lx, Ly, dx, dy
         self.wind_dir, self.wind_fetch, self.wind_U = wind_dir, wind_fetch, wind_U
         self.current_mag, self.current_dir = current_mag, current_dir
@@ -199,8 +201,16 @@ class OceanSurface(object):
             self.swell_coefs = (self.Nx * self.Ny * np.sqrt(2. * self.swell_dirspec * kx_res * ky_res) *
                                 random_swell).astype(np.complex64)
             self.wave_coefs = self.wave_coefs + self.swell_coefs
-        self._upload()
+        self._on_device = False
+        if device:
+            self._upload()
         self.initialized = True
+        return self
+
+    def to_device(self):
+        """Upload a surface initialised with ``device=False`` (no-op once on the device)."""
+        if not getattr(self, '_on_device', True):
+            self._upload()
         return self
 
     # ------------------------------------------------------------------------------
@@ -213,6 +223,7 @@ class OceanSurface(object):
         self._swell_d = (_device.to_device(self.swell_exp, np.complex64)
                          if self.swell_enable else None)
         self._plan_fields()
+        self._on_device = True
 
     def _plan_fields(self):
         names = []
