@@ -226,6 +226,160 @@ def run_reference(args, c, cfg_path):
 
 
 # ----------------------------------------------------------------------------------------
+# Batched and serving workloads (one GPU; replicas for N > 1 as for the default workload)
+def _workload_reference(args, specs, what):
+    """CPU oracle on a bounded sample of the workload's scenes (2 pulses of each of the
+    first three), as echoes/s."""
+    from oceansar_b200.serving import prepare_scene  # noqa: F401  (same cfg writer)
+    from oracle.sar_raw import SarRawSim
+    tot_e, tot_t = 0.0, 0.0
+    tmpd = tempfile.mkdtemp(prefix="ocs_ref_")
+    for k, sp in enumerate(specs[:3]):
+        path = os.path.join(tmpd, "s%d.cfg" % k)
+        with open(path, "w") as f:
+            f.write(sp["cfg"])
+        sim = SarRawSim(path, overrides=sp["overrides"], seed=sp["seed"])
+        sim.pulse(0)
+        t0 = time.perf_counter()
+        for a in (1, 2):
+            sim.pulse(a)
+        tot_t += time.perf_counter() - t0
+        tot_e += 2.0 * sim.surface.Nx * sim.surface.Ny * sim.num_ch
+    v = tot_e / tot_t
+    return {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": "2 pulses of each of the first 3 scenes of the %s workload (%.1f s)" % (what, tot_t)}
+
+
+def run_workload(args):
+    import torch
+    from oceansar_b200 import replicas
+    from oceansar_b200.serving import ScenePreparer, ServingLoop, batched_specs, run_batched, serving_requests
+    from oceansar_b200.tune import Autotuner
+    world, rank, local = dist_info()
+    what = args.workload
+    if what == "batched":
+        specs = batched_specs(args.scenes, seed=1 + 1000 * rank)
+    else:
+        specs = serving_requests(rate=args.rate, duration=args.duration, seed=2 + 1000 * rank)
+    if args.impl == "reference":
+        if rank == 0:
+            cpu = _workload_reference(args, specs, what)
+            print(json.dumps({"metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": args.gpus,
+                              "steps": 1, "warmup": 0, "higher_is_better": True, "scaling": "weak",
+                              "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+                              "config": {"workload": what}, "cpu_baseline": cpu,
+                              "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    torch.cuda.set_device(local)
+    import torch.distributed as dist
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=300))
+    prep = ScenePreparer(workers=args.workers)
+    clocks = ClockSampler(local)
+    tuner = Autotuner()
+    try:
+        if what == "batched":
+            t0 = time.perf_counter()
+            futs = [prep.submit(sp, args.precision) for sp in specs]
+            gens = [f.result() for f in futs]
+            host_prep = time.perf_counter() - t0
+            clocks.start()
+            rep = run_batched(gens, precision=args.precision, tuner=tuner)
+            clk = clocks.stop()
+            # end to end: spectra and scatterer indices from pinned host memory, the run,
+            # every raw cube back to pinned host memory
+            e2e = _batched_e2e(gens, args.precision, tuner, rep["pulse_block"])
+            sec = replicas.max_over_ranks(rep["device_s"], device="cuda")
+            ms = sec * 1e3
+            value = replicas.sum_over_ranks(rep["echoes"], device="cuda") / sec
+            line_extra = {"batched": {k: rep[k] for k in ("scenes", "echoes", "steps", "pulse_block", "tile_rows",
+                                                          "tune_s", "launches_first_step")},
+                          "host_prep_s": host_prep}
+            launches = rep["kernel_launches"]
+            e2e_d = e2e
+        else:
+            clocks.start()
+            loop = ServingLoop(precision=args.precision, hbm_budget=150e9, max_slots=64, pulse_block=16,
+                               preparer=prep, tuner=tuner)
+            rep = loop.run(specs)
+            clk = clocks.stop()
+            sec = replicas.max_over_ranks(rep["span_s"], device="cuda")
+            ms = sec * 1e3
+            value = replicas.sum_over_ranks(rep["echoes"], device="cuda") / sec
+            e2e_d = {"value": value, "unit": UNIT, "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                     "note": "arrival to raw cube in host memory for every request (wall clock)"}
+            line_extra = {"serving": {k: rep[k] for k in ("requests", "echoes", "span_s", "offered_echoes_per_s",
+                                                          "latency_p50_s", "latency_p99_s", "latency_max_s",
+                                                          "peak_reserved_bytes", "max_backlog",
+                                                          "queue_stable")},
+                          "rate_per_s": args.rate, "arrival_window_s": args.duration}
+            launches = None
+    finally:
+        prep.close()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = _workload_reference(args, specs, what)
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": 1, "warmup": 0,
+                "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
+                "config": {"workload": what, "precision": args.precision,
+                           "parallelism": "replicas" if world > 1 else "single-gpu",
+                           "l2": "working set of many scenes far above L2"},
+                "clocks": clk, "e2e": e2e_d, "gpu_launches": launches, "roofline": None,
+                "cpu_baseline": cpu}
+        line.update(line_extra)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def _batched_e2e(gens, precision, tuner, pulse_block):
+    """Echoes/s of the whole batch with host inputs and outputs inside the timed region."""
+    import torch
+    from oceansar_b200.radarsim.batch import SceneBatch
+    from oceansar_b200.serving import scene_echoes
+    batch = SceneBatch(max_slots=len(gens), precision=precision)
+    ins, outs = [], []
+    for g in gens:
+        cls = (g.surface.Nx, g.surface.Ny, g.npol * g.num_ch)
+        batch.add(g, tile_rows=tuner.tile_rows_for(precision, cls))
+        s = g.surface
+        pairs = [(torch.from_numpy(s.wave_coefs).pin_memory(), s._coefs_d),
+                 (torch.from_numpy(s.omega).pin_memory(), s._omega_d)]
+        if g.scat_bragg_enable:
+            pairs.append((torch.from_numpy(g.rndscat_m.ind0.astype(np.int32)).pin_memory(), g.rndscat_m.device()[1]))
+            pairs.append((torch.from_numpy(g.rndscat_p.ind0.astype(np.int32)).pin_memory(), g.rndscat_p.device()[1]))
+        ins.extend(pairs)
+        outs.append((g.raw_d, torch.empty(g.raw_d.shape, dtype=g.raw_d.dtype).pin_memory()))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for h, d in ins:
+        d.copy_(h, non_blocking=True)
+    while True:
+        for sl in batch.finished():
+            batch.remove(sl)
+        live = batch.live()
+        if not live:
+            break
+        batch.graph_step(min(pulse_block, min(batch.remaining(sl) for sl in live)))
+    for d, h in outs:
+        h.copy_(d, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    sec = e0.elapsed_time(e1) * 1e-3
+    batch.close()
+    echoes = sum(scene_echoes(g) for g in gens)
+    h2d = sum(h.numel() * h.element_size() for h, _ in ins)
+    d2h = sum(h.numel() * h.element_size() for _, h in outs)
+    return {"value": echoes / sec, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "ms_per_step": sec * 1e3}
+
+
+# ----------------------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -236,9 +390,19 @@ def main():
     ap.add_argument("--small", action="store_true", help="512^2 single-channel case (quick check)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--workload", default="c2", choices=["c2", "batched", "serving"],
+                    help="c2: the two-channel 2048^2 scene (default); batched: many scenes in one "
+                         "scene batch; serving: a Poisson request stream with continuous batching")
+    ap.add_argument("--scenes", type=int, default=64, help="batched: number of scenes")
+    ap.add_argument("--rate", type=float, default=20.0, help="serving: requests per second")
+    ap.add_argument("--duration", type=float, default=5.0, help="serving: seconds of arrivals")
+    ap.add_argument("--workers", type=int, default=None, help="host set-up worker processes")
     ap.add_argument("--profile-pulses", type=int, default=0,
                     help="run this many pulses with plain launches (for ncu) and exit")
     args = ap.parse_args()
+    if args.workload != "c2":
+        run_workload(args)
+        return
     c = C1 if args.small else C2
     tmpd = tempfile.mkdtemp(prefix="ocs_bench_")
     cfg_path = write_cfg(c, os.path.join(tmpd, "scene.cfg"))

@@ -24,6 +24,16 @@ def max_over_ranks(value, device=None):
     return float(t.item())
 
 
+def sum_over_ranks(value, device=None):
+    """Sum of a float over all ranks (the value itself without a process group)."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device or "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def job_throughput(units_per_rank, seconds_this_rank, device=None):
     """(throughput, max seconds): all ranks' units over the slowest rank's time."""
     import torch.distributed as dist
