@@ -313,6 +313,7 @@ def run_workload(args):
             line_extra = {"serving": {k: rep[k] for k in ("requests", "echoes", "span_s", "offered_echoes_per_s",
                                                           "latency_p50_s", "latency_p99_s", "latency_max_s",
                                                           "peak_reserved_bytes", "max_backlog",
+                                                          "gpu_busy_frac", "capacity_echoes_per_s",
                                                           "queue_stable")},
                           "rate_per_s": args.rate, "arrival_window_s": args.duration}
             launches = None

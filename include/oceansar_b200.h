@@ -277,9 +277,10 @@ typedef struct ocs_batch ocs_batch;    /* opaque engine handle                  
 int ocs_batch_create(int32_t max_slots, int32_t precision, ocs_batch **out);
 int ocs_batch_destroy(ocs_batch *batch);
 /* Put a scene in a slot with its pulse counter at 0 (the caller zeroes its raw cube and
- * NRCS accumulators).  Synchronous with respect to the stream. */
+ * NRCS accumulators).  Ordered on the stream (steps enqueued after it see the scene);
+ * returns without waiting for the stream. */
 int ocs_batch_set(ocs_batch *batch, int32_t slot, const ocs_scene_desc *scene, void *stream);
-/* Take the scene out of a slot.  Synchronous with respect to the stream. */
+/* Take the scene out of a slot.  Ordered on the stream; returns without waiting for it. */
 int ocs_batch_clear(ocs_batch *batch, int32_t slot, void *stream);
 /* Enqueue `pulses` steps: every slot whose counter is below its az_steps runs one pulse per
  * step; finished and empty slots cost nothing. */

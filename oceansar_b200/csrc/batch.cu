@@ -28,15 +28,30 @@ struct HostSlot {
 
 using namespace ocs;
 
+// Slot writes go through pinned staging (one region per slot) so that they are ordered on
+// the caller's stream without blocking the host; a slot's region is reused only after the
+// event of its previous copies has completed.
 struct ocs_batch {
     int max_slots = 0;
     int precision = 0;
     SlotState *d_slots = nullptr;
     char *d_sargs = nullptr;
     char *d_pargs = nullptr;
-    size_t sbytes = 0, pbytes = 0;
+    char *h_stage = nullptr;              // pinned: [max_slots][stage_bytes]
+    size_t sbytes = 0, pbytes = 0, stage_bytes = 0;
+    std::vector<cudaEvent_t> staged;      // per slot: its last staging copies
     std::vector<HostSlot> host;
 };
+
+static void batch_free(ocs_batch *b) {
+    for (cudaEvent_t e : b->staged)
+        if (e) cudaEventDestroy(e);
+    cudaFree(b->d_slots);
+    cudaFree(b->d_sargs);
+    cudaFree(b->d_pargs);
+    cudaFreeHost(b->h_stage);
+    delete b;
+}
 
 extern "C" int ocs_batch_create(int32_t max_slots, int32_t precision, ocs_batch **out) {
     if (!out || max_slots < 1 || max_slots > kMaxSlots) return OCS_ERR_ARG;
@@ -47,17 +62,19 @@ extern "C" int ocs_batch_create(int32_t max_slots, int32_t precision, ocs_batch 
     b->precision = precision;
     b->sbytes = (surface_args_bytes() + 255) & ~(size_t)255;
     b->pbytes = (pulse_args_bytes() + 255) & ~(size_t)255;
+    b->stage_bytes = ((sizeof(SlotState) + 255) & ~(size_t)255) + b->sbytes + b->pbytes;
     b->host.resize(max_slots);
+    b->staged.assign(max_slots, nullptr);
     cudaError_t e = cudaMalloc(&b->d_slots, sizeof(SlotState) * max_slots);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_sargs, b->sbytes * max_slots);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_pargs, b->pbytes * max_slots);
+    if (e == cudaSuccess) e = cudaMallocHost(&b->h_stage, b->stage_bytes * max_slots);
+    for (int i = 0; i < max_slots && e == cudaSuccess; ++i)
+        e = cudaEventCreateWithFlags(&b->staged[i], cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaMemset(b->d_slots, 0, sizeof(SlotState) * max_slots);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
-        cudaFree(b->d_slots);
-        cudaFree(b->d_sargs);
-        cudaFree(b->d_pargs);
-        delete b;
+        batch_free(b);
         return OCS_ERR_CUDA;
     }
     *out = b;
@@ -67,10 +84,7 @@ extern "C" int ocs_batch_create(int32_t max_slots, int32_t precision, ocs_batch 
 extern "C" int ocs_batch_destroy(ocs_batch *b) {
     if (!b) return OCS_ERR_ARG;
     const cudaError_t e = cudaDeviceSynchronize();
-    cudaFree(b->d_slots);
-    cudaFree(b->d_sargs);
-    cudaFree(b->d_pargs);
-    delete b;
+    batch_free(b);
     return e == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
 }
 
@@ -99,10 +113,16 @@ extern "C" int ocs_batch_set(ocs_batch *b, int32_t slot, const ocs_scene_desc *s
         h.pulse_items[w] = batch_pulse_items(sd->nx, sd->ny, tile_rows, h.nout, b->precision, w);
     h.used = true;
 
-    std::vector<char> sargs(b->sbytes, 0), pargs(b->pbytes, 0);
-    int st = surface_args_fill(sd, sargs.data(), &h.prog);
+    // the slot's staging region is free once its previous copies have run
+    if (cudaEventSynchronize(b->staged[slot]) != cudaSuccess) return OCS_ERR_CUDA;
+    char *stage = b->h_stage + b->stage_bytes * slot;
+    char *st_slot = stage;
+    char *st_sargs = stage + ((sizeof(SlotState) + 255) & ~(size_t)255);
+    char *st_pargs = st_sargs + b->sbytes;
+    memset(stage, 0, b->stage_bytes);
+    int st = surface_args_fill(sd, st_sargs, &h.prog);
     if (st != OCS_OK) return st;
-    st = pulse_args_fill(pd, pargs.data());
+    st = pulse_args_fill(pd, st_pargs);
     if (st != OCS_OK) return st;
 
     SlotState s;
@@ -127,14 +147,14 @@ extern "C" int ocs_batch_set(ocs_batch *b, int32_t slot, const ocs_scene_desc *s
     s.tmod_tab = sc->tmod_d;
     s.sargs = b->d_sargs + b->sbytes * slot;
     s.pargs = b->d_pargs + b->pbytes * slot;
+    memcpy(st_slot, &s, sizeof(s));
     cudaStream_t cs = (cudaStream_t)stream;
-    // pageable sources, then a stream synchronisation: the host buffers outlive the copies
-    cudaError_t e = cudaMemcpyAsync(b->d_sargs + b->sbytes * slot, sargs.data(), b->sbytes,
-                                    cudaMemcpyHostToDevice, cs);
+    cudaError_t e = cudaMemcpyAsync(b->d_sargs + b->sbytes * slot, st_sargs, b->sbytes, cudaMemcpyHostToDevice, cs);
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(b->d_pargs + b->pbytes * slot, pargs.data(), b->pbytes, cudaMemcpyHostToDevice, cs);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_slots + slot, &s, sizeof(s), cudaMemcpyHostToDevice, cs);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
+        e = cudaMemcpyAsync(b->d_pargs + b->pbytes * slot, st_pargs, b->pbytes, cudaMemcpyHostToDevice, cs);
+    // the slot record last: kernels that run after it see complete arguments
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_slots + slot, st_slot, sizeof(s), cudaMemcpyHostToDevice, cs);
+    if (e == cudaSuccess) e = cudaEventRecord(b->staged[slot], cs);
     if (e != cudaSuccess) return OCS_ERR_CUDA;
     b->host[slot] = h;
     return OCS_OK;
@@ -142,10 +162,12 @@ extern "C" int ocs_batch_set(ocs_batch *b, int32_t slot, const ocs_scene_desc *s
 
 extern "C" int ocs_batch_clear(ocs_batch *b, int32_t slot, void *stream) {
     if (!b || slot < 0 || slot >= b->max_slots) return OCS_ERR_ARG;
-    const int zero = 0;
+    if (cudaEventSynchronize(b->staged[slot]) != cudaSuccess) return OCS_ERR_CUDA;
+    int *zero = reinterpret_cast<int *>(b->h_stage + b->stage_bytes * slot);
+    *zero = 0;
     cudaStream_t cs = (cudaStream_t)stream;
-    cudaError_t e = cudaMemcpyAsync(&b->d_slots[slot].active, &zero, sizeof(int), cudaMemcpyHostToDevice, cs);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(cs);
+    cudaError_t e = cudaMemcpyAsync(&b->d_slots[slot].active, zero, sizeof(int), cudaMemcpyHostToDevice, cs);
+    if (e == cudaSuccess) e = cudaEventRecord(b->staged[slot], cs);
     if (e != cudaSuccess) return OCS_ERR_CUDA;
     b->host[slot] = HostSlot();
     return OCS_OK;

@@ -48,6 +48,7 @@ class SceneBatch(object):
         _capi.call("ocs_batch_create", self.max_slots, PRECISIONS[precision], ctypes.byref(h))
         self._h = h
         self._slots = [None] * self.max_slots
+        self._upload = torch.cuda.Stream()
         self._graphs = {}
         self.max_graphs = 64
         self.steps_run = 0
@@ -83,7 +84,7 @@ class SceneBatch(object):
         """Place ``gen`` (a RawGenerator of this batch's precision) in a slot; returns it."""
         if gen.precision != self.precision:
             raise ValueError('scene precision %s differs from the batch (%s)' % (gen.precision, self.precision))
-        if gen.surface._aux:
+        if gen.surface.choppy_enable:
             raise NotImplementedError('choppy surfaces run through RawGenerator, not the scene batch')
         if slot is None:
             free = self.free_slots()
@@ -92,14 +93,20 @@ class SceneBatch(object):
             slot = free[0]
         if self._slots[slot] is not None:
             raise ValueError('slot %d is occupied' % slot)
-        gen.to_device()
-        sched = getattr(gen, '_batch_schedule', None)
-        if sched is None:
-            tables, refreshes, t_last = gen.pulse_schedule()
-            dev = {k: (None if v is None else _device.to_device(v, v.dtype)) for k, v in tables.items()}
-            sched = gen._batch_schedule = (dev, refreshes, t_last)
+        # uploads go on a stream of their own, so that placing a scene never waits for the
+        # steps already enqueued; the batch's stream then waits for the uploads
+        with torch.cuda.stream(self._upload):
+            gen.to_device()
+            sched = getattr(gen, '_batch_schedule', None)
+            if sched is None:
+                tables, refreshes, t_last = gen.pulse_schedule()
+                dev = {k: (None if v is None else _device.to_device(v, v.dtype)) for k, v in tables.items()}
+                sched = gen._batch_schedule = (dev, refreshes, t_last)
         dev, refreshes, t_last = sched
-        gen.reset()
+        compute = self.stream if self.stream is not None else torch.cuda.current_stream()
+        compute.wait_stream(self._upload)
+        with torch.cuda.stream(compute):
+            gen.reset()
         gen._refreshes = list(refreshes)
         d = gen.desc
         d.az_step, d.az_now, d.refresh, d.tind = 0, 0.0, 0, 0

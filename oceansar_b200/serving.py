@@ -196,7 +196,7 @@ def run_batched(gens, precision='mixed', tuner=None, pulse_block=None, max_slots
     n = len(gens)
     batch = SceneBatch(max_slots=max_slots or max(1, n), precision=precision)
     for g in gens:
-        batch.add(g.to_device())
+        batch.add(g)
     tuned_rows, t_tune = {}, 0.0
     if tuner is not None:
         t0 = time.perf_counter()
@@ -278,6 +278,7 @@ class ServingLoop(object):
         retiring = []                             # raw cube copy to the host in flight
         inflight = collections.deque()            # events of enqueued blocks
         reserved = 0.0
+        busy = 0.0                                # device time of the enqueued blocks
         peak_reserved = 0.0
         max_backlog = 0
         stream = torch.cuda.current_stream()
@@ -290,7 +291,7 @@ class ServingLoop(object):
                 r = waiting[0]
                 if r.need is None:
                     r.need = self._need(r.spec)
-                if reserved + r.need > self.hbm_budget and (running or preparing or ready):
+                if reserved + r.need > self.hbm_budget and (running or preparing or ready or retiring):
                     break
                 waiting.popleft()
                 reserved += r.need
@@ -298,7 +299,8 @@ class ServingLoop(object):
                 r.t_admit = now
                 r.future = self.preparer.submit(r.spec, self.precision)
                 preparing.append(r)
-            max_backlog = max(max_backlog, sum(1 for r in waiting if r.arrival <= now))
+            max_backlog = max(max_backlog, len(preparing) + len(ready) +
+                              sum(1 for r in waiting if r.arrival <= now))
             # 2. prepared scenes, in admission order
             while preparing and preparing[0].future.done():
                 r = preparing.popleft()
@@ -310,7 +312,7 @@ class ServingLoop(object):
                 r = ready.popleft()
                 rows = self.tuner.tile_rows_for(self.precision, (r.gen.surface.Nx, r.gen.surface.Ny,
                                                                  r.gen.npol * r.gen.num_ch)) if self.tuner else 0
-                r.slot = batch.add(r.gen.to_device(), tile_rows=rows)
+                r.slot = batch.add(r.gen, tile_rows=rows)
                 r.t_start = time.perf_counter() - t0
                 r.echoes = scene_echoes(r.gen)
                 running[r.slot] = r
@@ -331,12 +333,16 @@ class ServingLoop(object):
             live = batch.live()
             if live:
                 k = min(self.pulse_block, min(batch.remaining(s) for s in live))
+                b0 = torch.cuda.Event(enable_timing=True)
+                b0.record(stream)
                 batch.graph_step(k)
-                ev = torch.cuda.Event()
-                ev.record(stream)
-                inflight.append(ev)
+                b1 = torch.cuda.Event(enable_timing=True)
+                b1.record(stream)
+                inflight.append((b0, b1))
                 while len(inflight) > 2:            # keep the host at most two blocks ahead
-                    inflight.popleft().synchronize()
+                    e0, e1 = inflight.popleft()
+                    e1.synchronize()
+                    busy += e0.elapsed_time(e1) * 1e-3
             # 6. retired requests whose copy has landed
             still = []
             for r in retiring:
@@ -355,6 +361,8 @@ class ServingLoop(object):
                 if ready or preparing or (waiting and waiting[0].arrival > time.perf_counter() - t0):
                     time.sleep(0.0005)
         torch.cuda.synchronize()
+        for e0, e1 in inflight:
+            busy += e0.elapsed_time(e1) * 1e-3
         t_end = time.perf_counter() - t0
         batch.close()
         lat = np.array([r.t_done - r.arrival for r in reqs])
@@ -366,7 +374,11 @@ class ServingLoop(object):
                    offered_echoes_per_s=offered,
                    latency_p50_s=float(np.percentile(lat, 50)), latency_p99_s=float(np.percentile(lat, 99)),
                    latency_max_s=float(lat.max()), peak_reserved_bytes=peak_reserved, max_backlog=max_backlog,
-                   queue_stable=bool(offered <= (echoes / span if span > 0 else 0.0)))
+                   gpu_busy_s=busy, gpu_busy_frac=busy / span if span > 0 else 0.0,
+                   capacity_echoes_per_s=echoes / busy if busy > 0 else 0.0,
+                   # the queue is stable when the offered load is below what the GPU
+                   # sustains while it has work (echoes per busy second)
+                   queue_stable=bool(busy > 0 and offered < echoes / busy))
         self.requests = reqs
         return rep
 
