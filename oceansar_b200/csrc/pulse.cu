@@ -63,24 +63,97 @@ struct PulseArgs {
     int az_steps;
 };
 
-// Inputs of one facet, loaded one row ahead of use.
+// Asynchronous global -> shared copies (cp.async): each thread copies the words it will
+// read itself, so a cp.async.wait_group by that thread is all the ordering needed.
+OCS_D void cp_async(void *dst, const void *src, int bytes) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    if (bytes == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src) : "memory");
+    else if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+    else asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+OCS_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> OCS_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Staging of the per-facet inputs in shared memory: kStageRows rows of every input array
+// ([8] float32 fields, [4] sqrt(RCS) of type T, [2] int32 scatterer offsets, kPulseCols
+// columns each) in a ring, filled kStageRows - 1 rows ahead of use, and two slots of the
+// gathered scatterer-series values (complex128 of both Bragg lines), filled one row ahead.
+constexpr int kStageRows = 3;
+template <typename T> OCS_HD constexpr size_t stage_slot_bytes() {
+    return (8 * 4 + 4 * sizeof(T) + 2 * 4) * (size_t)kPulseCols;
+}
+template <typename T> OCS_HD constexpr size_t stage_bytes() {
+    return kStageRows * stage_slot_bytes<T>() + 2 * 2 * 16 * (size_t)kPulseCols + 16;
+}
+
+template <typename T> struct Stage {
+    unsigned char *base;          // 16-byte aligned
+    OCS_D float *f(int slot, int k) const {
+        return reinterpret_cast<float *>(base + slot * stage_slot_bytes<T>()) + k * kPulseCols + threadIdx.x;
+    }
+    OCS_D T *scat(int slot, int k) const {
+        return reinterpret_cast<T *>(base + slot * stage_slot_bytes<T>() + 32 * kPulseCols) + k * kPulseCols +
+               threadIdx.x;
+    }
+    OCS_D int *ind(int slot, int k) const {
+        return reinterpret_cast<int *>(base + slot * stage_slot_bytes<T>() + (32 + 4 * sizeof(T)) * kPulseCols) +
+               k * kPulseCols + threadIdx.x;
+    }
+    OCS_D double2 *gather(int g, int k) const {
+        return reinterpret_cast<double2 *>(base + kStageRows * stage_slot_bytes<T>()) + (2 * g + k) * kPulseCols +
+               threadIdx.x;
+    }
+};
+
+// Inputs of one facet.
 template <typename T> struct FacetIn {
     float dx, dy, dz, diffx, diffy, diffxx, diffyy, diffxy;
     T scat[2][2];
-    int ind0_m, ind0_p;
+    // start the copies of facet idx's inputs into stage slot `slot`
     template <typename A>
-    OCS_D void load(const A &a, long long idx, long long npix, const T *scat_buf, bool load_scat) {
-        dx = a.dx_f[idx];
-        dy = a.dy_f[idx];
-        dz = a.dz_f[idx];
-        if (a.diffx) { diffx = a.diffx[idx]; diffy = a.diffy[idx]; }
-        if (a.do_kodis) { diffxx = a.diffxx[idx]; diffyy = a.diffyy[idx]; diffxy = a.diffxy[idx]; }
-        if (a.do_bragg) { ind0_m = a.ind0_m[idx]; ind0_p = a.ind0_p[idx]; }
+    static OCS_D void issue(const A &a, const Stage<T> &st, int slot, long long idx, long long npix,
+                            const T *scat_buf, bool load_scat) {
+        cp_async(st.f(slot, 0), a.dx_f + idx, 4);
+        cp_async(st.f(slot, 1), a.dy_f + idx, 4);
+        cp_async(st.f(slot, 2), a.dz_f + idx, 4);
+        if (a.diffx) {
+            cp_async(st.f(slot, 3), a.diffx + idx, 4);
+            cp_async(st.f(slot, 4), a.diffy + idx, 4);
+        }
+        if (a.do_kodis) {
+            cp_async(st.f(slot, 5), a.diffxx + idx, 4);
+            cp_async(st.f(slot, 6), a.diffyy + idx, 4);
+            cp_async(st.f(slot, 7), a.diffxy + idx, 4);
+        }
+        if (a.do_bragg) {
+            cp_async(st.ind(slot, 0), a.ind0_m + idx, 4);
+            cp_async(st.ind(slot, 1), a.ind0_p + idx, 4);
+        }
+        if (load_scat)
+            for (int k = 0; k < 2 * a.npol; ++k) cp_async(st.scat(slot, k), scat_buf + k * npix + idx, sizeof(T));
+    }
+    // start the gathers of the scatterer-series values of the facet staged in `slot`
+    template <typename A>
+    static OCS_D void issue_gather(const A &a, const Stage<T> &st, int slot, int g) {
+        int i0 = *st.ind(slot, 0) + a.tmod_m;
+        i0 = i0 >= a.n_m ? i0 - a.n_m : i0;
+        int i1 = *st.ind(slot, 1) + a.tmod_p;
+        i1 = i1 >= a.n_p ? i1 - a.n_p : i1;
+        cp_async(st.gather(g, 0), a.s_m + 2 * (long long)i0, 16);
+        cp_async(st.gather(g, 1), a.s_p + 2 * (long long)i1, 16);
+    }
+    template <typename A>
+    OCS_D void read(const A &a, const Stage<T> &st, int slot, bool load_scat) {
+        dx = *st.f(slot, 0);
+        dy = *st.f(slot, 1);
+        dz = *st.f(slot, 2);
+        if (a.diffx) { diffx = *st.f(slot, 3); diffy = *st.f(slot, 4); }
+        if (a.do_kodis) { diffxx = *st.f(slot, 5); diffyy = *st.f(slot, 6); diffxy = *st.f(slot, 7); }
 #pragma unroll
         for (int p = 0; p < 2; ++p) {
             if (load_scat && p < a.npol) {
-                scat[p][0] = scat_buf[(2 * p) * npix + idx];
-                scat[p][1] = scat_buf[(2 * p + 1) * npix + idx];
+                scat[p][0] = *st.scat(slot, 2 * p);
+                scat[p][1] = *st.scat(slot, 2 * p + 1);
             } else {
                 scat[p][0] = (T)0;
                 scat[p][1] = (T)0;
@@ -146,12 +219,14 @@ template <typename T> struct PulseSmem {
     double *r_az;
     cplx<T> *r_fac;
     double *sred;
+    Stage<T> stage;
 };
 
 template <typename T, int NOUT, int S, int RCAP>
 OCS_HD constexpr size_t pulse_smem_bytes(int nch) {
     return (size_t)wtab_len<T, S>(kSincTaps, kSincOvs) * sizeof(T) + (size_t)NOUT * kPulseNbw * 2 * sizeof(T) +
-           5 * RCAP * sizeof(double) + (size_t)RCAP * nch * sizeof(cplx<T>) + 32 * sizeof(double);
+           5 * RCAP * sizeof(double) + (size_t)RCAP * nch * sizeof(cplx<T>) + 32 * sizeof(double) +
+           stage_bytes<T>();
 }
 
 template <typename T, int NOUT, int S, int RCAP>
@@ -162,6 +237,8 @@ OCS_D PulseSmem<T> pulse_smem(unsigned char *smem, int nch) {
     sm.r_az = reinterpret_cast<double *>(sm.bins + NOUT * kPulseNbw * 2);
     sm.r_fac = reinterpret_cast<cplx<T> *>(sm.r_az + 5 * RCAP);            // [rows][nch]
     sm.sred = reinterpret_cast<double *>(sm.r_fac + RCAP * nch);
+    const size_t st = reinterpret_cast<size_t>(sm.sred + 32);
+    sm.stage.base = reinterpret_cast<unsigned char *>((st + 15) & ~(size_t)15);
     return sm;
 }
 
@@ -217,12 +294,30 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
         const long long npix = (long long)a.nx * a.ny;
         T *scat = reinterpret_cast<T *>(a.scat);
         const bool load_scat = a.do_bragg && !a.refresh;
-        // software pipeline: the inputs of row i+1 are loaded while row i is processed
-        FacetIn<T> cur, nxt;
-        cur.load(a, (long long)y0 * a.nx + x, npix, scat, load_scat);
+        // software pipeline through shared memory: the inputs of row i + kStageRows - 1 and
+        // the scatterer-series gathers of row i + 1 are in flight while row i is processed
+        const Stage<T> &st = sm.stage;
+        const long long idx0 = (long long)y0 * a.nx + x;
+        for (int r = 0; r < kStageRows - 1; ++r) {
+            if (r < nrows) FacetIn<T>::issue(a, st, r, idx0 + (long long)r * a.nx, npix, scat, load_scat);
+            cp_async_commit();
+        }
+        cp_async_wait<kStageRows - 2>();
+        if (a.do_bragg) FacetIn<T>::issue_gather(a, st, 0, 0);
+        cp_async_commit();
+        FacetIn<T> cur;
         for (int i = 0; i < nrows; ++i) {
-            const long long idx = (long long)(y0 + i) * a.nx + x;
-            if (i + 1 < nrows) nxt.load(a, idx + a.nx, npix, scat, load_scat);
+            const long long idx = idx0 + (long long)i * a.nx;
+            {
+                const int r = i + kStageRows - 1;
+                if (r < nrows) FacetIn<T>::issue(a, st, r % kStageRows, idx0 + (long long)r * a.nx, npix, scat,
+                                                 load_scat);
+                cp_async_commit();
+            }
+            cp_async_wait<1>();                 // rows <= i + 1 and the gathers of row i have landed
+            if (a.do_bragg && i + 1 < nrows) FacetIn<T>::issue_gather(a, st, (i + 1) % kStageRows, (i + 1) & 1);
+            cp_async_commit();
+            cur.read(a, st, i % kStageRows, load_scat);
             const double az = sm.r_az[i], sin_az = sm.r_az[RCAP + i];
             // slant range: sr - cos_inc*Dz + az/2*sin_az + Dx*sin_inc + Dy*sin_az, float64,
             // left to right, no fused multiply-adds (bit-identical with numpy)
@@ -288,12 +383,8 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
                     e0 = {(T)c0, (T)s0};
                     e1 = {(T)c1, (T)s1};
                 }
-                int i0 = cur.ind0_m + a.tmod_m;
-                i0 = i0 >= a.n_m ? i0 - a.n_m : i0;
-                int i1 = cur.ind0_p + a.tmod_p;
-                i1 = i1 >= a.n_p ? i1 - a.n_p : i1;
-                const double2 smd = reinterpret_cast<const double2 *>(a.s_m)[i0];
-                const double2 spd = reinterpret_cast<const double2 *>(a.s_p)[i1];
+                const double2 smd = *st.gather(i & 1, 0);
+                const double2 spd = *st.gather(i & 1, 1);
                 const cplx<T> sm = {(T)smd.x, (T)smd.y};
                 const cplx<T> sp = {(T)spd.x, (T)spd.y};
 #pragma unroll
@@ -326,8 +417,8 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
             }
             if (bin_d > -(1 << 29))
                 win.add(bin_d - kSincTaps / 2, lut, coef, sm.wtab, a.sinc, kSincTaps, kSincOvs, cb);
-            cur = nxt;
         }
+        cp_async_wait<0>();
     }
     win.flush(cb);
     __syncthreads();
