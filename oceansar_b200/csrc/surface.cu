@@ -507,9 +507,9 @@ static cudaError_t launch_cols(const SurfaceArgs &a, cudaStream_t st) {
         case 64: return launch_cols_n<64, 4>(a, st);
         case 128: return launch_cols_n<128, 4>(a, st);
         case 256: return launch_cols_n<256, 4>(a, st);
-        case 512: return launch_cols_n<512, 4>(a, st);
-        case 1024: return launch_cols_n<1024, 4>(a, st);
-        case 2048: return launch_cols_n<2048, 4>(a, st);
+        case 512: return launch_cols_n<512, 8>(a, st);
+        case 1024: return launch_cols_n<1024, 8>(a, st);
+        case 2048: return launch_cols_n<2048, 8>(a, st);
         case 4096: return launch_cols_n<4096, 4>(a, st);
         case 8192: return launch_cols_n<8192, 2>(a, st);
         default: return launch_cols_n<0, 4>(a, st);
@@ -618,7 +618,11 @@ int surface_key(int n) {
     }
 }
 
-int surface_cols_tile(int key) { return key == 8192 ? 2 : 4; }
+// Column tile width per column length: wider tiles give longer contiguous row segments
+// (loads of TILE complex64, stores of TILE float32 per row) where shared memory allows.
+int surface_cols_tile(int key) {
+    return key == 8192 ? 2 : ((key == 512 || key == 1024 || key == 2048) ? 8 : 4);
+}
 
 long long surface_rows_smem(int key, int nx) {
     const size_t b = rows_smem_bytes(key, nx);
@@ -652,9 +656,9 @@ int batch_launch_cols(const BatchRef &b, int key, int grid, size_t smem, cudaStr
         case 64: return batch_cols_n<64, 4>(b, grid, smem, st);
         case 128: return batch_cols_n<128, 4>(b, grid, smem, st);
         case 256: return batch_cols_n<256, 4>(b, grid, smem, st);
-        case 512: return batch_cols_n<512, 4>(b, grid, smem, st);
-        case 1024: return batch_cols_n<1024, 4>(b, grid, smem, st);
-        case 2048: return batch_cols_n<2048, 4>(b, grid, smem, st);
+        case 512: return batch_cols_n<512, 8>(b, grid, smem, st);
+        case 1024: return batch_cols_n<1024, 8>(b, grid, smem, st);
+        case 2048: return batch_cols_n<2048, 8>(b, grid, smem, st);
         case 4096: return batch_cols_n<4096, 4>(b, grid, smem, st);
         case 8192: return batch_cols_n<8192, 2>(b, grid, smem, st);
         case 0: return batch_cols_n<0, 4>(b, grid, smem, st);

@@ -60,6 +60,8 @@ def test_golden_surfaces(name):
 @pytest.mark.parametrize("n,compute,choppy", [
     (512, ['D', 'Diff', 'Diff2'], False),
     (2048, ['D', 'Diff', 'Diff2', 'hMTF'], False),
+    (2048, ['D', 'Diff', 'Diff2'], False),
+    (1024, ['D', 'Diff'], False),
     (256, ['D', 'Diff', 'Diff2', 'V', 'A'], True),
     (96, ['D', 'Diff', 'Diff2'], False),
 ])
