@@ -63,6 +63,21 @@ int ocs_chan_profile_c64(const double *srg_d, const float *scene_d, int64_t npts
                          int n_sinc_samples, int sinc_ovs, float *output_d, int64_t nbins,
                          void *stream);
 
+/* ocs_chan_profile_f64 for facets laid out as a [ny][nx] surface (azimuth rows, ground-
+ * range columns; the order sar_raw flattens them in, sar_raw_nompi.py:535): the same sum
+ * into output[nbins], computed column-wise so that each thread's range bin barely moves.
+ * Replaces chan_profile_numba (range_profile.py:83-116) when the caller keeps the 2-D
+ * shape; the result equals ocs_chan_profile_f64 on the flattened arrays up to summation
+ * order.  _c64: the single-precision scene / output form (no reference counterpart). */
+int ocs_chan_profile_2d_f64(const double *srg_d, const double *scene_d, int64_t ny, int64_t nx,
+                            double binsize, double min_sr, const float *sinc_vec_d,
+                            int n_sinc_samples, int sinc_ovs, double *output_d, int64_t nbins,
+                            void *stream);
+int ocs_chan_profile_2d_c64(const double *srg_d, const float *scene_d, int64_t ny, int64_t nx,
+                            double binsize, double min_sr, const float *sinc_vec_d,
+                            int n_sinc_samples, int sinc_ovs, float *output_d, int64_t nbins,
+                            void *stream);
+
 
 /* ------------------------------------------------------------------------------------
  * Per-pulse surface synthesis.

@@ -33,6 +33,10 @@ SIGNATURES = {
     "ocs_chan_profile_rows_f64": [c_ptr, c_ptr, c_i64, c_i64, c_dbl, c_dbl, c_ptr, c_int, c_int, c_ptr,
                                   c_i64, c_ptr],
     "ocs_chan_profile_c64": [c_ptr, c_ptr, c_i64, c_dbl, c_dbl, c_ptr, c_int, c_int, c_ptr, c_i64, c_ptr],
+    "ocs_chan_profile_2d_f64": [c_ptr, c_ptr, c_i64, c_i64, c_dbl, c_dbl, c_ptr, c_int, c_int, c_ptr, c_i64,
+                                c_ptr],
+    "ocs_chan_profile_2d_c64": [c_ptr, c_ptr, c_i64, c_i64, c_dbl, c_dbl, c_ptr, c_int, c_int, c_ptr, c_i64,
+                                c_ptr],
     "ocs_surface_workspace_bytes": [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32],
     "ocs_surface_prepare": [ctypes.c_int32, ctypes.c_int32, c_ptr, c_ptr],
     "ocs_surface_update": [c_ptr, c_flt, c_ptr],

@@ -101,6 +101,124 @@ static int launch_chan_profile(const double *srg, const void *scene, long long n
     return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
 }
 
+// ---------------------------------------------------------------------------------------
+// Two-dimensional layout: the facets are a [ny][nx] surface (rows = azimuth, columns =
+// ground range), as sar_raw flattens them.  A CTA takes a tile of kC2Cols columns x
+// kC2Rows rows; a thread owns one column and walks down the rows, so a warp reads 32
+// consecutive facets of a row (coalesced) and every thread's range bin drifts only with
+// the azimuth curvature and the surface displacement -- its register window almost never
+// moves.  The inputs of each row are staged in shared memory two rows ahead with cp.async
+// (each thread copies, and later reads, only its own words).
+constexpr int kC2Cols = 128;
+constexpr int kC2Rows = 64;
+constexpr int kC2Stage = 3;
+constexpr int kC2Nbw = 256;
+
+template <typename T> OCS_HD constexpr size_t c2_stage_bytes() {
+    return (size_t)kC2Stage * kC2Cols * (sizeof(double) + sizeof(cplx<T>));
+}
+
+template <typename T, int S>
+__global__ void __launch_bounds__(kC2Cols, 4)
+chan_profile_2d_kernel(const double *__restrict__ srg, const cplx<T> *__restrict__ scene, int ny, int nx,
+                       double binsize, double min_sr, const float *__restrict__ sinc, int taps, int ovs,
+                       T *__restrict__ out, int nbins) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T *wtab = reinterpret_cast<T *>(smem_raw);
+    const int wlen = wtab_len<T, S>(taps, ovs);
+    T *acc = wtab + ((wlen + 3) & ~3);
+    double *st_srg = reinterpret_cast<double *>(
+        (reinterpret_cast<size_t>(acc + 2 * kC2Nbw) + 15) & ~(size_t)15);          // [kC2Stage][kC2Cols]
+    cplx<T> *st_sc = reinterpret_cast<cplx<T> *>(st_srg + kC2Stage * kC2Cols);      // [kC2Stage][kC2Cols]
+
+    const int tiles_x = (nx + kC2Cols - 1) / kC2Cols;
+    const int x0 = (blockIdx.x % tiles_x) * kC2Cols;
+    const int y0 = (blockIdx.x / tiles_x) * kC2Rows;
+    const int x = x0 + threadIdx.x;
+    const int nrows = min(kC2Rows, ny - y0);
+
+    build_wtab<T, S>(wtab, sinc, taps, ovs);
+    CtaBins<T, 1> cb;
+    cb.acc = acc;
+    cb.nbw = kC2Nbw;
+    cb.nout = 1;
+    cb.nbins = nbins;
+    cb.out = out;
+    cb.out_stride = 0;
+    {
+        int b0, l0;
+        bin_and_lut(srg[(long long)y0 * nx + x0], min_sr, binsize, ovs, b0, l0);
+        cb.cta_base = (b0 > -(1 << 29)) ? b0 - kC2Nbw / 4 : 0;
+    }
+    cb.zero();
+    __syncthreads();
+
+    BinWindow<T, S, 1> win;
+    win.reset();
+    if (x < nx) {
+        const long long idx0 = (long long)y0 * nx + x;
+        auto issue = [&](int r) {
+            if (r < nrows) {
+                const long long g = idx0 + (long long)r * nx;
+                const int slot = (r % kC2Stage) * kC2Cols + threadIdx.x;
+                const unsigned d0 = (unsigned)__cvta_generic_to_shared(st_srg + slot);
+                const unsigned d1 = (unsigned)__cvta_generic_to_shared(st_sc + slot);
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d0), "l"(srg + g) : "memory");
+                if (sizeof(cplx<T>) == 8)
+                    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d1), "l"(scene + g) : "memory");
+                else
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d1), "l"(scene + g) : "memory");
+            }
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
+        };
+        for (int r = 0; r < kC2Stage - 1; ++r) issue(r);
+        const int half = taps / 2;
+        for (int i = 0; i < nrows; ++i) {
+            issue(i + kC2Stage - 1);
+            asm volatile("cp.async.wait_group %0;\n" ::"n"(kC2Stage - 1) : "memory");
+            const int slot = (i % kC2Stage) * kC2Cols + threadIdx.x;
+            int bin_d, lut;
+            bin_and_lut(st_srg[slot], min_sr, binsize, ovs, bin_d, lut);
+            if (bin_d < -(1 << 29)) continue;
+            cplx<T> c[1] = {st_sc[slot]};
+            win.add(bin_d - half, lut, c, wtab, sinc, taps, ovs, cb);
+        }
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    }
+    win.flush(cb);
+    __syncthreads();
+    cb.flush_to_global();
+}
+
+template <typename T, int S>
+static int launch_chan_profile_2d(const double *srg, const void *scene, long long ny, long long nx, double binsize,
+                                  double min_sr, const float *sinc, int taps, int ovs, T *out, int nbins,
+                                  cudaStream_t stream) {
+    if (taps < 1 || taps > S || ovs < 1 || ny < 0 || nx < 0 || nbins < 0) return OCS_ERR_ARG;
+    if (ny == 0 || nx == 0 || nbins == 0) return OCS_OK;
+    if (ny > 0x7fffffffLL || nx > 0x7fffffffLL) return OCS_ERR_SIZE;
+    const int wlen = wtab_len<T, S>(taps, ovs);
+    const size_t smem = (size_t)((wlen + 3) & ~3) * sizeof(T) + (size_t)kC2Nbw * 2 * sizeof(T) + 16 +
+                        c2_stage_bytes<T>();
+    const long long grid = ((nx + kC2Cols - 1) / kC2Cols) * ((ny + kC2Rows - 1) / kC2Rows);
+    if (grid > 0x7fffffffLL) return OCS_ERR_SIZE;
+    auto kern = chan_profile_2d_kernel<T, S>;
+    if (ensure_smem((const void *)kern, smem) != cudaSuccess) return OCS_ERR_CUDA;
+    kern<<<(unsigned)grid, kC2Cols, smem, stream>>>(srg, reinterpret_cast<const cplx<T> *>(scene), (int)ny, (int)nx,
+                                                      binsize, min_sr, sinc, taps, ovs, out, nbins);
+    return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
+}
+
+template <typename T>
+static int launch_chan_profile_2d_any(const double *srg, const void *scene, long long ny, long long nx,
+                                      double binsize, double min_sr, const float *sinc, int taps, int ovs, T *out,
+                                      int nbins, cudaStream_t stream) {
+    if (taps <= 8)
+        return launch_chan_profile_2d<T, 12>(srg, scene, ny, nx, binsize, min_sr, sinc, taps, ovs, out, nbins,
+                                             stream);
+    return launch_chan_profile_2d<T, 16>(srg, scene, ny, nx, binsize, min_sr, sinc, taps, ovs, out, nbins, stream);
+}
+
 }  // namespace ocs
 
 extern "C" int ocs_chan_profile_f64(const double *srg, const double *scene, int64_t npts,
@@ -140,4 +258,26 @@ extern "C" int ocs_chan_profile_c64(const double *srg, const float *scene, int64
     return ocs::launch_chan_profile<float, 16>(srg, scene, 1, npts, binsize, min_sr, sinc_vec,
                                                n_sinc_samples, sinc_ovs, output, (int)nbins,
                                                (cudaStream_t)stream);
+}
+
+extern "C" int ocs_chan_profile_2d_f64(const double *srg, const double *scene, int64_t ny, int64_t nx,
+                                       double binsize, double min_sr, const float *sinc_vec, int n_sinc_samples,
+                                       int sinc_ovs, double *output, int64_t nbins, void *stream) {
+    if (ny < 0 || nx < 0 || nbins < 0) return OCS_ERR_ARG;
+    if (ny == 0 || nx == 0 || nbins == 0) return OCS_OK;
+    if (!srg || !scene || !sinc_vec || !output) return OCS_ERR_ARG;
+    if (nbins > 0x3fffffff) return OCS_ERR_SIZE;
+    return ocs::launch_chan_profile_2d_any<double>(srg, scene, ny, nx, binsize, min_sr, sinc_vec, n_sinc_samples,
+                                                   sinc_ovs, output, (int)nbins, (cudaStream_t)stream);
+}
+
+extern "C" int ocs_chan_profile_2d_c64(const double *srg, const float *scene, int64_t ny, int64_t nx,
+                                       double binsize, double min_sr, const float *sinc_vec, int n_sinc_samples,
+                                       int sinc_ovs, float *output, int64_t nbins, void *stream) {
+    if (ny < 0 || nx < 0 || nbins < 0) return OCS_ERR_ARG;
+    if (ny == 0 || nx == 0 || nbins == 0) return OCS_OK;
+    if (!srg || !scene || !sinc_vec || !output) return OCS_ERR_ARG;
+    if (nbins > 0x3fffffff) return OCS_ERR_SIZE;
+    return ocs::launch_chan_profile_2d_any<float>(srg, scene, ny, nx, binsize, min_sr, sinc_vec, n_sinc_samples,
+                                                  sinc_ovs, output, (int)nbins, (cudaStream_t)stream);
 }

@@ -23,9 +23,10 @@ def chan_profile_numba(srg, scene, binsize, min_sr, sinc_vec, n_sinc_samples, si
                        rg_only=False, stream=None):
     """``output += range profile of (srg, scene)``; see ``include/oceansar_b200.h``.
 
-    ``srg``/``scene``: float64 / complex128 of the same shape (flattened unless
-    ``rg_only``; [naz, npts] with ``rg_only``); ``output``: complex128 [nbins] (or
-    [naz, nbins]) numpy array or CUDA tensor, updated in place.
+    ``srg``/``scene``: float64 / complex128 of the same shape: flattened, or a 2-D
+    [ny, nx] surface (summed column-wise by ``ocs_chan_profile_2d_f64``; same result up to
+    summation order), or [naz, npts] rows with ``rg_only``; ``output``: complex128 [nbins]
+    (or [naz, nbins]) numpy array or CUDA tensor, updated in place.
     """
     n_sinc_samples = int(n_sinc_samples)
     sinc_ovs = int(sinc_ovs)
@@ -52,6 +53,11 @@ def chan_profile_numba(srg, scene, binsize, min_sr, sinc_vec, n_sinc_samples, si
         _capi.call("ocs_chan_profile_rows_f64", _device.ptr(srg_d), _device.ptr(scene_d), naz, npts,
                    float(binsize), float(min_sr), _device.ptr(sinc_d), n_sinc_samples, sinc_ovs,
                    _device.ptr(out_d), out_d.shape[1], sp)
+    elif srg_d.dim() == 2:
+        # a [ny][nx] surface: the column-walking kernel (same sum, other summation order)
+        _capi.call("ocs_chan_profile_2d_f64", _device.ptr(srg_d), _device.ptr(scene_d), srg_d.shape[0],
+                   srg_d.shape[1], float(binsize), float(min_sr), _device.ptr(sinc_d), n_sinc_samples,
+                   sinc_ovs, _device.ptr(out_d), out_d.numel(), sp)
     else:
         _capi.call("ocs_chan_profile_f64", _device.ptr(srg_d), _device.ptr(scene_d), srg_d.numel(),
                    float(binsize), float(min_sr), _device.ptr(sinc_d), n_sinc_samples, sinc_ovs,

@@ -129,3 +129,42 @@ def test_single_precision_kernel():
     _capi.call("ocs_chan_profile_c64", _device.ptr(srg_d), _device.ptr(sc_d), srg.size, 2.725, 0.0,
                _device.ptr(sinc_d), 8, 20, _device.ptr(out_d), 160, _device.stream_ptr())
     assert rel(out_d.cpu().numpy(), ref) < 1e-5
+
+
+@pytest.mark.parametrize("shape", [(64, 64, 32), (97, 300, 90), (1024, 2048, 512), (5, 7, 16)])
+def test_two_dimensional_layout(shape):
+    """The [ny, nx] column-walking kernel gives the flattened sum (edges: ragged tiles,
+    bins outside [0, nbins), a non-finite facet)."""
+    from oceansar_b200.radarsim import range_profile as rp
+    ny, nx, nbins = shape
+    srg, scene = _synthetic(ny, nx, nbins, 5)
+    srg = srg - 3.0                                     # some facets fall below bin 0
+    scene[len(scene) // 3] = np.nan + 0j
+    sinc = rp.calc_sinc_vec(8, 20, Fs=1.1)
+    ref = np.zeros(nbins, complex)
+    orp.chan_profile(srg, scene, 2.725, 0.0, sinc, 8, 20, ref)
+    out = np.zeros(nbins, complex)
+    rp.chan_profile_numba(srg.reshape(ny, nx), scene.reshape(ny, nx), 2.725, 0.0, sinc, 8, 20, out)
+    fin = np.isfinite(ref)
+    assert np.array_equal(fin, np.isfinite(out))
+    assert rel(out[fin], ref[fin]) < 1e-10
+
+
+def test_two_dimensional_c64():
+    import ctypes
+    from oceansar_b200 import _capi
+    from oceansar_b200.radarsim import range_profile as rp
+    ny, nx, nbins = 300, 700, 200
+    srg, scene = _synthetic(ny, nx, nbins, 6)
+    sinc = rp.calc_sinc_vec(8, 20, Fs=1.1)
+    ref = np.zeros(nbins, complex)
+    orp.chan_profile(srg, scene, 2.725, 0.0, sinc, 8, 20, ref)
+    s_d = torch.tensor(srg, dtype=torch.float64, device="cuda")
+    c_d = torch.tensor(np.stack([scene.real, scene.imag], -1), dtype=torch.float32, device="cuda")
+    w_d = torch.tensor(sinc, dtype=torch.float32, device="cuda")
+    o_d = torch.zeros(nbins, 2, dtype=torch.float32, device="cuda")
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _capi.call("ocs_chan_profile_2d_c64", s_d.data_ptr(), c_d.data_ptr(), ny, nx, 2.725, 0.0, w_d.data_ptr(), 8, 20,
+               o_d.data_ptr(), nbins, st)
+    out = o_d.cpu().numpy().astype(np.float64)
+    assert rel(out[:, 0] + 1j * out[:, 1], ref) < 1e-5
