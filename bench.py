@@ -225,6 +225,52 @@ def run_reference(args, c, cfg_path):
     print(json.dumps(line), flush=True)
 
 
+def accumulation_roofline(peak, peak_src, n=4096, nbins=2048, reps=10):
+    """Standalone facet-to-bin accumulation (``ocs_chan_profile_2d_c64`` / ``_f64``) on a
+    seeded n x n surface layout (slant range along the columns, azimuth curvature along the
+    rows, 1 m jitter): algorithmic bytes = range (8 B) + scene (8 B c64 / 16 B c128) per
+    facet; inputs (268 / 403 MB) exceed the L2."""
+    import ctypes
+    import torch
+    from oceansar_b200 import _capi
+    from oceansar_b200.radarsim.range_profile import calc_sinc_vec
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.arange(n, device="cuda", dtype=torch.float64)
+    y = x - n / 2
+    sr0 = 627e3
+    srg = (sr0 + x[None, :] * np.sin(np.radians(35.0)) + (y[:, None] + 3000.0) ** 2 / (2 * sr0) +
+           torch.randn(n, n, generator=g, device="cuda", dtype=torch.float64)).contiguous()
+    binsize = 2.99792458e8 / (2 * 50e6) / 1.1
+    min_sr = float(srg.min()) - 10.0
+    sinc = torch.tensor(calc_sinc_vec(8, 20, Fs=1.1), dtype=torch.float32, device="cuda")
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    lib = _capi.load()
+    out = {}
+    for name, fn, dt, bpf in (("c64", lib.ocs_chan_profile_2d_c64, torch.float32, 16),
+                              ("f64", lib.ocs_chan_profile_2d_f64, torch.float64, 24)):
+        sc = torch.randn(n, n, 2, generator=g, device="cuda", dtype=torch.float64).to(dt)
+        o = torch.zeros(nbins, 2, device="cuda", dtype=dt)
+        call = lambda: fn(srg.data_ptr(), sc.data_ptr(), n, n, binsize, min_sr, sinc.data_ptr(), 8, 20,  # noqa: E731
+                          o.data_ptr(), nbins, st)
+        for _ in range(3):
+            assert call() == 0
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            call()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        gbs = n * n * bpf / (ms * 1e-3) / 1e9
+        out[name] = {"ms": round(ms, 4), "facets_per_s": n * n / (ms * 1e-3), "GBps": round(gbs, 1),
+                     "frac": round(gbs / peak, 4), "alg_bytes_per_facet": bpf}
+        del sc, o
+    out.update({"kernel": "chan_profile_2d_kernel", "grid": [n, n], "nbins": nbins, "peak": peak,
+                "peak_source": peak_src, "bound": "hbm"})
+    return out
+
+
 # ----------------------------------------------------------------------------------------
 # Batched and serving workloads (one GPU; replicas for N > 1 as for the default workload)
 def _workload_reference(args, specs, what):
@@ -398,11 +444,21 @@ def main():
     ap.add_argument("--rate", type=float, default=20.0, help="serving: requests per second")
     ap.add_argument("--duration", type=float, default=5.0, help="serving: seconds of arrivals")
     ap.add_argument("--workers", type=int, default=None, help="host set-up worker processes")
+    ap.add_argument("--accumulation-only", action="store_true",
+                    help="time only the standalone accumulation kernels and print their line")
     ap.add_argument("--profile-pulses", type=int, default=0,
                     help="run this many pulses with plain launches (for ncu) and exit")
     args = ap.parse_args()
     if args.workload != "c2":
         run_workload(args)
+        return
+    if args.accumulation_only:
+        import torch
+        torch.cuda.set_device(dist_info()[2])
+        peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+        peak, src = ((json.load(open(peaks_path))["hbm_gbs"], "measured") if os.path.exists(peaks_path)
+                     else (6650.0, "fallback"))
+        print(json.dumps({"accumulation": accumulation_roofline(peak, src)}), flush=True)
         return
     c = C1 if args.small else C2
     tmpd = tempfile.mkdtemp(prefix="ocs_bench_")
@@ -553,6 +609,11 @@ def main():
         del g64
         torch.cuda.empty_cache()
 
+    # ---- standalone accumulation (chan_profile drop-in, [ny][nx] layout) -------------------
+    accum = None
+    if not args.small:
+        accum = accumulation_roofline(peak, peak_src)
+
     # ---- CPU baseline (oracle port) -------------------------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -573,7 +634,7 @@ def main():
                            "l2": "inputs larger than L2 (~0.5 GB working set)",
                            "graph": "whole scene replayed from one CUDA graph"},
                 "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
-                "cpu_baseline": cpu, "fp64": fp64}
+                "cpu_baseline": cpu, "fp64": fp64, "accumulation": accum}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -136,6 +136,7 @@ chan_profile_2d_kernel(const double *__restrict__ srg, const cplx<T> *__restrict
     const int y0 = (blockIdx.x / tiles_x) * kC2Rows;
     const int x = x0 + threadIdx.x;
     const int nrows = min(kC2Rows, ny - y0);
+    const double inv_binsize = 1.0 / binsize;
 
     build_wtab<T, S>(wtab, sinc, taps, ovs);
     CtaBins<T, 1> cb;
@@ -178,7 +179,10 @@ chan_profile_2d_kernel(const double *__restrict__ srg, const cplx<T> *__restrict
             asm volatile("cp.async.wait_group %0;\n" ::"n"(kC2Stage - 1) : "memory");
             const int slot = (i % kC2Stage) * kC2Cols + threadIdx.x;
             int bin_d, lut;
-            bin_and_lut(st_srg[slot], min_sr, binsize, ovs, bin_d, lut);
+            // FP64: IEEE division, bin / LUT bit-identical with numpy; single precision:
+            // reciprocal multiply (a one-ulp difference in the bin coordinate)
+            if (sizeof(T) == 8) bin_and_lut(st_srg[slot], min_sr, binsize, ovs, bin_d, lut);
+            else bin_and_lut_fast(st_srg[slot], min_sr, inv_binsize, ovs, bin_d, lut);
             if (bin_d < -(1 << 29)) continue;
             cplx<T> c[1] = {st_sc[slot]};
             win.add(bin_d - half, lut, c, wtab, sinc, taps, ovs, cb);

@@ -61,6 +61,7 @@ struct PulseArgs {
     double *nrcs_spec;                      // [az_steps]  sum |E_spec|^2
     double *nrcs_bragg;                     // [npol][az_steps] sum RCS (refresh pulses)
     int az_steps;
+    int tile_rows;                          // rows per tile of a single-scene launch
 };
 
 // Asynchronous global -> shared copies (cp.async): each thread copies the words it will
@@ -442,11 +443,11 @@ pulse_kernel(const __grid_constant__ PulseArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const PulseSmem<T> sm = pulse_smem<T, NOUT, S, kPulseRows>(smem, a.nch);
     build_wtab<T, S>(sm.wtab, a.sinc, kSincTaps, kSincOvs);
-    const int tiles = ((a.nx + kPulseCols - 1) / kPulseCols) * ((a.ny + kPulseRows - 1) / kPulseRows);
+    const int tiles = ((a.nx + kPulseCols - 1) / kPulseCols) * ((a.ny + a.tile_rows - 1) / a.tile_rows);
     double spec_sum = 0.0, bragg_sum[2] = {0.0, 0.0};
-    // persistent CTAs: each walks tiles of kPulseCols columns x kPulseRows rows
+    // persistent CTAs: each walks tiles of kPulseCols columns x tile_rows rows
     for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x)
-        pulse_tile<T, NOUT, S, kPulseRows>(a, tile, kPulseRows, sm, spec_sum, bragg_sum);
+        pulse_tile<T, NOUT, S, kPulseRows>(a, tile, a.tile_rows, sm, spec_sum, bragg_sum);
     pulse_nrcs<T>(a, sm, spec_sum, bragg_sum);
 }
 
@@ -536,14 +537,23 @@ batch_pulse_kernel(const __grid_constant__ BatchRef b) {
 }
 
 template <typename T, int NOUT, int S>
-static int launch_pulse(const PulseArgs &a, cudaStream_t st) {
+static int launch_pulse(PulseArgs a, cudaStream_t st) {
     const size_t smem = pulse_smem_bytes<T, NOUT, S, kPulseRows>(a.nch);
     auto k = pulse_kernel<T, NOUT, S>;
     if (ensure_smem((const void *)k, smem) != cudaSuccess)
         return OCS_ERR_CUDA;
-    const long long tiles = (long long)((a.nx + kPulseCols - 1) / kPulseCols) * ((a.ny + kPulseRows - 1) / kPulseRows);
     const int resident = resident_ctas((const void *)k, kPulseCols, smem);
     if (resident <= 0) return OCS_ERR_CUDA;
+    // Tile height: the tallest (<= kPulseRows) that still gives every resident CTA slot a
+    // tile in the last wave, so that no SM runs one tile more than the others.
+    const int tiles_x = (a.nx + kPulseCols - 1) / kPulseCols;
+    const long long want = (long long)resident * (((long long)tiles_x * ((a.ny + kPulseRows - 1) / kPulseRows) +
+                                                   resident - 1) / resident);
+    long long per_col = want / tiles_x;
+    if (per_col < 1) per_col = 1;
+    int rows = (int)((a.ny + per_col - 1) / per_col);
+    a.tile_rows = rows < 16 ? (a.ny < 16 ? a.ny : 16) : (rows > kPulseRows ? kPulseRows : rows);
+    const long long tiles = (long long)tiles_x * ((a.ny + a.tile_rows - 1) / a.tile_rows);
     const long long grid = tiles < resident ? tiles : resident;
     k<<<(unsigned)grid, kPulseCols, smem, st>>>(a);
     return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
