@@ -266,6 +266,11 @@ def accumulation_roofline(peak, peak_src, n=4096, nbins=2048, reps=10):
         out[name] = {"ms": round(ms, 4), "facets_per_s": n * n / (ms * 1e-3), "GBps": round(gbs, 1),
                      "frac": round(gbs / peak, 4), "alg_bytes_per_facet": bpf}
         del sc, o
+    try:
+        traffic = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))["accumulation"]["c64"]
+    except (OSError, ValueError, KeyError):
+        traffic = None
+    out["c64"]["traffic"] = traffic
     out.update({"kernel": "chan_profile_2d_kernel", "grid": [n, n], "nbins": nbins, "peak": peak,
                 "peak_source": peak_src, "bound": "hbm"})
     return out
