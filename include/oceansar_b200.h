@@ -214,6 +214,15 @@ typedef struct {
     double *nrcs_spec_d;                 /* float64 [az_steps]: += sum |E_spec|^2            */
     double *nrcs_bragg_d;                /* float64 [npol][az_steps]: += sum RCS at refresh  */
     void *rowtab_d;                      /* ocs_pulse_workspace_bytes(ny, nch) bytes         */
+    /* Romeiser LUT mode (romeiser97.py:71-134): on refresh pulses the Bragg RCS is looked up
+     * at (round((az - lut_az0)/lut_daz), clamp(round((Diffy - lut_dy0)/lut_ddy)),
+     * clamp(round((Diffx - lut_dx0)/lut_ddx))) instead of evaluated.  lut_d: [npol][2][naz]
+     * [ndy][ndx] float64 (F64) / float32 (MIXED); NULL: direct model.  Negative azimuth
+     * indices count from the end, as numpy indexing does; larger ones are the caller's error
+     * (checked on the host). */
+    const void *lut_d;
+    int32_t lut_naz, lut_ndy, lut_ndx;
+    double lut_az0, lut_daz, lut_dy0, lut_ddy, lut_dx0, lut_ddx;
 } ocs_pulse_desc;
 
 /* Workspace of ocs_pulse (per-pulse table of the row quantities); < 0 on invalid sizes. */

@@ -32,7 +32,10 @@ class PulseDesc(ctypes.Structure):
                 ("scat_d", P), ("s_m_d", P), ("s_p_d", P), ("n_m", I64), ("n_p", I64),
                 ("ind0_m_d", P), ("ind0_p_d", P),
                 ("sinc_d", P), ("raw_d", P), ("nbins", I32),
-                ("nrcs_spec_d", P), ("nrcs_bragg_d", P), ("rowtab_d", P)]
+                ("nrcs_spec_d", P), ("nrcs_bragg_d", P), ("rowtab_d", P),
+                ("lut_d", P), ("lut_naz", I32), ("lut_ndy", I32), ("lut_ndx", I32),
+                ("lut_az0", F64), ("lut_daz", F64), ("lut_dy0", F64), ("lut_ddy", F64),
+                ("lut_dx0", F64), ("lut_ddx", F64)]
 
 
 class RcsDesc(ctypes.Structure):

@@ -62,7 +62,35 @@ struct PulseArgs {
     double *nrcs_bragg;                     // [npol][az_steps] sum RCS (refresh pulses)
     int az_steps;
     int tile_rows;                          // rows per tile of a single-scene launch
+    const void *lut;                        // Romeiser LUT [npol][2][naz][ndy][ndx] (T), or null
+    int lut_naz, lut_ndy, lut_ndx;
+    double lut_az0, lut_daz, lut_dy0, lut_ddy, lut_dx0, lut_ddx;
 };
+
+// LUT mode of the Romeiser model (romeiser97.py:109-134): RCS of both Bragg lines of
+// polarisation p at (azimuth index of the row, clamped slope indices of the facet).
+// Indices round half to even from float64 differences and divisions, as numpy does.
+template <typename T>
+OCS_D void romeiser_lut(const PulseArgs &a, int az_ind, float diffx, float diffy, int p, T (&r)[2]) {
+    int iy = (int)rint(ddiv(dsub((double)diffy, a.lut_dy0), a.lut_ddy));
+    int ix = (int)rint(ddiv(dsub((double)diffx, a.lut_dx0), a.lut_ddx));
+    iy = iy > 0 ? (iy < a.lut_ndy ? iy : a.lut_ndy - 1) : 0;
+    ix = ix > 0 ? (ix < a.lut_ndx ? ix : a.lut_ndx - 1) : 0;
+    const T *lut = static_cast<const T *>(a.lut);
+    const long long plane = (long long)a.lut_naz * a.lut_ndy * a.lut_ndx;
+    const long long off = ((long long)az_ind * a.lut_ndy + iy) * a.lut_ndx + ix;
+    r[0] = lut[(2LL * p) * plane + off];
+    r[1] = lut[(2LL * p + 1) * plane + off];
+}
+
+// Azimuth index of a row's ground-projected azimuth angle (negative: from the end, as numpy
+// indexing takes it; out-of-table rows are rejected by the host before launch, and are
+// clamped here so that no access leaves the table).
+OCS_D int lut_az_index(const PulseArgs &a, double azp) {
+    int i = (int)rint(ddiv(dsub(azp, a.lut_az0), a.lut_daz));
+    if (i < 0) i += a.lut_naz;
+    return i < 0 ? 0 : (i >= a.lut_naz ? a.lut_naz - 1 : i);
+}
 
 // Asynchronous global -> shared copies (cp.async): each thread copies the words it will
 // read itself, so a cp.async.wait_group by that thread is all the ordering needed.
@@ -344,8 +372,20 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
                 T sc[2][2];                                            // [pol][line]
                 if (a.refresh) {
                     T hh[2], vv[2];
-                    romeiser_facet<T>(a.rom, (T)inc_c, (T)sm.r_az[2 * RCAP + i], (T)sm.r_az[3 * RCAP + i], (T)sm.r_az[4 * RCAP + i],
-                                      (T)cur.diffx, (T)cur.diffy, hh, vv);
+                    if (a.lut) {
+                        // the table holds the model's output polarisation(s) in output order
+                        const int ai = lut_az_index(a, sm.r_az[2 * RCAP + i]);
+                        T r0[2], r1[2];
+                        romeiser_lut<T>(a, ai, cur.diffx, cur.diffy, 0, r0);
+                        if (a.npol == 2) romeiser_lut<T>(a, ai, cur.diffx, cur.diffy, 1, r1);
+                        else { r1[0] = r0[0]; r1[1] = r0[1]; }
+                        const bool vv_first = a.rom.pol == POL_VV;
+                        hh[0] = vv_first ? r1[0] : r0[0]; hh[1] = vv_first ? r1[1] : r0[1];
+                        vv[0] = vv_first ? r0[0] : r1[0]; vv[1] = vv_first ? r0[1] : r1[1];
+                    } else {
+                        romeiser_facet<T>(a.rom, (T)inc_c, (T)sm.r_az[2 * RCAP + i], (T)sm.r_az[3 * RCAP + i],
+                                          (T)sm.r_az[4 * RCAP + i], (T)cur.diffx, (T)cur.diffy, hh, vv);
+                    }
                     if (a.use_hmtf) {
                         float hm = a.hmtf[idx];
                         hm = hm < -1.f ? -1.f : hm;
@@ -625,6 +665,15 @@ static int fill_pulse_args(const ocs_pulse_desc *d, PulseArgs &a) {
     a.raw_out_stride = (long long)d->az_steps * d->nbins;
     a.raw_row = (long long)d->az_step * d->nbins;
     a.nrcs_spec = d->nrcs_spec_d; a.nrcs_bragg = d->nrcs_bragg_d; a.az_steps = d->az_steps;
+    a.lut = d->lut_d;
+    if (a.lut) {
+        if (d->lut_naz < 1 || d->lut_ndy < 1 || d->lut_ndx < 1 || !(d->lut_daz != 0.0) || !(d->lut_ddy != 0.0) ||
+            !(d->lut_ddx != 0.0))
+            return OCS_ERR_ARG;
+        a.lut_naz = d->lut_naz; a.lut_ndy = d->lut_ndy; a.lut_ndx = d->lut_ndx;
+        a.lut_az0 = d->lut_az0; a.lut_daz = d->lut_daz; a.lut_dy0 = d->lut_dy0; a.lut_ddy = d->lut_ddy;
+        a.lut_dx0 = d->lut_dx0; a.lut_ddx = d->lut_ddx;
+    }
     return OCS_OK;
 }
 

@@ -4,7 +4,10 @@
   builds the reference's interpolation table of the omni-directional spectrum on the host
   (k = 1, 1.1, ... < 2 k0); ``rcs`` runs the float64 sm_100a kernel behind
   ``ocs_rcs_romeiser``.  Inside ``sar_raw`` the same device function runs fused in the
-  per-pulse kernel.  The LUT mode (``use_lut=True``, ``:71-92, 109-134``) is not built.
+  per-pulse kernel.  The LUT mode (``use_lut=True``, ``:71-92, 109-134``) tabulates the
+  model over (azimuth, slope_y, slope_x) at the mean incidence with the same device
+  function, on first use; lookups round half to even and clamp the slopes as the reference
+  does (on the host for ``rcs``, inside the pulse kernel for ``sar_raw``).
 * ``RCSKodis`` -- stationary-phase specular field (``nrcs/kodis.py:27-73``) behind
   ``ocs_field_kodis``.
 """
@@ -39,9 +42,6 @@ class RCSRomeiser97(object):
     def __init__(self, k0, inc_angle, pol, dx, dy, wind_U, wind_dir, wind_fetch, sw_spec_func,
                  sw_spread_func, d, numba=True, rmss_x=0.1, rmss_y=0.1, az_span=np.radians(1),
                  use_lut=True):
-        if use_lut:
-            raise NotImplementedError('RCSRomeiser97 LUT mode (use_lut=True) is not built; '
-                                      'use use_lut=False (direct evaluation)')
         if pol not in POL_CODES:
             raise ValueError('pol must be vv, hh or DP')
         if (sw_spread_func == 'none') and (sw_spec_func == 'elfouhaily'):
@@ -62,6 +62,89 @@ class RCSRomeiser97(object):
         self.spread_code = spread.DEVICE_CODES[sw_spread_func]
         self.spread_consts = spread.elfouhaily_delta_coeffs(self.wind_U, self.wind_fetch)
         self._tab = None
+        self._lut_dev = {}
+        self._lut_rcs = None
+        if use_lut:
+            self._lut_grid(rmss_x, rmss_y, az_span)
+            self.use_lut = True
+
+    # ---- LUT mode (romeiser97.py:71-92) --------------------------------------------------
+    def _lut_grid(self, rmss_x, rmss_y, az_span):
+        """Table axes: slopes in steps of 0.0025 over +-5 rms slopes (rms floored at 0.01),
+        azimuth in steps of 0.05 deg over az_span plus one step either side."""
+        step, nsig = 0.0025, 5
+        # np.max over a list: float32 rms slopes are promoted to float64 (as the reference's)
+        sx, sy = np.max([rmss_x, 0.01]), np.max([rmss_y, 0.01])
+        nx = int(sx * nsig * 2 / step)
+        ny = int(sy * nsig * 2 / step)
+        self.lut_Diffx = (-nsig * sx + np.arange(nx) * step)[np.newaxis, np.newaxis, :]
+        self.lut_Diffy = (-nsig * sy + np.arange(ny) * step)[np.newaxis, :, np.newaxis]
+        az_step = np.radians(0.05)
+        naz_in = int(az_span / az_step)
+        self.lut_az = (-az_span / 2 + np.arange(-1, naz_in + 2) * az_step)[:, np.newaxis, np.newaxis]
+        self._lut_shape = (naz_in + 3, ny, nx)
+
+    def lut_params(self):
+        """(naz, ndy, ndx, az0, daz, dy0, ddy, dx0, ddx) of the table, float64 as numpy forms them."""
+        naz, ndy, ndx = self._lut_shape
+        return (naz, ndy, ndx, float(self.lut_az.min()), float(self.lut_az[1, 0, 0] - self.lut_az[0, 0, 0]),
+                float(self.lut_Diffy[0, 0, 0]), float(self.lut_Diffy[0, 1, 0] - self.lut_Diffy[0, 0, 0]),
+                float(self.lut_Diffx[0, 0, 0]), float(self.lut_Diffx[0, 0, 1] - self.lut_Diffx[0, 0, 0]))
+
+    def _lut_device64(self):
+        """The table on the device, float64 [npol][2][naz][ndy][ndx] (pol order: the
+        model's outputs, hh then vv for 'DP'), evaluated by the direct model at the mean
+        incidence (romeiser97.py:83-91)."""
+        if 'f64' not in self._lut_dev:
+            naz, ndy, ndx = self._lut_shape
+            az = np.repeat(self.lut_az.ravel(), ndy).reshape(naz * ndy, 1)
+            dx = np.broadcast_to(self.lut_Diffx.reshape(1, ndx), (naz * ndy, ndx))
+            dy = np.broadcast_to(np.tile(self.lut_Diffy.ravel(), naz).reshape(naz * ndy, 1), (naz * ndy, ndx))
+            inc_keep = self.inc_angle
+            self.inc_angle = np.float64(np.mean(inc_keep))
+            try:
+                outs = self._rcs_direct_device(az, dx, dy)
+            finally:
+                self.inc_angle = inc_keep
+            import torch
+            self._lut_dev['f64'] = torch.stack([o.reshape(2, naz, ndy, ndx) for o in outs]).contiguous()
+        return self._lut_dev['f64']
+
+    def lut_device(self, precision):
+        """Device table in the pulse kernel's real type (float64 'f64', float32 'mixed')."""
+        t = self._lut_device64()
+        if precision == 'f64':
+            return t
+        if 'f32' not in self._lut_dev:
+            import torch
+            self._lut_dev['f32'] = t.to(torch.float32).contiguous()
+        return self._lut_dev['f32']
+
+    @property
+    def lut_rcs(self):
+        """The table as the reference holds it: [2][naz][ndy][ndx] or an (hh, vv) pair."""
+        if self._lut_rcs is None:
+            t = self._lut_device64().cpu().numpy()
+            self._lut_rcs = (t[0], t[1]) if self.pol == 'DP' else t[0]
+        return self._lut_rcs
+
+    def rcs_lut(self, az_angle, diffx, diffy):
+        """Table lookup (romeiser97.py:109-134)."""
+        az_ind = (np.round((az_angle - self.lut_az.min()) /
+                           (self.lut_az[1, 0, 0] - self.lut_az[0, 0, 0]))).astype(int)
+        dy = (np.round((diffy - self.lut_Diffy[0, 0, 0]) /
+                       (self.lut_Diffy[0, 1, 0] - self.lut_Diffy[0, 0, 0]))).astype(int)
+        dx = (np.round((diffx - self.lut_Diffx[0, 0, 0]) /
+                       (self.lut_Diffx[0, 0, 1] - self.lut_Diffx[0, 0, 0]))).astype(int)
+        dy = np.where(dy > 0, dy, 0)
+        dx = np.where(dx > 0, dx, 0)
+        dy = np.where(dy < self.lut_Diffy.shape[1], dy, self.lut_Diffy.shape[1] - 1)
+        dx = np.where(dx < self.lut_Diffx.shape[2], dx, self.lut_Diffx.shape[2] - 1)
+        lut = self.lut_rcs
+        if self.pol == 'DP':
+            return (np.stack([lut[0][0][az_ind, dy, dx], lut[0][1][az_ind, dy, dx]]),
+                    np.stack([lut[1][0][az_ind, dy, dx], lut[1][1][az_ind, dy, dx]]))
+        return lut[:, az_ind, dy, dx]
 
     def device_tables(self):
         if self._tab is None:
@@ -84,6 +167,15 @@ class RCSRomeiser97(object):
 
     def rcs(self, az_angle, diffx, diffy):
         """RCS of both Bragg lines, float64 [2, Ny, Nx]; a (hh, vv) pair for 'DP'."""
+        if self.use_lut:
+            return self.rcs_lut(az_angle, diffx, diffy)
+        outs = self._rcs_direct_device(az_angle, diffx, diffy)
+        if self.pol == 'DP':
+            return outs[0].cpu().numpy(), outs[1].cpu().numpy()
+        return outs[0].cpu().numpy()
+
+    def _rcs_direct_device(self, az_angle, diffx, diffy):
+        """Direct model on the device: list of float64 [2, Ny, Nx] tensors (hh, vv for 'DP')."""
         diffx = np.asarray(diffx)
         ny, nx = diffx.shape
         dxd = _device.to_device(diffx, np.float64)
@@ -106,10 +198,15 @@ class RCSRomeiser97(object):
         desc.out_vv_d = out_vv.data_ptr() if want_vv else None
         _capi.call("ocs_rcs_romeiser", ctypes.addressof(desc), _device.stream_ptr())
         if self.pol == 'DP':
-            return out_hh.cpu().numpy(), out_vv.cpu().numpy()
-        return (out_hh if want_hh else out_vv).cpu().numpy()
+            return [out_hh, out_vv]
+        return [out_hh if want_hh else out_vv]
 
-    rcs_numba = rcs
+    def rcs_numba(self, az_angle, diffx, diffy):
+        """The direct model (romeiser97.py:252-393), whatever the LUT setting."""
+        outs = self._rcs_direct_device(az_angle, diffx, diffy)
+        if self.pol == 'DP':
+            return outs[0].cpu().numpy(), outs[1].cpu().numpy()
+        return outs[0].cpu().numpy()
 
 
 class RCSKodis(object):

@@ -176,6 +176,7 @@ class RawGenerator(object):
                                                 np.arctan2(u_eff[1], u_eff[0]), s.wind_fetch,
                                                 srg.scat_bragg_spec, srg.scat_bragg_spread,
                                                 srg.scat_bragg_d, rmss_x=s.rmss_x, rmss_y=s.rmss_y,
+                                                az_span=(self.t_span * v_ground + s.Ly) / gr0,
                                                 use_lut=bool(srg.use_lut))
         self._on_device = False
         if device:
@@ -251,6 +252,11 @@ class RawGenerator(object):
             d.s_m_d, d.s_p_d, d.n_m, d.n_p = sm.data_ptr(), sp.data_ptr(), int(self.rndscat_m.N), \
                 int(self.rndscat_p.N)
             d.ind0_m_d, d.ind0_p_d = im.data_ptr(), ip.data_ptr()
+            if self.rcs_bragg.use_lut:
+                self._lut_d = self.rcs_bragg.lut_device(self.precision)
+                d.lut_d = self._lut_d.data_ptr()
+                (d.lut_naz, d.lut_ndy, d.lut_ndx, d.lut_az0, d.lut_daz, d.lut_dy0, d.lut_ddy, d.lut_dx0,
+                 d.lut_ddx) = self.rcs_bragg.lut_params()
         d.sinc_d = self._sinc_d.data_ptr()
         d.raw_d = self.raw_d.data_ptr()
         d.nbins = self.rg_samp
@@ -279,6 +285,7 @@ class RawGenerator(object):
         if self.scat_bragg_enable:
             d.tind = self.rndscat_m.tind(t_now)
             if (t_now - self.t_last_rcs_bragg) > self.ocean_dt:
+                self._lut_check(az_now)
                 d.refresh = 1
                 self.t_last_rcs_bragg = t_now
                 self._refreshes.append(az_step)
@@ -314,12 +321,28 @@ class RawGenerator(object):
                 tind = self.rndscat_m.tind(t_now)
                 tmod[a] = (tind % int(self.rndscat_m.N), tind % int(self.rndscat_p.N))
                 if (t_now - t_last) > self.ocean_dt:
+                    self._lut_check(az_now[a])
                     flags[a] |= 2
                     t_last = t_now
                     refreshes.append(a)
         tables = dict(t=t32, add=add, swell_rot=rot if s.swell_enable else None, az_now=az_now,
                       flags=flags, tmod=tmod)
         return tables, refreshes, t_last
+
+    def _lut_check(self, az_now):
+        """LUT mode: the rows' azimuth indices must exist in the table, as numpy indexing
+        requires (negative ones count from the end); raise IndexError as the reference's
+        lookup would (romeiser97.py:117, 134)."""
+        if not (self.scat_bragg_enable and self.rcs_bragg.use_lut):
+            return
+        m = self.rcs_bragg
+        az = (self.surface.y - az_now).reshape((self.surface.Ny, 1))
+        ind = np.round((np.arcsin(az / self.gr0) - m.lut_az.min()) /
+                       (m.lut_az[1, 0, 0] - m.lut_az[0, 0, 0])).astype(int)
+        n = m.lut_az.shape[0]
+        if ind.max() >= n or ind.min() < -n:
+            bad = int(ind.max() if ind.max() >= n else ind.min())
+            raise IndexError('index %d is out of bounds for axis 0 with size %d' % (bad, n))
 
     def run(self, steps=None):
         for a in (range(self.az_steps) if steps is None else steps):

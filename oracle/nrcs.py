@@ -21,8 +21,6 @@ class RCSRomeiser97:
     def __init__(self, k0, inc_angle, pol, dx, dy, wind_U, wind_dir, wind_fetch,
                  sw_spec_func, sw_spread_func, d, numba=True, rmss_x=0.1, rmss_y=0.1,
                  az_span=np.radians(1), use_lut=False):
-        if use_lut:
-            raise NotImplementedError('LUT mode is not restated by the oracle')
         self.wind_U, self.wind_dir, self.wind_fetch = wind_U, wind_dir, wind_fetch
         self.dx, self.dy, self.pol, self.k0 = dx, dy, pol, k0
         self.inc_angle, self.d = inc_angle, d
@@ -32,6 +30,52 @@ class RCSRomeiser97:
         self.interp_k = k
         self.interp_S = spectrum
         self.spec_interpolator = interpolate.interp1d(k, spectrum, bounds_error=False, fill_value=1)
+        self.use_lut = False
+        if use_lut:
+            self._build_lut(rmss_x, rmss_y, az_span)
+
+    def _build_lut(self, rmss_x, rmss_y, az_span):
+        """LUT over (azimuth, slope_y, slope_x) at the mean incidence (romeiser97.py:71-92):
+        slope steps 0.0025 over +-5 rms slopes (rms floored at 0.01), azimuth steps 0.05 deg
+        over az_span plus one step either side; every entry is the direct model."""
+        step = 0.0025
+        nsig = 5
+        # np.max over a list: float32 rms slopes are promoted to float64 (as the reference's)
+        sx, sy = np.max([rmss_x, 0.01]), np.max([rmss_y, 0.01])
+        nx = int(sx * nsig * 2 / step)
+        ny = int(sy * nsig * 2 / step)
+        self.lut_Diffx = (-nsig * sx + np.arange(nx) * step)[np.newaxis, np.newaxis, :]
+        self.lut_Diffy = (-nsig * sy + np.arange(ny) * step)[np.newaxis, :, np.newaxis]
+        az_step = np.radians(0.05)
+        naz_in = int(az_span / az_step)
+        self.lut_az = (-az_span / 2 + np.arange(-1, naz_in + 2) * az_step)[:, np.newaxis, np.newaxis]
+        shape = (naz_in + 3, ny, nx)
+        inc_keep = self.inc_angle
+        self.inc_angle = inc_keep.mean() + np.zeros_like(self.lut_Diffx)
+        self.lut_rcs = self.rcs(self.lut_az + np.zeros(shape), self.lut_Diffx + np.zeros(shape),
+                                self.lut_Diffy + np.zeros(shape))
+        self.inc_angle = inc_keep
+        self.use_lut = True
+
+    def lut_indices(self, az_angle, diffx, diffy):
+        """LUT indices of facets (romeiser97.py:109-123): round half to even, slopes clamped
+        to the table, azimuth indices as numpy indexing takes them."""
+        az_ind = np.round((az_angle - self.lut_az.min()) /
+                          (self.lut_az[1, 0, 0] - self.lut_az[0, 0, 0])).astype(int)
+        dy = np.round((diffy - self.lut_Diffy[0, 0, 0]) /
+                      (self.lut_Diffy[0, 1, 0] - self.lut_Diffy[0, 0, 0])).astype(int)
+        dx = np.round((diffx - self.lut_Diffx[0, 0, 0]) /
+                      (self.lut_Diffx[0, 0, 1] - self.lut_Diffx[0, 0, 0])).astype(int)
+        dy = np.clip(dy, 0, self.lut_Diffy.shape[1] - 1)
+        dx = np.clip(dx, 0, self.lut_Diffx.shape[2] - 1)
+        return az_ind, dy, dx
+
+    def rcs_lut(self, az_angle, diffx, diffy):
+        a, dy, dx = self.lut_indices(az_angle, diffx, diffy)
+        if self.pol == 'DP':
+            return (np.stack([self.lut_rcs[0][0][a, dy, dx], self.lut_rcs[0][1][a, dy, dx]]),
+                    np.stack([self.lut_rcs[1][0][a, dy, dx], self.lut_rcs[1][1][a, dy, dx]]))
+        return self.lut_rcs[:, a, dy, dx]
 
     @staticmethod
     def _kernel(inc_angle, az_angle, diffx, diffy, k0, pol, wind_dir, d):
@@ -67,6 +111,8 @@ class RCSRomeiser97:
         return k_b, theta_inp, T_hh, T_vv, bad
 
     def rcs(self, az_angle, diffx, diffy):
+        if self.use_lut:
+            return self.rcs_lut(az_angle, diffx, diffy)
         diffx = np.asarray(diffx, dtype=np.float64)
         diffy = np.asarray(diffy, dtype=np.float64)
         az = np.broadcast_to(np.asarray(az_angle, dtype=np.float64), diffx.shape)

@@ -10,7 +10,7 @@ reference functions on the raw-data-generation path:
 
 * ``radarsim/range_profile.py``  ``calc_sinc_vec`` / ``chan_profile_numba``
 * ``surfaces/ocean.py``          ``OceanSurface.init`` and the ``t`` setter
-* ``nrcs/romeiser97.py``         ``RCSRomeiser97.rcs`` (numba path)
+* ``nrcs/romeiser97.py``         ``RCSRomeiser97.rcs`` (numba path and LUT mode)
 * ``nrcs/kodis.py``              ``RCSKodis.field``
 * ``closure/*.py``               ``grid_coherence`` / ``randomscat_ts``
 * ``utils/geometry.py``, ``utils/misc.py``  geometry helpers and ``optimize_fftsize``
@@ -183,6 +183,35 @@ def gen_rcs():
     save("rcs_romeiser.npz", **out)
 
 
+def gen_rcs_lut():
+    """RCSRomeiser97 in LUT mode (romeiser97.py:71-92, 109-134): a small LUT (rmss 0.02 /
+    0.015, 0.3 deg azimuth span) and its lookups on slopes that partly fall outside it."""
+    f0 = 5.405e9
+    k0 = 2 * np.pi * f0 / const.c
+    Ny, Nx = 48, 40
+    rs = np.random.RandomState(9)
+    diffx = (0.04 * rs.randn(Ny, Nx)).astype(np.float32)
+    diffy = (0.03 * rs.randn(Ny, Nx)).astype(np.float32)
+    inc = np.deg2rad(np.linspace(30., 40., Nx)).reshape(1, Nx)
+    y = np.linspace(-1200, 1200, Ny).astype(np.float32).astype(np.float64)
+    az_angle = np.arcsin((y / 5e5)).reshape(Ny, 1)
+    out = dict(diffx=diffx, diffy=diffy, inc=inc, az_angle=az_angle, k0=np.array(k0))
+    for pol in ('vv', 'hh', 'DP'):
+        m = nrcs.RCSRomeiser97(k0, inc, pol, 1.0, 1.0, 10.0, np.deg2rad(20.), 500e3, 'elfouhaily', 'elfouhaily',
+                               0.125, rmss_x=0.02, rmss_y=0.015, az_span=np.deg2rad(0.3), use_lut=True)
+        r = m.rcs(az_angle, diffx, diffy)
+        if pol == 'DP':
+            out["lut_hh"], out["lut_vv"] = np.asarray(m.lut_rcs[0]), np.asarray(m.lut_rcs[1])
+            out["DP_hh"], out["DP_vv"] = r
+        else:
+            out["lut_" + pol + "_single"] = np.asarray(m.lut_rcs)
+            out[pol] = r
+    out["lut_az"] = m.lut_az.ravel()
+    out["lut_Diffx"] = m.lut_Diffx.ravel()
+    out["lut_Diffy"] = m.lut_Diffy.ravel()
+    save("rcs_romeiser_lut.npz", **out)
+
+
 def gen_kodis():
     f0 = 5.405e9
     k0 = 2 * np.pi * f0 / const.c
@@ -319,7 +348,7 @@ scat_bragg_model=romeiser97
 scat_bragg_spec=elfouhaily
 scat_bragg_spread={bspread}
 scat_bragg_d=0.125
-use_lut=False
+use_lut={lut}
 """
 
 SAR_CASES = {
@@ -327,19 +356,24 @@ SAR_CASES = {
     "c1small": dict(inc=35., pol='vv', prf=1000., v_ground=7600., ant_l=120., num_ch=1, b_ati=0,
                     b_xti=0, Lx=64, Ly=64, dx=1., dy=1., fmp=2, depth=1e5, wind_dir=0., wind_U=10.,
                     dswell=False, freq_r=0.079, swell=False, spread='cos2s', cur=0., choppy=False,
-                    hmtf=False, spec_on=True, bspread='cos2s'),
+                    hmtf=False, spec_on=True, bspread='cos2s', lut=False),
     # two along-track channels, dual pol, hMTF, choppy waves, monochromatic swell, current
     "c2small": dict(inc=35., pol='DP', prf=1500., v_ground=7600., ant_l=100., num_ch=2, b_ati=10.,
                     b_xti=0, Lx=64, Ly=32, dx=1., dy=1., fmp=2, depth=1e5, wind_dir=45., wind_U=7.,
                     dswell=False, freq_r=0.079, swell=True, spread='elfouhaily', cur=0.2,
-                    choppy=True, hmtf=True, spec_on=True, bspread='elfouhaily'),
+                    choppy=True, hmtf=True, spec_on=True, bspread='elfouhaily', lut=False),
     # four channels (ATI 0/5/10/0 m, one 2 m XTI), directional swell, 0.5 m grid, hh
     "c3small": dict(inc=30., pol='hh', prf=2000., v_ground=7600., ant_l=130., num_ch=4,
                     b_ati='[0., 5., 10., 0.]', b_xti='[0., 0., 0., 2.]', Lx=24, Ly=27, dx=0.5, dy=0.5,
                     fmp=3, depth=1e5, wind_dir=30., wind_U=15., dswell=True,
                     freq_r=float(np.sqrt(const.g / (2 * np.pi * 250.))), swell=False,
                     spread='elfouhaily', cur=0., choppy=False, hmtf=False, spec_on=True,
-                    bspread='elfouhaily'),
+                    bspread='elfouhaily', lut=False),
+    # the single-channel case with the Romeiser LUT mode (romeiser97.py:71-134)
+    "c1lut": dict(inc=35., pol='vv', prf=1000., v_ground=7600., ant_l=120., num_ch=1, b_ati=0,
+                  b_xti=0, Lx=64, Ly=64, dx=1., dy=1., fmp=2, depth=1e5, wind_dir=0., wind_U=10.,
+                  dswell=False, freq_r=0.079, swell=False, spread='cos2s', cur=0., choppy=False,
+                  hmtf=False, spec_on=True, bspread='cos2s', lut=True),
 }
 
 
@@ -401,7 +435,7 @@ after_trap=1.0
 """
 
 
-def gen_cfg_and_sar():
+def gen_cfg_and_sar(only=None):
     res = {}
     qpath = os.path.join(OUT, "cfg", "quirks.cfg")
     os.makedirs(os.path.dirname(qpath), exist_ok=True)
@@ -416,6 +450,8 @@ def gen_cfg_and_sar():
     print("wrote cfg_parsed.json")
 
     for name in SAR_CASES:
+        if only and name not in only:
+            continue
         path = os.path.join(OUT, "cfg", name + ".cfg")
         calls = []
         orig = sar_raw_nompi.raw.chan_profile_numba
@@ -460,6 +496,8 @@ if __name__ == "__main__":
         gen_surfaces()
     if "rcs" in which:
         gen_rcs()
+    if "rcs_lut" in which:
+        gen_rcs_lut()
     if "kodis" in which:
         gen_kodis()
     if "closure" in which:
@@ -468,3 +506,5 @@ if __name__ == "__main__":
         gen_geometry()
     if "sar" in which:
         gen_cfg_and_sar()
+    if "sar_lut" in which:
+        gen_cfg_and_sar(only=["c1lut"])

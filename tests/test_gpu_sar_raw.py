@@ -53,7 +53,7 @@ def stagewise(name, precision, steps=None):
     return got, ref, gen, osim
 
 
-@pytest.mark.parametrize("name", ["c1small", "c2small", "c3small"])
+@pytest.mark.parametrize("name", ["c1small", "c2small", "c3small", "c1lut"])
 def test_stagewise_f64(name):
     got, ref, gen, osim = stagewise(name, "f64")
     assert rel_l2(got, ref) < 1e-10, rel_l2(got, ref)
@@ -62,7 +62,7 @@ def test_stagewise_f64(name):
     np.testing.assert_allclose(nr, nref, rtol=1e-9)
 
 
-@pytest.mark.parametrize("name", ["c1small", "c2small", "c3small"])
+@pytest.mark.parametrize("name", ["c1small", "c2small", "c3small", "c1lut"])
 def test_stagewise_mixed(name):
     got, ref, gen, osim = stagewise(name, "mixed")
     assert got.dtype == np.complex64
@@ -70,7 +70,7 @@ def test_stagewise_mixed(name):
     assert e < 1e-4 and ph < 1e-3, (e, ph)
 
 
-@pytest.mark.parametrize("name", ["c1small", "c2small", "c3small"])
+@pytest.mark.parametrize("name", ["c1small", "c2small", "c3small", "c1lut"])
 @pytest.mark.parametrize("precision", ["f64", "mixed"])
 def test_end_to_end_against_reference(name, precision):
     from oceansar_b200.radarsim.sar_raw_nompi import RawGenerator
@@ -84,6 +84,27 @@ def test_end_to_end_against_reference(name, precision):
     print(name, precision, "rel L2 %.3e  max phase %.3e rad" % (e, ph))
     assert e < 1e-4 and ph < 1e-3, (e, ph)
     np.testing.assert_allclose(nrcs_avg, d["NRCS_avg"], rtol=1e-5)
+
+
+def test_standalone_rcs_lut_golden():
+    """Romeiser LUT mode: the table (built on the GPU) and the lookups, against the reference."""
+    from oceansar_b200 import nrcs
+    d = np.load(os.path.join(G, "rcs_romeiser_lut.npz"))
+    k0 = float(d["k0"])
+    for pol in ("vv", "hh", "DP"):
+        m = nrcs.RCSRomeiser97(k0, d["inc"], pol, 1.0, 1.0, 10.0, np.deg2rad(20.), 500e3, 'elfouhaily',
+                               'elfouhaily', 0.125, rmss_x=0.02, rmss_y=0.015, az_span=np.deg2rad(0.3),
+                               use_lut=True)
+        r = m.rcs(d["az_angle"], d["diffx"], d["diffy"])
+        if pol == "DP":
+            pairs = ((m.lut_rcs[0], d["lut_hh"]), (m.lut_rcs[1], d["lut_vv"]), (r[0], d["DP_hh"]), (r[1], d["DP_vv"]))
+        else:
+            pairs = ((m.lut_rcs, d["lut_%s_single" % pol]), (r, d[pol]))
+        for got, ref in pairs:
+            assert got.shape == ref.shape
+            fin = np.isfinite(ref)
+            np.testing.assert_array_equal(np.isfinite(got), fin)
+            np.testing.assert_allclose(got[fin], ref[fin], rtol=1e-10, atol=1e-300)
 
 
 def test_standalone_rcs_and_kodis_golden():

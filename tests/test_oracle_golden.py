@@ -42,7 +42,7 @@ def test_chan_profile_bit_exact(case):
     np.testing.assert_array_equal(out, g["out"])
 
 
-@pytest.mark.parametrize("name", ["c1small", "c2small", "c3small"])
+@pytest.mark.parametrize("name", ["c1small", "c2small", "c3small", "c1lut"])
 def test_chan_profile_captured_calls_bit_exact(name):
     d = load("sar_raw_%s.npz" % name)
     sinc = range_profile.calc_sinc_vec(8, 20, Fs=1.1)
@@ -127,6 +127,29 @@ def test_romeiser_rcs():
     np.testing.assert_allclose(m.interp_S, d["interp_S"], rtol=1e-15)
 
 
+def test_romeiser_lut_mode():
+    """LUT mode (romeiser97.py:71-134): the table and the lookups, against the reference."""
+    d = load("rcs_romeiser_lut.npz")
+    k0 = float(d["k0"])
+    for pol in ("vv", "hh", "DP"):
+        m = nrcs.RCSRomeiser97(k0, d["inc"], pol, 1.0, 1.0, 10.0, np.deg2rad(20.), 500e3, 'elfouhaily',
+                               'elfouhaily', 0.125, rmss_x=0.02, rmss_y=0.015, az_span=np.deg2rad(0.3),
+                               use_lut=True)
+        np.testing.assert_array_equal(m.lut_az.ravel(), d["lut_az"])
+        np.testing.assert_array_equal(m.lut_Diffx.ravel(), d["lut_Diffx"])
+        np.testing.assert_array_equal(m.lut_Diffy.ravel(), d["lut_Diffy"])
+        r = m.rcs(d["az_angle"], d["diffx"], d["diffy"])
+        if pol == "DP":
+            pairs = ((m.lut_rcs[0], d["lut_hh"]), (m.lut_rcs[1], d["lut_vv"]), (r[0], d["DP_hh"]), (r[1], d["DP_vv"]))
+        else:
+            pairs = ((m.lut_rcs, d["lut_%s_single" % pol]), (r, d[pol]))
+        for got, ref in pairs:
+            assert got.shape == ref.shape
+            fin = np.isfinite(ref)
+            np.testing.assert_array_equal(np.isfinite(got), fin)
+            np.testing.assert_allclose(got[fin], ref[fin], rtol=1e-12, atol=0)
+
+
 def test_kodis_field():
     d = load("kodis.npz")
     m = nrcs.RCSKodis(d["inc"], float(d["k0"]), 1.0, 1.0)
@@ -191,13 +214,13 @@ def _cfg_json(cfg):
 def test_cfg_parser():
     with open(os.path.join(G, "cfg_parsed.json")) as f:
         ref = json.load(f)
-    for name in ("quirks", "c1small", "c2small", "c3small"):
+    for name in ("quirks", "c1small", "c2small", "c3small", "c1lut"):
         cfg = ConfigFile(os.path.join(G, "cfg", name + ".cfg"))
         assert cfg.sections[1:] == ref[name]["sections"]
         assert _cfg_json(cfg) == ref[name]["values"]
 
 
-@pytest.mark.parametrize("name", ["c1small", "c2small", "c3small"])
+@pytest.mark.parametrize("name", ["c1small", "c2small", "c3small", "c1lut"])
 def test_sar_raw_end_to_end(name):
     d = load("sar_raw_%s.npz" % name)
     raw, nrcs_avg, sim = sar_raw(os.path.join(G, "cfg", name + ".cfg"), seed=0)
