@@ -17,7 +17,7 @@ derives them from the geometry, ``:264-278``).
 import numpy as np
 from scipy import linalg
 
-from . import closure, geometry as geo, nrcs, range_profile as rp, spectra
+from . import closure, geometry as geo, ka, nrcs, range_profile as rp, spectra
 from .cfg import ConfigFile
 from .surface import OceanSurface
 
@@ -117,9 +117,14 @@ class SarRawSim:
         self.NRCS_avg_vv = np.zeros(self.az_steps, dtype=float)
         self.NRCS_avg_hh = np.zeros(self.az_steps, dtype=float)
         if self.scat_spec_enable:
-            if self.scat_spec_mode != 'kodis':
+            if self.scat_spec_mode == 'kodis':
+                self.rcs_spec = nrcs.RCSKodis(self.inc, k0, s.dx, s.dy)
+            elif self.scat_spec_mode in ('fa', 'spa'):
+                # sar_raw_nompi.py:296-299: a phase screen is drawn (and not used afterwards)
+                self.spec_ph0 = np.random.uniform(0., 2. * np.pi, size=[s.Ny, s.Nx])
+                self.rcs_spec = ka.RCSKA(self.scat_spec_mode, k0, s.x, s.y, s.dx, s.dy)
+            else:
                 raise NotImplementedError('specular mode %s' % self.scat_spec_mode)
-            self.rcs_spec = nrcs.RCSKodis(self.inc, k0, s.dx, s.dy)
         if self.scat_bragg_enable:
             if srg.scat_bragg_model != 'romeiser97':
                 raise NotImplementedError('Bragg model %s' % srg.scat_bragg_model)
@@ -161,13 +166,28 @@ class SarRawSim:
             scene_hh = np.zeros([s.Ny, s.Nx], dtype=complex)
         if self.do_vv:
             scene_vv = np.zeros([s.Ny, s.Nx], dtype=complex)
-        if self.scat_spec_enable:
+        if self.scat_spec_enable and self.scat_spec_mode == 'kodis':
             Esn_sp = np.sqrt(4. * np.pi) * self.rcs_spec.field(az_proj_angle, sr_surface, s.Diffx,
                                                                 s.Diffy, s.Diffxx, s.Diffyy, s.Diffxy)
             if self.do_hh:
                 scene_hh += Esn_sp
             if self.do_vv:
                 scene_vv += Esn_sp
+        elif self.scat_spec_enable:
+            # Kirchhoff modes (sar_raw_nompi.py:402-426): per polarisation, two-way phase of the
+            # facet's slant range times the monostatic field
+            for do, pol_tmp in ((self.do_hh, 'hh'), (self.do_vv, 'vv')):
+                if not do:
+                    continue
+                Esn_sp = (np.exp(-1j * (2. * self.k0 * sr_surface)) * (4. * np.pi) ** 1.5 *
+                          self.rcs_spec.field(1, 1, pol_tmp[0], pol_tmp[1], self.inc, self.inc, az_proj_angle,
+                                              az_proj_angle + np.pi, s.Dz, s.Diffx, s.Diffy, s.Diffxx, s.Diffyy,
+                                              s.Diffxy))
+                if pol_tmp == 'hh':
+                    scene_hh += Esn_sp
+                else:
+                    scene_vv += Esn_sp
+        if self.scat_spec_enable:
             self.NRCS_avg_hh[az_step] += (np.sum(np.abs(Esn_sp) ** 2) / self.surface_area)
             self.NRCS_avg_vv[az_step] += self.NRCS_avg_hh[az_step]
         if self.scat_bragg_enable:

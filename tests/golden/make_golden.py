@@ -12,6 +12,7 @@ reference functions on the raw-data-generation path:
 * ``surfaces/ocean.py``          ``OceanSurface.init`` and the ``t`` setter
 * ``nrcs/romeiser97.py``         ``RCSRomeiser97.rcs`` (numba path and LUT mode)
 * ``nrcs/kodis.py``              ``RCSKodis.field``
+* ``nrcs/ka.py``                 ``RCSKA.field`` / ``rcs`` (facet approach, stationary phase)
 * ``closure/*.py``               ``grid_coherence`` / ``randomscat_ts``
 * ``utils/geometry.py``, ``utils/misc.py``  geometry helpers and ``optimize_fftsize``
 * ``ocs_io/cfg.py``              ``ConfigFile`` parsing of the ``.cfg`` files in ``cfg/``
@@ -212,6 +213,45 @@ def gen_rcs_lut():
     save("rcs_romeiser_lut.npz", **out)
 
 
+def gen_ka():
+    """RCSKA (nrcs/ka.py:41-310) field and rcs, facet approach and stationary phase, all four
+    polarisation pairs, monostatic, on seeded float32 surface derivatives."""
+    f0 = 5.405e9
+    k0 = 2 * np.pi * f0 / const.c
+    Ny, Nx = 40, 36
+    rs = np.random.RandomState(11)
+    x = np.arange(Nx) * 1.0 - Nx / 2
+    y = np.arange(Ny) * 1.0 - Ny / 2
+    Dz = (0.4 * rs.randn(Ny, Nx)).astype(np.float32)
+    Diffx = (0.08 * rs.randn(Ny, Nx)).astype(np.float32)
+    Diffy = (0.08 * rs.randn(Ny, Nx)).astype(np.float32)
+    Diffxx = (0.05 * rs.randn(Ny, Nx)).astype(np.float32)
+    Diffyy = (0.05 * rs.randn(Ny, Nx)).astype(np.float32)
+    Diffxy = (0.03 * rs.randn(Ny, Nx)).astype(np.float32)
+    Diffxx[0, 0] = Diffyy[0, 0] = Diffxy[0, 0] = 0.0          # J = 0
+    # slopes near tan(inc) so that some stationary points fall inside their facet
+    inc = np.deg2rad(np.linspace(30., 40., Nx)).reshape(1, Nx)
+    # rows 2-9: slopes facing the radar and strong curvature, so that stationary points fall
+    # inside their facets (both signs of J)
+    for r in range(2, 10):
+        Diffx[r, :] = (np.tan(inc[0]) + 0.3 * rs.randn(Nx)).astype(np.float32)
+        Diffy[r, :] = (0.3 * rs.randn(Nx)).astype(np.float32)
+        Diffxx[r, :] = 1.0
+        Diffyy[r, :] = 1.0 if r < 6 else -1.0
+        Diffxy[r, :] = 0.2
+    az = np.arcsin(np.linspace(-300, 300, Ny) / 5e5).reshape(Ny, 1)
+    out = dict(x=x, y=y, Dz=Dz, Diffx=Diffx, Diffy=Diffy, Diffxx=Diffxx, Diffyy=Diffyy, Diffxy=Diffxy,
+               inc=inc, az=az, k0=np.array(k0))
+    for mode in ('fa', 'spa'):
+        m = nrcs.RCSKA(mode, k0, x, y, 1.0, 1.0)
+        for pi_, ps in (('h', 'h'), ('v', 'v'), ('h', 'v'), ('v', 'h')):
+            E = m.field(1, 1, pi_, ps, inc, inc, az, az + np.pi, Dz, Diffx, Diffy, Diffxx, Diffyy, Diffxy)
+            out['E_%s_%s%s' % (mode, pi_, ps)] = E
+        out['rcs_%s_vv' % mode] = m.rcs('v', 'v', inc, inc, az, az + np.pi, Dz, Diffx, Diffy, Diffxx, Diffyy,
+                                        Diffxy)
+    save("ka.npz", **out)
+
+
 def gen_kodis():
     f0 = 5.405e9
     k0 = 2 * np.pi * f0 / const.c
@@ -342,7 +382,7 @@ use_hmtf={hmtf}
 nesz=-300.
 wh_tol=2.73    ; wave-height tolerance added to the range window
 scat_spec_enable={spec_on}
-scat_spec_mode=kodis
+scat_spec_mode={spec_mode}
 scat_bragg_enable=True
 scat_bragg_model=romeiser97
 scat_bragg_spec=elfouhaily
@@ -356,24 +396,33 @@ SAR_CASES = {
     "c1small": dict(inc=35., pol='vv', prf=1000., v_ground=7600., ant_l=120., num_ch=1, b_ati=0,
                     b_xti=0, Lx=64, Ly=64, dx=1., dy=1., fmp=2, depth=1e5, wind_dir=0., wind_U=10.,
                     dswell=False, freq_r=0.079, swell=False, spread='cos2s', cur=0., choppy=False,
-                    hmtf=False, spec_on=True, bspread='cos2s', lut=False),
+                    hmtf=False, spec_on=True, bspread='cos2s', lut=False, spec_mode='kodis'),
     # two along-track channels, dual pol, hMTF, choppy waves, monochromatic swell, current
     "c2small": dict(inc=35., pol='DP', prf=1500., v_ground=7600., ant_l=100., num_ch=2, b_ati=10.,
                     b_xti=0, Lx=64, Ly=32, dx=1., dy=1., fmp=2, depth=1e5, wind_dir=45., wind_U=7.,
                     dswell=False, freq_r=0.079, swell=True, spread='elfouhaily', cur=0.2,
-                    choppy=True, hmtf=True, spec_on=True, bspread='elfouhaily', lut=False),
+                    choppy=True, hmtf=True, spec_on=True, bspread='elfouhaily', lut=False, spec_mode='kodis'),
     # four channels (ATI 0/5/10/0 m, one 2 m XTI), directional swell, 0.5 m grid, hh
     "c3small": dict(inc=30., pol='hh', prf=2000., v_ground=7600., ant_l=130., num_ch=4,
                     b_ati='[0., 5., 10., 0.]', b_xti='[0., 0., 0., 2.]', Lx=24, Ly=27, dx=0.5, dy=0.5,
                     fmp=3, depth=1e5, wind_dir=30., wind_U=15., dswell=True,
                     freq_r=float(np.sqrt(const.g / (2 * np.pi * 250.))), swell=False,
                     spread='elfouhaily', cur=0., choppy=False, hmtf=False, spec_on=True,
-                    bspread='elfouhaily', lut=False),
+                    bspread='elfouhaily', lut=False, spec_mode='kodis'),
     # the single-channel case with the Romeiser LUT mode (romeiser97.py:71-134)
+    # Kirchhoff specular scattering (nrcs/ka.py): facet approach and stationary phase, dual pol
+    "c1fa": dict(inc=35., pol='DP', prf=1000., v_ground=7600., ant_l=120., num_ch=1, b_ati=0,
+                 b_xti=0, Lx=64, Ly=64, dx=1., dy=1., fmp=2, depth=1e5, wind_dir=0., wind_U=10.,
+                 dswell=False, freq_r=0.079, swell=False, spread='cos2s', cur=0., choppy=False,
+                 hmtf=False, spec_on=True, bspread='cos2s', lut=False, spec_mode='fa'),
+    "c1spa": dict(inc=35., pol='vv', prf=1000., v_ground=7600., ant_l=120., num_ch=1, b_ati=0,
+                  b_xti=0, Lx=64, Ly=64, dx=1., dy=1., fmp=2, depth=1e5, wind_dir=0., wind_U=10.,
+                  dswell=False, freq_r=0.079, swell=False, spread='cos2s', cur=0., choppy=False,
+                  hmtf=False, spec_on=True, bspread='cos2s', lut=False, spec_mode='spa'),
     "c1lut": dict(inc=35., pol='vv', prf=1000., v_ground=7600., ant_l=120., num_ch=1, b_ati=0,
                   b_xti=0, Lx=64, Ly=64, dx=1., dy=1., fmp=2, depth=1e5, wind_dir=0., wind_U=10.,
                   dswell=False, freq_r=0.079, swell=False, spread='cos2s', cur=0., choppy=False,
-                  hmtf=False, spec_on=True, bspread='cos2s', lut=True),
+                  hmtf=False, spec_on=True, bspread='cos2s', lut=True, spec_mode='kodis'),
 }
 
 
@@ -500,6 +549,8 @@ if __name__ == "__main__":
         gen_rcs_lut()
     if "kodis" in which:
         gen_kodis()
+    if "ka" in which:
+        gen_ka()
     if "closure" in which:
         gen_closure()
     if "geometry" in which:
@@ -508,3 +559,5 @@ if __name__ == "__main__":
         gen_cfg_and_sar()
     if "sar_lut" in which:
         gen_cfg_and_sar(only=["c1lut"])
+    if "sar_ka" in which:
+        gen_cfg_and_sar(only=["c1fa", "c1spa"])

@@ -42,7 +42,7 @@ def test_chan_profile_bit_exact(case):
     np.testing.assert_array_equal(out, g["out"])
 
 
-@pytest.mark.parametrize("name", ["c1small", "c2small", "c3small", "c1lut"])
+@pytest.mark.parametrize("name", ["c1small", "c2small", "c3small", "c1lut", "c1fa", "c1spa"])
 def test_chan_profile_captured_calls_bit_exact(name):
     d = load("sar_raw_%s.npz" % name)
     sinc = range_profile.calc_sinc_vec(8, 20, Fs=1.1)
@@ -150,6 +150,22 @@ def test_romeiser_lut_mode():
             np.testing.assert_allclose(got[fin], ref[fin], rtol=1e-12, atol=0)
 
 
+def test_ka_field():
+    """Kirchhoff specular field (nrcs/ka.py), facet approach and stationary phase."""
+    from oracle.ka import RCSKA
+    d = load("ka.npz")
+    for mode in ("fa", "spa"):
+        m = RCSKA(mode, float(d["k0"]), d["x"], d["y"], 1.0, 1.0)
+        for pp in ("hh", "vv", "hv", "vh"):
+            E = m.field(1, 1, pp[0], pp[1], d["inc"], d["inc"], d["az"], d["az"] + np.pi, d["Dz"], d["Diffx"],
+                        d["Diffy"], d["Diffxx"], d["Diffyy"], d["Diffxy"])
+            np.testing.assert_array_equal(E != 0, d["E_%s_%s" % (mode, pp)] != 0)
+            np.testing.assert_allclose(E, d["E_%s_%s" % (mode, pp)], rtol=1e-13, atol=0)
+        r = m.rcs('v', 'v', d["inc"], d["inc"], d["az"], d["az"] + np.pi, d["Dz"], d["Diffx"], d["Diffy"],
+                  d["Diffxx"], d["Diffyy"], d["Diffxy"])
+        np.testing.assert_allclose(r, d["rcs_%s_vv" % mode], rtol=1e-12, atol=0)
+
+
 def test_kodis_field():
     d = load("kodis.npz")
     m = nrcs.RCSKodis(d["inc"], float(d["k0"]), 1.0, 1.0)
@@ -214,13 +230,13 @@ def _cfg_json(cfg):
 def test_cfg_parser():
     with open(os.path.join(G, "cfg_parsed.json")) as f:
         ref = json.load(f)
-    for name in ("quirks", "c1small", "c2small", "c3small", "c1lut"):
+    for name in ("quirks", "c1small", "c2small", "c3small", "c1lut", "c1fa", "c1spa"):
         cfg = ConfigFile(os.path.join(G, "cfg", name + ".cfg"))
         assert cfg.sections[1:] == ref[name]["sections"]
         assert _cfg_json(cfg) == ref[name]["values"]
 
 
-@pytest.mark.parametrize("name", ["c1small", "c2small", "c3small", "c1lut"])
+@pytest.mark.parametrize("name", ["c1small", "c2small", "c3small", "c1lut", "c1fa", "c1spa"])
 def test_sar_raw_end_to_end(name):
     d = load("sar_raw_%s.npz" % name)
     raw, nrcs_avg, sim = sar_raw(os.path.join(G, "cfg", name + ".cfg"), seed=0)
