@@ -223,6 +223,13 @@ typedef struct {
     const void *lut_d;
     int32_t lut_naz, lut_ndy, lut_ndx;
     double lut_az0, lut_daz, lut_dy0, lut_ddy, lut_dx0, lut_ddx;
+    /* Specular model when do_kodis is set: 0 Kodis (kodis.py), 1 Kirchhoff facet approach,
+     * 2 Kirchhoff stationary phase (ka.py; sar_raw_nompi.py:402-426, per polarisation
+     * exp(-2j k0 r) (4 pi)^1.5 RCSKA.field).  x_d: float32 [nx] facet x positions (Kirchhoff
+     * only); ka_dx / ka_dy: facet sizes; ka_K: RCSKA's constant for R_i = R_s = 1. */
+    int32_t spec_mode;
+    const float *x_d;
+    double ka_dx, ka_dy, ka_K_re, ka_K_im;
 } ocs_pulse_desc;
 
 /* Workspace of ocs_pulse (per-pulse table of the row quantities); < 0 on invalid sizes. */
@@ -270,6 +277,25 @@ typedef struct {
 } ocs_kodis_desc;
 
 int ocs_field_kodis(const ocs_kodis_desc *desc, void *stream);
+
+/* ocs_field_ka replaces RCSKA.field (oceansar/nrcs/ka.py:110-284), monostatic: complex128
+ * [ny][nx] Kirchhoff-approximation field by the facet approach (mode 0) or the stationary-
+ * phase approximation (mode 1) for incident / scattered polarisations pol_i, pol_s (0 = h,
+ * 1 = v).  theta / phi are broadcast to the grid through their strides (elements). */
+typedef struct {
+    int32_t nx, ny;
+    const double *x_d, *y_d;                           /* float64 [nx], [ny] facet positions   */
+    const double *theta_d; int64_t theta_row_stride, theta_col_stride;   /* incidence [rad]  */
+    const double *phi_d; int64_t phi_row_stride, phi_col_stride;         /* azimuth [rad]    */
+    const float *dz_d, *diffx_d, *diffy_d;             /* float32 [ny][nx]                     */
+    const float *diffxx_d, *diffyy_d, *diffxy_d;       /* float32 [ny][nx] (mode 1 only)       */
+    double k0, dx, dy;
+    double K_re, K_im;                                 /* -1j k0 exp(-1j k0 (R_i+R_s)) / ((4 pi)^2 R_i R_s) */
+    int32_t mode, pol_i, pol_s;
+    double *out_d;                                     /* complex128 [ny][nx]                  */
+} ocs_ka_desc;
+
+int ocs_field_ka(const ocs_ka_desc *desc, void *stream);
 
 /* ---- Scene batch ----------------------------------------------------------------------
  * Many independent scenes (any mix of grid sizes, geometries and channel counts) advanced

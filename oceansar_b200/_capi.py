@@ -47,6 +47,7 @@ SIGNATURES = {
     "ocs_pulse_workspace_bytes": [ctypes.c_int32, ctypes.c_int32],
     "ocs_rcs_romeiser": [c_ptr, c_ptr],
     "ocs_field_kodis": [c_ptr, c_ptr],
+    "ocs_field_ka": [c_ptr, c_ptr],
     "ocs_batch_create": [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(c_ptr)],
     "ocs_batch_destroy": [c_ptr],
     "ocs_batch_set": [c_ptr, ctypes.c_int32, c_ptr, c_ptr],

@@ -35,7 +35,8 @@ class PulseDesc(ctypes.Structure):
                 ("nrcs_spec_d", P), ("nrcs_bragg_d", P), ("rowtab_d", P),
                 ("lut_d", P), ("lut_naz", I32), ("lut_ndy", I32), ("lut_ndx", I32),
                 ("lut_az0", F64), ("lut_daz", F64), ("lut_dy0", F64), ("lut_ddy", F64),
-                ("lut_dx0", F64), ("lut_ddx", F64)]
+                ("lut_dx0", F64), ("lut_ddx", F64),
+                ("spec_mode", I32), ("x_d", P), ("ka_dx", F64), ("ka_dy", F64), ("ka_K_re", F64), ("ka_K_im", F64)]
 
 
 class RcsDesc(ctypes.Structure):
@@ -66,3 +67,13 @@ class SceneDesc(ctypes.Structure):
     _fields_ = [("surface", ctypes.c_void_p), ("pulse", ctypes.c_void_p), ("tile_rows", ctypes.c_int32),
                 ("t_d", ctypes.c_void_p), ("add_d", ctypes.c_void_p), ("swell_rot_d", ctypes.c_void_p),
                 ("az_now_d", ctypes.c_void_p), ("flags_d", ctypes.c_void_p), ("tmod_d", ctypes.c_void_p)]
+
+
+class KaDesc(ctypes.Structure):
+    """``ocs_ka_desc``: Kirchhoff-approximation field."""
+    _fields_ = [("nx", I32), ("ny", I32), ("x_d", P), ("y_d", P),
+                ("theta_d", P), ("theta_row_stride", I64), ("theta_col_stride", I64),
+                ("phi_d", P), ("phi_row_stride", I64), ("phi_col_stride", I64),
+                ("dz_d", P), ("diffx_d", P), ("diffy_d", P), ("diffxx_d", P), ("diffyy_d", P), ("diffxy_d", P),
+                ("k0", F64), ("dx", F64), ("dy", F64), ("K_re", F64), ("K_im", F64),
+                ("mode", I32), ("pol_i", I32), ("pol_s", I32), ("out_d", P)]

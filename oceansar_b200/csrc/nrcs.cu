@@ -111,3 +111,65 @@ extern "C" int ocs_field_kodis(const ocs_kodis_desc *d, void *stream) {
     kodis_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(a);
     return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
 }
+
+// ---------------------------------------------------------------------------------------
+// Kirchhoff-approximation specular field (RCSKA.field, oceansar/nrcs/ka.py:110-284).
+namespace ocs {
+struct KaArgs {
+    int nx, ny;
+    const double *x, *y;
+    const double *theta;
+    long long th_rs, th_cs;
+    const double *phi;
+    long long ph_rs, ph_cs;
+    const float *dz, *diffx, *diffy, *diffxx, *diffyy, *diffxy;
+    KaParams kp;
+    int pol_i, pol_s;
+    double *out;
+};
+
+__global__ void ka_kernel(const __grid_constant__ KaArgs a) {
+    const long long n = (long long)a.nx * a.ny;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(i / a.nx), c = (int)(i - (long long)r * a.nx);
+        const double th = a.theta[r * a.th_rs + c * a.th_cs];
+        const double ph = a.phi[r * a.ph_rs + c * a.ph_cs];
+        double st, ct, sp, cp;
+        sincos(th, &st, &ct);
+        sincos(ph, &sp, &cp);
+        const c128 e = ka_facet(a.kp, a.pol_i, a.pol_s, a.x[c], a.y[r], st, ct, tan(th), sp, cp, a.dz[i], a.diffx[i],
+                                a.diffy[i], a.diffxx[i], a.diffyy[i], a.diffxy[i]);
+        a.out[2 * i] = e.re;
+        a.out[2 * i + 1] = e.im;
+    }
+}
+}  // namespace ocs
+
+extern "C" int ocs_field_ka(const ocs_ka_desc *d, void *stream) {
+    if (!d || d->nx < 1 || d->ny < 1 || !d->x_d || !d->y_d || !d->theta_d || !d->phi_d || !d->dz_d ||
+        !d->diffx_d || !d->diffy_d || !d->out_d)
+        return OCS_ERR_ARG;
+    if (d->mode != 0 && d->mode != 1) return OCS_ERR_ARG;
+    if (d->mode == 1 && (!d->diffxx_d || !d->diffyy_d || !d->diffxy_d)) return OCS_ERR_ARG;
+    if ((d->pol_i != 0 && d->pol_i != 1) || (d->pol_s != 0 && d->pol_s != 1)) return OCS_ERR_ARG;
+    KaArgs a;
+    memset(&a, 0, sizeof(a));
+    a.nx = d->nx; a.ny = d->ny;
+    a.x = d->x_d; a.y = d->y_d;
+    a.theta = d->theta_d; a.th_rs = d->theta_row_stride; a.th_cs = d->theta_col_stride;
+    a.phi = d->phi_d; a.ph_rs = d->phi_row_stride; a.ph_cs = d->phi_col_stride;
+    a.dz = d->dz_d; a.diffx = d->diffx_d; a.diffy = d->diffy_d;
+    // the facet approach never reads the curvatures; give it valid pointers anyway
+    a.diffxx = d->diffxx_d ? d->diffxx_d : d->diffx_d;
+    a.diffyy = d->diffyy_d ? d->diffyy_d : d->diffx_d;
+    a.diffxy = d->diffxy_d ? d->diffxy_d : d->diffx_d;
+    a.kp.k0 = d->k0; a.kp.dx = d->dx; a.kp.dy = d->dy; a.kp.K_re = d->K_re; a.kp.K_im = d->K_im;
+    a.kp.mode = d->mode;
+    a.pol_i = d->pol_i; a.pol_s = d->pol_s;
+    a.out = d->out_d;
+    const long long n = (long long)d->nx * d->ny;
+    long long blocks = (n + 255) / 256;
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    ka_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(a);
+    return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
+}

@@ -7,6 +7,8 @@
 //   interpolation of the omni-directional spectrum on k = 1, 1.1, ... < 2 k0, fill 1
 //   outside, times the spreading function) and the bad_ones mask.
 // * kodis_facet: the Kodis (1966) stationary-phase specular field, oceansar/nrcs/kodis.py:38-73.
+// * ka_facet: the monostatic Kirchhoff-approximation field of a facet, oceansar/nrcs/ka.py:110-284
+//   (facet approach and stationary-phase approximation).
 #pragma once
 #include "common.cuh"
 
@@ -203,6 +205,109 @@ OCS_D cplx<T> kodis_facet(const KodisParams &kp, double sr, double sin_inc, doub
     }
     v = cmul(v, e);
     return {v.re / sq, v.im / sq};
+}
+
+// Principal square root of a complex number: t = sqrt((|z| + |re|) / 2) on the larger side.
+OCS_D c128 csqrt128(c128 z) {
+    const double r = hypot(z.re, z.im);
+    if (z.re >= 0.0) {
+        const double t = sqrt(0.5 * (r + z.re));
+        return {t, t == 0.0 ? 0.0 : z.im / (2.0 * t)};
+    }
+    const double t = sqrt(0.5 * (r - z.re));
+    return {fabs(z.im) / (2.0 * t), copysign(t, z.im)};
+}
+
+OCS_D c128 cmulr(c128 a, double s) { return {dmul(a.re, s), dmul(a.im, s)}; }
+OCS_D c128 cmul128(c128 a, c128 b) {
+    return {dsub(dmul(a.re, b.re), dmul(a.im, b.im)), dadd(dmul(a.re, b.im), dmul(a.im, b.re))};
+}
+
+struct KaParams {
+    double k0, dx, dy;
+    double K_re, K_im;        // -1j k0 exp(-1j k0 (R_i + R_s)) / ((4 pi)^2 R_i R_s)
+    int mode;                 // 0: facet approach, 1: stationary phase
+};
+
+// Monostatic Kirchhoff field of one facet (RCSKA.field, ka.py:110-284) for the incident /
+// scattered polarisations pol_i, pol_s (0 = h, 1 = v).  st, ct, tt: sin / cos / tan of the
+// incidence; sp, cp: sin / cos of the azimuth; (x, y) the facet position.  The float32
+// surface derivatives enter as the reference combines them: the normal's norm and
+// components, the curvature determinant and its inverse are float32 quantities.
+OCS_D c128 ka_facet(const KaParams &kp, int pol_i, int pol_s, double x, double y, double st, double ct,
+                    double tt, double sp, double cp, float Dz, float Dx, float Dy, float Dxx, float Dyy,
+                    float Dxy) {
+    const double hv[2][3] = {{-sp, cp, 0.0}, {-(ct * cp), -(ct * sp), -st}};
+    const double *ai = hv[pol_i], *as = hv[pol_s];
+    const float nn = sqrtf(fadd(fadd(fmul(Dx, Dx), fmul(Dy, Dy)), 1.f));
+    const double n[3] = {(double)__fdiv_rn(-Dx, nn), (double)__fdiv_rn(-Dy, nn), (double)__fdiv_rn(1.f, nn)};
+    const double ni[3] = {st * cp, st * sp, -ct};
+    const double ns[3] = {-(st * cp), -(st * sp), ct};
+    const double q[3] = {kp.k0 * (ns[0] - ni[0]), kp.k0 * (ns[1] - ni[1]), kp.k0 * (ns[2] - ni[2])};
+    double t[3] = {ni[1] * n[2] - ni[2] * n[1], ni[2] * n[0] - ni[0] * n[2], ni[0] * n[1] - ni[1] * n[0]};
+    const double tn = sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+    t[0] /= tn; t[1] /= tn; t[2] /= tn;
+    const double d[3] = {ni[1] * t[2] - ni[2] * t[1], ni[2] * t[0] - ni[0] * t[2], ni[0] * t[1] - ni[1] * t[0]};
+    const double cos_l = -(n[0] * ni[0] + n[1] * ni[1] + n[2] * ni[2]);
+    // Fresnel coefficients, eps = 73 + 18j
+    const c128 root = csqrt128({73.0 + cos_l * cos_l - 1.0, 18.0});
+    const c128 ec = {73.0 * cos_l, 18.0 * cos_l};
+    const c128 r_v = cdiv<double>({ec.re - root.re, ec.im - root.im}, {ec.re + root.re, ec.im + root.im});
+    const c128 r_h = cdiv<double>({cos_l - root.re, -root.im}, {cos_l + root.re, root.im});
+    const double a_t = ai[0] * t[0] + ai[1] * t[1] + ai[2] * t[2];
+    const double a_d = ai[0] * d[0] + ai[1] * d[1] + ai[2] * d[2];
+    const double n_ni = -cos_l;
+    const double nxt[3] = {n[1] * t[2] - n[2] * t[1], n[2] * t[0] - n[0] * t[2], n[0] * t[1] - n[1] * t[0]};
+    const c128 c1 = cmulr({1.0 + r_h.re, r_h.im}, a_t);
+    const c128 c2 = cmulr(cmulr({1.0 - r_v.re, -r_v.im}, n_ni), a_d);
+    const c128 c3 = cmulr(cmulr({1.0 - r_h.re, -r_h.im}, n_ni), a_t);
+    const c128 c4 = cmulr({1.0 + r_v.re, r_v.im}, a_d);
+    c128 es[3], hs[3];
+    for (int k = 0; k < 3; ++k) {
+        es[k] = {c1.re * nxt[k] - c2.re * t[k], c1.im * nxt[k] - c2.im * t[k]};
+        hs[k] = {-(c3.re * t[k] + c4.re * nxt[k]), -(c3.im * t[k] + c4.im * nxt[k])};
+    }
+    // p = a_s . (n_s x (n x E_s - n_s x eta n x H_s))
+    c128 u[3];
+    for (int k = 0; k < 3; ++k) {
+        const int k1 = (k + 1) % 3, k2 = (k + 2) % 3;
+        const c128 w = {ns[k1] * hs[k2].re - ns[k2] * hs[k1].re, ns[k1] * hs[k2].im - ns[k2] * hs[k1].im};
+        u[k] = {es[k].re - w.re, es[k].im - w.im};
+    }
+    c128 p = {0.0, 0.0};
+    for (int k = 0; k < 3; ++k) {
+        const int k1 = (k + 1) % 3, k2 = (k + 2) % 3;
+        const c128 z = {ns[k1] * u[k2].re - ns[k2] * u[k1].re, ns[k1] * u[k2].im - ns[k2] * u[k1].im};
+        p = {p.re + as[k] * z.re, p.im + as[k] * z.im};
+    }
+    const c128 K = {kp.K_re, kp.K_im};
+    if (kp.mode == 1) {
+        const float J = fsub(fmul(Dxx, Dyy), fmul(Dxy, Dxy));
+        if (J == 0.f) return {0.0, 0.0};                      // J -> NaN: never stationary
+        const float J_abs = fabsf(J);
+        const double inv_j = (double)__fdiv_rn(1.f, J_abs);
+        const double tsp = dmul(tt, sp), tcp = dmul(tt, cp);
+        const double dxv = dmul(inv_j, dsub(dmul((double)Dxy, dsub((double)Dy, tsp)), dmul((double)Dyy, dsub((double)Dx, tcp))));
+        const double dyv = dmul(inv_j, dsub(dmul((double)Dxy, dsub((double)Dx, tcp)), dmul((double)Dxx, dsub((double)Dy, tsp))));
+        const double hx = 0.5 * kp.dx, hy = 0.5 * kp.dy;
+        if (!((-hx < dxv) && (dxv < hx) && (-hy < dyv) && (dyv < hy))) return {0.0, 0.0};
+        const double dzv = dadd(dmul(dxv, (double)Dx), dmul(dyv, (double)Dy));
+        const c128 eps = (J > 0.f) ? c128{(double)((Dxx > 0.f) - (Dxx < 0.f)), 0.0} : c128{0.0, 1.0};
+        c128 e = cmul128(cmul128(eps, p), K);
+        e = cmul128(e, cexpi(dadd(dadd(dmul(q[0], dxv), dmul(q[1], dyv)), dmul(q[2], dzv))));
+        e = cmulr(cmulr(e, 2.0), 3.141592653589793);
+        e = {ddiv(e.re, q[2]), ddiv(e.im, q[2])};
+        e = cmulr(e, (double)nn);
+        const double sj = (double)sqrtf(J_abs);
+        return {ddiv(e.re, sj), ddiv(e.im, sj)};
+    }
+    // facet approach: I = exp(-i q.r) |n| dx dy sinc((q_x + q_z Diffx) dx/2) sinc((q_y + q_z Diffy) dy/2)
+    const double qr = dadd(dadd(dmul(q[0], x), dmul(q[1], y)), dmul(q[2], (double)Dz));
+    c128 I = cexpi(-qr);
+    I = cmulr(cmulr(cmulr(I, (double)nn), kp.dx), kp.dy);
+    I = cmulr(I, np_sinc(ddiv(dmul(dadd(q[0], dmul(q[2], (double)Dx)), kp.dx), 2.0)));
+    I = cmulr(I, np_sinc(ddiv(dmul(dadd(q[1], dmul(q[2], (double)Dy)), kp.dy), 2.0)));
+    return cmul128(cmul128(K, I), p);
 }
 
 }  // namespace ocs

@@ -62,10 +62,25 @@ struct PulseArgs {
     double *nrcs_bragg;                     // [npol][az_steps] sum RCS (refresh pulses)
     int az_steps;
     int tile_rows;                          // rows per tile of a single-scene launch
+    int spec_mode;                          // 0 Kodis, 1 Kirchhoff facet approach, 2 stationary phase
+    const float *x_f;                       // [nx] facet x positions (Kirchhoff)
+    KaParams ka;
     const void *lut;                        // Romeiser LUT [npol][2][naz][ndy][ndx] (T), or null
     int lut_naz, lut_ndy, lut_ndx;
     double lut_az0, lut_daz, lut_dy0, lut_ddy, lut_dx0, lut_ddx;
 };
+
+// Kirchhoff specular term of one facet and polarisation code pc (0 = hh, 1 = vv),
+// sar_raw_nompi.py:402-426: exp(-1j (2 k0 r)) (4 pi)^1.5 RCSKA.field(1, 1, ...).  Only the
+// Kirchhoff instantiations of the pulse kernel (KA = true) contain it.
+OCS_D c128 ka_specular(const KaParams &kp, int pc, double srs, double x, double y, double st,
+                                         double ct, double tt, double sp, double cp, float dz, float dx, float dy,
+                                         float dxx, float dyy, float dxy) {
+    const c128 e = ka_facet(kp, pc, pc, x, y, st, ct, tt, sp, cp, dz, dx, dy, dxx, dyy, dxy);
+    const c128 ph = cexpi(-dmul(2.0 * kp.k0, srs));
+    const double s15 = 44.54662397465366;                // (4 pi)^1.5
+    return cmul128(cmulr(ph, s15), e);
+}
 
 // LUT mode of the Romeiser model (romeiser97.py:109-134): RCS of both Bragg lines of
 // polarisation p at (azimuth index of the row, clamped slope indices of the facet).
@@ -274,7 +289,7 @@ OCS_D PulseSmem<T> pulse_smem(unsigned char *smem, int nch) {
 // One tile of kPulseCols columns x tile_rows rows: NRCS, scene and accumulation of every
 // facet into this pulse's raw rows; the tile's NRCS sums are added to spec_sum and
 // bragg_sum.
-template <typename T, int NOUT, int S, int RCAP>
+template <typename T, int NOUT, int S, int RCAP, bool KA = false>
 OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSmem<T> &sm, double &spec_sum,
                       double (&bragg_sum)[2]) {
     const int tiles_x = (a.nx + kPulseCols - 1) / kPulseCols;
@@ -359,7 +374,17 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
             else bin_and_lut_fast(srs, a.min_sr, a.inv_binsize, kSincOvs, bin_d, lut);
 
             cplx<T> scene[2] = {{(T)0, (T)0}, {(T)0, (T)0}};      // per polarisation
-            if (a.do_kodis) {
+            if constexpr (KA) {
+                c128 last = {0.0, 0.0};
+                for (int p = 0; p < a.npol; ++p) {
+                    const int pc = a.rom.pol == POL_DP ? p : (a.rom.pol == POL_HH ? 0 : 1);
+                    last = ka_specular(a.ka, pc, srs, (double)a.x_f[x], (double)a.y[y0 + i], sin_i, cos_i, tan_i,
+                                       sm.r_az[4 * RCAP + i], sm.r_az[3 * RCAP + i], cur.dz, cur.diffx, cur.diffy,
+                                       cur.diffxx, cur.diffyy, cur.diffxy);
+                    scene[p] = {(T)last.re, (T)last.im};
+                }
+                spec_sum += last.re * last.re + last.im * last.im;
+            } else if (a.do_kodis) {
                 const cplx<T> e = kodis_facet<T>(a.kodis, srs, sin_i, cos_i, tan_i, sm.r_az[3 * RCAP + i], sm.r_az[4 * RCAP + i],
                                                  cur.diffx, cur.diffy, cur.diffxx, cur.diffyy, cur.diffxy);
                 const T s4 = (T)3.5449077018110318;                 // sqrt(4 pi)
@@ -477,7 +502,7 @@ OCS_D void pulse_nrcs(const PulseArgs &a, const PulseSmem<T> &sm, double spec_su
     }
 }
 
-template <typename T, int NOUT, int S>
+template <typename T, int NOUT, int S, bool KA>
 __global__ void __launch_bounds__(kPulseCols, (sizeof(T) == 4 && NOUT < 4) ? 4 : 2)
 pulse_kernel(const __grid_constant__ PulseArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -487,7 +512,7 @@ pulse_kernel(const __grid_constant__ PulseArgs a) {
     double spec_sum = 0.0, bragg_sum[2] = {0.0, 0.0};
     // persistent CTAs: each walks tiles of kPulseCols columns x tile_rows rows
     for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x)
-        pulse_tile<T, NOUT, S, kPulseRows>(a, tile, a.tile_rows, sm, spec_sum, bragg_sum);
+        pulse_tile<T, NOUT, S, kPulseRows, KA>(a, tile, a.tile_rows, sm, spec_sum, bragg_sum);
     pulse_nrcs<T>(a, sm, spec_sum, bragg_sum);
 }
 
@@ -579,7 +604,7 @@ batch_pulse_kernel(const __grid_constant__ BatchRef b) {
 template <typename T, int NOUT, int S>
 static int launch_pulse(PulseArgs a, cudaStream_t st) {
     const size_t smem = pulse_smem_bytes<T, NOUT, S, kPulseRows>(a.nch);
-    auto k = pulse_kernel<T, NOUT, S>;
+    auto k = a.spec_mode != 0 ? pulse_kernel<T, NOUT, S, true> : pulse_kernel<T, NOUT, S, false>;
     if (ensure_smem((const void *)k, smem) != cudaSuccess)
         return OCS_ERR_CUDA;
     const int resident = resident_ctas((const void *)k, kPulseCols, smem);
@@ -665,6 +690,12 @@ static int fill_pulse_args(const ocs_pulse_desc *d, PulseArgs &a) {
     a.raw_out_stride = (long long)d->az_steps * d->nbins;
     a.raw_row = (long long)d->az_step * d->nbins;
     a.nrcs_spec = d->nrcs_spec_d; a.nrcs_bragg = d->nrcs_bragg_d; a.az_steps = d->az_steps;
+    a.spec_mode = d->do_kodis ? d->spec_mode : 0;
+    if (a.spec_mode < 0 || a.spec_mode > 2) return OCS_ERR_ARG;
+    if (a.spec_mode != 0 && !d->x_d) return OCS_ERR_ARG;
+    a.x_f = d->x_d;
+    a.ka.k0 = d->k0; a.ka.dx = d->ka_dx; a.ka.dy = d->ka_dy; a.ka.K_re = d->ka_K_re; a.ka.K_im = d->ka_K_im;
+    a.ka.mode = a.spec_mode == 2 ? 1 : 0;
     a.lut = d->lut_d;
     if (a.lut) {
         if (d->lut_naz < 1 || d->lut_ndy < 1 || d->lut_ndx < 1 || !(d->lut_daz != 0.0) || !(d->lut_ddy != 0.0) ||

@@ -10,13 +10,15 @@
   does (on the host for ``rcs``, inside the pulse kernel for ``sar_raw``).
 * ``RCSKodis`` -- stationary-phase specular field (``nrcs/kodis.py:27-73``) behind
   ``ocs_field_kodis``.
+* ``RCSKA`` -- Kirchhoff-approximation specular field (``nrcs/ka.py:41-310``), facet
+  approach ('fa') or stationary phase ('spa'), monostatic, behind ``ocs_field_ka``.
 """
 import ctypes
 
 import numpy as np
 
 from .. import _capi, _device, spec, spread
-from .._structs import KodisDesc, RcsDesc
+from .._structs import KaDesc, KodisDesc, RcsDesc
 
 EPS_SW = 73 + 18j
 POL_CODES = {'vv': 0, 'hh': 1, 'DP': 2}
@@ -246,4 +248,51 @@ class RCSKodis(object):
         return out.cpu().numpy()
 
 
-models = {'kodis': RCSKodis, 'romeiser97': RCSRomeiser97}
+
+
+class RCSKA(object):
+    """Kirchhoff approximation (``nrcs/ka.py:41-310``), mode 'fa' or 'spa'."""
+
+    def __init__(self, mode, k0, x, y, dx, dy):
+        if mode not in ('fa', 'spa'):
+            raise ValueError('mode must be fa or spa')
+        self.mode, self.k0, self.dx, self.dy = mode, k0, dx, dy
+        self.x = np.asarray(x, dtype=np.float64)
+        self.y = np.asarray(y, dtype=np.float64)
+        self.shape = [self.y.shape[0], self.x.shape[0], 3]
+        self._xy = None
+
+    def constant(self, R_i=1, R_s=1):
+        """K = -1j k0 exp(-1j k0 (R_i + R_s)) / ((4 pi)^2 R_i R_s), as numpy evaluates it."""
+        return complex(-1j * self.k0 * np.exp(-1j * self.k0 * (R_i + R_s)) / ((4. * np.pi) ** 2. * R_i * R_s))
+
+    def device_positions(self):
+        if self._xy is None:
+            self._xy = (_device.to_device(self.x, np.float64), _device.to_device(self.y, np.float64))
+        return self._xy
+
+    def field(self, R_i, R_s, pol_i, pol_s, theta_i, theta_s, phi_i, phi_s, Dz, Diffx, Diffy, Diffxx, Diffyy,
+              Diffxy, monostatic=True):
+        if not monostatic:
+            raise NotImplementedError('bistatic Kirchhoff geometry is not built')
+        ny, nx = np.shape(Dz)
+        xd, yd = self.device_positions()
+        th = np.asarray(theta_i, dtype=np.float64).reshape(1, -1)
+        thd, trs, tcs = _broadcast_strides(th if th.size > 1 else th.reshape(()), ny, nx)
+        phd, prs, pcs = _broadcast_strides(phi_i, ny, nx)
+        f = [_device.to_device(a, np.float32) for a in (Dz, Diffx, Diffy, Diffxx, Diffyy, Diffxy)]
+        out = _device.empty((ny, nx), np.complex128)
+        K = self.constant(R_i, R_s)
+        desc = KaDesc(nx, ny, xd.data_ptr(), yd.data_ptr(), thd.data_ptr(), trs, tcs, phd.data_ptr(), prs, pcs,
+                      *[t.data_ptr() for t in f], float(self.k0), float(self.dx), float(self.dy), K.real, K.imag,
+                      0 if self.mode == 'fa' else 1, 0 if pol_i == 'h' else 1, 0 if pol_s == 'h' else 1,
+                      out.data_ptr())
+        _capi.call("ocs_field_ka", ctypes.addressof(desc), _device.stream_ptr())
+        return out.cpu().numpy()
+
+    def rcs(self, pol_i, pol_s, theta_i, theta_s, phi_i, phi_s, Dz, Diffx, Diffy, Diffxx, Diffyy, Diffxy):
+        return (4. * np.pi) ** 2. * np.abs(self.field(1, 1, pol_i, pol_s, theta_i, theta_s, phi_i, phi_s, Dz, Diffx,
+                                                     Diffy, Diffxx, Diffyy, Diffxy)) ** 2.
+
+
+models = {'ka': RCSKA, 'kodis': RCSKodis, 'romeiser97': RCSRomeiser97}

@@ -84,6 +84,8 @@ class SceneBatch(object):
         """Place ``gen`` (a RawGenerator of this batch's precision) in a slot; returns it."""
         if gen.precision != self.precision:
             raise ValueError('scene precision %s differs from the batch (%s)' % (gen.precision, self.precision))
+        if gen.scat_spec_enable and gen.scat_spec_mode != 'kodis':
+            raise NotImplementedError('Kirchhoff specular scenes run through RawGenerator, not the scene batch')
         if gen.surface.choppy_enable:
             raise NotImplementedError('choppy surfaces run through RawGenerator, not the scene batch')
         if slot is None:

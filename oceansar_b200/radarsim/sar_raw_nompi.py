@@ -84,9 +84,8 @@ class RawGenerator(object):
         self.use_hmtf = bool(srg.use_hmtf)
         self.scat_spec_enable = bool(srg.scat_spec_enable)
         self.scat_bragg_enable = bool(srg.scat_bragg_enable)
-        if self.scat_spec_enable and srg.scat_spec_mode != 'kodis':
-            if srg.scat_spec_mode in ('fa', 'spa'):
-                raise NotImplementedError('Kirchhoff (fa / spa) specular scattering is not built')
+        self.scat_spec_mode = srg.scat_spec_mode if self.scat_spec_enable else 'kodis'
+        if self.scat_spec_enable and self.scat_spec_mode not in ('kodis', 'fa', 'spa'):
             raise NotImplementedError('RCS mode %s for specular scattering not implemented' % srg.scat_spec_mode)
         if self.scat_bragg_enable and srg.scat_bragg_model != 'romeiser97':
             raise NotImplementedError('RCS model %s for Bragg scattering not implemented' % srg.scat_bragg_model)
@@ -161,7 +160,12 @@ class RawGenerator(object):
 
         # ---- scattering models (:293-340; global RNG draw 2: rndscat_p then rndscat_m) ---
         if self.scat_spec_enable:
-            self.rcs_spec = nrcs.RCSKodis(self.inc, k0, s.dx, s.dy)
+            if self.scat_spec_mode == 'kodis':
+                self.rcs_spec = nrcs.RCSKodis(self.inc, k0, s.dx, s.dy)
+            else:
+                # sar_raw_nompi.py:296-299: the reference draws a phase screen here (unused)
+                self.spec_ph0 = np.random.uniform(0., 2. * np.pi, size=[s.Ny, s.Nx])
+                self.rcs_spec = nrcs.RCSKA(self.scat_spec_mode, k0, s.x, s.y, s.dx, s.dy)
         if self.scat_bragg_enable:
             tau_c = grid_coherence(oc.wind_U, s.dx, f0)
             self.rndscat_p = randomscat_ts(tau_c, (s.Ny, s.Nx), self.prf)
@@ -238,7 +242,15 @@ class RawGenerator(object):
             int(self.use_hmtf)
         d.facet_dx, d.facet_dy = float(s.dx), float(s.dy)
         if self.scat_spec_enable:
-            d.kodis_R_re, d.kodis_R_im = float(self.rcs_spec.R.real), float(self.rcs_spec.R.imag)
+            if self.scat_spec_mode == 'kodis':
+                d.kodis_R_re, d.kodis_R_im = float(self.rcs_spec.R.real), float(self.rcs_spec.R.imag)
+            else:
+                d.spec_mode = 1 if self.scat_spec_mode == 'fa' else 2
+                self._x_d = _device.to_device(s.x, np.float32)
+                d.x_d = self._x_d.data_ptr()
+                d.ka_dx, d.ka_dy = float(s.dx), float(s.dy)
+                K = self.rcs_spec.constant(1, 1)
+                d.ka_K_re, d.ka_K_im = K.real, K.imag
         if self.scat_bragg_enable:
             self.rcs_bragg.fill(d)
             d.bragg_d = float(self.rcs_bragg.d)

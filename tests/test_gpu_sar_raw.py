@@ -53,7 +53,7 @@ def stagewise(name, precision, steps=None):
     return got, ref, gen, osim
 
 
-@pytest.mark.parametrize("name", ["c1small", "c2small", "c3small", "c1lut"])
+@pytest.mark.parametrize("name", ["c1small", "c2small", "c3small", "c1lut", "c1fa", "c1spa"])
 def test_stagewise_f64(name):
     got, ref, gen, osim = stagewise(name, "f64")
     assert rel_l2(got, ref) < 1e-10, rel_l2(got, ref)
@@ -62,7 +62,7 @@ def test_stagewise_f64(name):
     np.testing.assert_allclose(nr, nref, rtol=1e-9)
 
 
-@pytest.mark.parametrize("name", ["c1small", "c2small", "c3small", "c1lut"])
+@pytest.mark.parametrize("name", ["c1small", "c2small", "c3small", "c1lut", "c1fa", "c1spa"])
 def test_stagewise_mixed(name):
     got, ref, gen, osim = stagewise(name, "mixed")
     assert got.dtype == np.complex64
@@ -70,7 +70,7 @@ def test_stagewise_mixed(name):
     assert e < 1e-4 and ph < 1e-3, (e, ph)
 
 
-@pytest.mark.parametrize("name", ["c1small", "c2small", "c3small", "c1lut"])
+@pytest.mark.parametrize("name", ["c1small", "c2small", "c3small", "c1lut", "c1fa", "c1spa"])
 @pytest.mark.parametrize("precision", ["f64", "mixed"])
 def test_end_to_end_against_reference(name, precision):
     from oceansar_b200.radarsim.sar_raw_nompi import RawGenerator
@@ -105,6 +105,23 @@ def test_standalone_rcs_lut_golden():
             fin = np.isfinite(ref)
             np.testing.assert_array_equal(np.isfinite(got), fin)
             np.testing.assert_allclose(got[fin], ref[fin], rtol=1e-10, atol=1e-300)
+
+
+def test_standalone_ka_golden():
+    """Kirchhoff specular field (nrcs/ka.py) on the GPU against the reference's own output."""
+    from oceansar_b200 import nrcs
+    d = np.load(os.path.join(G, "ka.npz"))
+    for mode in ("fa", "spa"):
+        m = nrcs.RCSKA(mode, float(d["k0"]), d["x"], d["y"], 1.0, 1.0)
+        for pp in ("hh", "vv", "hv", "vh"):
+            E = m.field(1, 1, pp[0], pp[1], d["inc"], d["inc"], d["az"], d["az"] + np.pi, d["Dz"], d["Diffx"],
+                        d["Diffy"], d["Diffxx"], d["Diffyy"], d["Diffxy"])
+            ref = d["E_%s_%s" % (mode, pp)]
+            np.testing.assert_array_equal(E != 0, ref != 0)
+            assert rel_l2(E, ref) < 1e-10, (mode, pp, rel_l2(E, ref))
+        r = m.rcs('v', 'v', d["inc"], d["inc"], d["az"], d["az"] + np.pi, d["Dz"], d["Diffx"], d["Diffy"],
+                  d["Diffxx"], d["Diffyy"], d["Diffxy"])
+        assert rel_l2(r, d["rcs_%s_vv" % mode]) < 1e-10
 
 
 def test_standalone_rcs_and_kodis_golden():
