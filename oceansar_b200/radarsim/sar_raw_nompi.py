@@ -25,6 +25,7 @@ from .. import _capi, _device, nrcs, swell_spec
 from .._structs import PulseDesc
 from ..closure import grid_coherence, randomscat_ts
 from ..ocs_io.cfg import ConfigFile
+from ..ocs_io.raw import RawFile
 from ..surfaces import OceanSurface
 from ..utils import geometry as geo
 from ..utils.misc import db2lin, optimize_fftsize
@@ -481,9 +482,11 @@ def sar_raw(cfg_file, output_file, ocean_file, reuse_ocean_file, errors_file, re
             plot_save=True, precision='f64'):
     """Drop-in for ``sar_raw_nompi.sar_raw``: simulate and write the raw file.
 
-    The raw file and the ocean state file are ``.npz`` containers holding the reference's
-    variable names (``raw_data_r``/``raw_data_i`` [pol, ch, az, rg], ``NRCS_avg``, ...).
-    ``errors_file`` / ``plot_save`` are accepted and unused, as in the reference.
+    The raw file (``RawFile``: ``raw_data_r``/``raw_data_i`` [pol, ch, az, rg], ``NRCS_avg``,
+    geometry scalars, baselines) and the ocean state file (``OceanStateFile``) are netCDF
+    classic files with the reference's dimensions, variables and units; a file name ending
+    in ``.npz`` gets the same variables in a numpy container instead.  ``errors_file`` /
+    ``plot_save`` are accepted and unused, as in the reference.
     """
     cfg = ConfigFile(cfg_file)
     gen = RawGenerator(cfg, precision=precision)
@@ -492,8 +495,17 @@ def sar_raw(cfg_file, output_file, ocean_file, reuse_ocean_file, errors_file, re
     gen.run()
     total_raw, nrcs_avg = gen.finish(add_noise=True)
     if output_file:
-        np.savez(output_file, raw_data_r=total_raw.real, raw_data_i=total_raw.imag, NRCS_avg=nrcs_avg,
-                 inc_angle=np.rad2deg(gen.inc_angle), f0=gen.f0, num_ch=gen.num_ch, ant_L=gen.ant_l_tx,
-                 prf=gen.prf, v_ground=gen.v_ground, orbit_alt=cfg.sar.alt, sr0=gen.sr_near,
-                 rg_sampling=gen.rg_bw * gen.over_fs, rg_bw=gen.rg_bw, b_ati=gen.b_ati, b_xti=gen.b_xti)
+        values = dict(NRCS_avg=nrcs_avg, inc_angle=np.rad2deg(gen.inc_angle), f0=gen.f0, num_ch=gen.num_ch,
+                      ant_L=gen.ant_l_tx, prf=gen.prf, v_ground=gen.v_ground, orbit_alt=cfg.sar.alt,
+                      sr0=gen.sr_near, rg_sampling=gen.rg_bw * gen.over_fs, rg_bw=gen.rg_bw, b_ati=gen.b_ati,
+                      b_xti=gen.b_xti)
+        if str(output_file).endswith('.npz'):
+            np.savez(output_file, raw_data_r=total_raw.real, raw_data_i=total_raw.imag, **values)
+        else:
+            # sar_raw_nompi.py:580-600
+            f = RawFile(output_file, 'w', raw_dim=total_raw.shape)
+            f.set('raw_data*', total_raw)
+            for k, v in values.items():
+                f.set(k, v)
+            f.close()
     return total_raw, nrcs_avg

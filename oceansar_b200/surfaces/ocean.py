@@ -10,8 +10,8 @@
   writes the requested float32 fields into device buffers.  Reading an attribute such
   as ``surface.Dz`` returns a host numpy copy (the reference's type); ``field(name)``
   returns the device tensor without copying.
-* ``save`` / ``load`` (``ocean.py:244-373``) keep the state-file variables in a ``.npz``
-  (netCDF4 is not available in this environment).
+* ``save`` / ``load`` (``ocean.py:244-373``) write / read the state-file variables as a
+  netCDF classic ``OceanStateFile`` (or a ``.npz`` container for names ending in ``.npz``).
 """
 import ctypes
 
@@ -20,6 +20,8 @@ import torch
 from scipy import linalg
 
 from .. import _capi, _device, spec, spread
+from ..ocs_io import netcdf3
+from ..ocs_io.state import OceanStateFile
 
 G = 9.80665
 
@@ -30,6 +32,13 @@ CODES = {'Dz': 0, 'Dx': 1, 'Dy': 2, 'Diffx': 3, 'Diffy': 4, 'Diffxx': 5, 'Diffyy
 GROUPS = {'D': ['Dx', 'Dy', 'Dz'], 'Diff': ['Diffx', 'Diffy'], 'Diff2': ['Diffxx', 'Diffyy', 'Diffxy'],
           'V': ['Vx', 'Vy', 'Vz'], 'A': ['Ax', 'Ay', 'Az'], 'hMTF': ['hMTF']}
 FIELD_NAMES = [f for g in ('D', 'Diff', 'Diff2', 'V', 'A', 'hMTF') for f in GROUPS[g]]
+
+
+class _Vars(dict):
+    """Variables of a state file, with the ``files`` listing of an ``.npz`` archive."""
+    @property
+    def files(self):
+        return list(self.keys())
 
 
 class SurfaceDesc(ctypes.Structure):
@@ -284,7 +293,12 @@ class OceanSurface(object):
     def load(self, state_file, compute=[]):
         """Restore a surface written by ``save`` (``ocean.py:244-332``)."""
         try:
-            st = np.load(state_file, allow_pickle=False)
+            if netcdf3.is_netcdf3(state_file):
+                ds = netcdf3.Dataset(state_file, 'r')
+                st = {k: v[:] for k, v in ds.variables.items()}
+                st = _Vars(st)
+            else:
+                st = np.load(state_file, allow_pickle=False)
         except (OSError, ValueError):
             raise RuntimeError('Error loading OTGI File')
         g = lambda k: st[k][()]  # noqa: E731
@@ -328,7 +342,8 @@ class OceanSurface(object):
         self.initialized = True
 
     def save(self, state_file):
-        """Write the state-file variables (``ocean.py:334-373``) to ``state_file`` (.npz)."""
+        """Write the state-file variables (``ocean.py:334-373``) to ``state_file``: a netCDF
+        classic ``OceanStateFile``, or a numpy container for names ending in ``.npz``."""
         if not self.initialized:
             raise Exception('Surface not initialized')
         d = dict(Nx=np.uint32(self.Nx), Ny=np.uint32(self.Ny), Lx=np.float32(self.Lx),
@@ -346,8 +361,15 @@ class OceanSurface(object):
                  choppy_enable=np.float32(1 if self.choppy_enable else 0))
         if self.swell_enable:
             d['swell_ph0'] = np.float32(self.swell_ph0)
-        with open(state_file, 'wb') as f:
-            np.savez(f, **d)
+        if str(state_file).endswith('.npz'):
+            with open(state_file, 'wb') as f:
+                np.savez(f, **d)
+            return
+        # netCDF classic OceanStateFile (ocean.py:334-373)
+        f = OceanStateFile(state_file, 'w', ocean_dim=(self.Ny, self.Nx))
+        for k, v in d.items():
+            f.set(k, v)
+        f.close()
 
     # ------------------------------------------------------------------------------
     @property
