@@ -281,17 +281,20 @@ class RawGenerator(object):
         self._refreshes = []
 
     # ------------------------------------------------------------------------------------
-    def pulse(self, az_step, update_surface=True):
+    def pulse(self, az_step, update_surface=True, buffer=0, surface_stream=None):
         """One iteration of the azimuth loop (``sar_raw_nompi.py:349-535``).
 
         ``update_surface=False`` keeps whatever the surface field buffers hold (used to
-        feed externally computed fields, stage by stage)."""
+        feed externally computed fields, stage by stage).  ``buffer`` selects the field set
+        (1: the second set of ``run_overlapped``); ``surface_stream`` the stream of the
+        surface update (default: the pulse's)."""
         t_now = az_step * self.t_step
         az_now = (t_now - self.t_span / 2.) * self.v_ground
         if update_surface and ((not self.frozen) or az_step == 0):
             # a frozen ocean keeps the t = 0 surface (the reference leaves it unset)
-            self.surface.set_t(t_now, stream=self.stream)
-        d = self.desc
+            self.surface.set_t(t_now, stream=surface_stream if surface_stream is not None else self.stream,
+                               buffer=buffer)
+        d = self.desc if buffer == 0 else self._desc_b
         d.az_step = int(az_step)
         d.az_now = float(az_now)
         d.refresh = 0
@@ -361,6 +364,62 @@ class RawGenerator(object):
         for a in (range(self.az_steps) if steps is None else steps):
             self.pulse(a)
 
+    def can_overlap(self):
+        """Whether ``run_overlapped`` applies (not for choppy or frozen surfaces)."""
+        return not self.surface._aux and not self.frozen
+
+    def _second_desc(self):
+        """The pulse descriptor reading the second field set."""
+        if getattr(self, '_desc_b', None) is None:
+            fb = self.surface.second_buffer()
+            d = PulseDesc.from_buffer_copy(self.desc)
+            d.b_ati, d.b_xti = self._b_ati, self._b_xti
+            d.dx_d, d.dy_d, d.dz_d = fb['Dx'].data_ptr(), fb['Dy'].data_ptr(), fb['Dz'].data_ptr()
+            d.diffx_d, d.diffy_d = fb['Diffx'].data_ptr(), fb['Diffy'].data_ptr()
+            if 'Diffxx' in fb:
+                d.diffxx_d, d.diffyy_d, d.diffxy_d = (fb['Diffxx'].data_ptr(), fb['Diffyy'].data_ptr(),
+                                                      fb['Diffxy'].data_ptr())
+            if 'hMTF' in fb:
+                d.hmtf_d = fb['hMTF'].data_ptr()
+            self._desc_b = d
+        return self._desc_b
+
+    def run_overlapped(self, steps=None):
+        """The azimuth loop with the surface of pulse a + 1 synthesised on a second stream,
+        into the other of two field sets, while pulse a's kernels read theirs.  Same result
+        as ``run`` (only the kernels' overlap on the GPU differs).  Enqueued on the current
+        stream (forked and joined), so it can be recorded into a CUDA graph."""
+        if not self.can_overlap():
+            return self.run(steps)
+        self._second_desc()
+        steps = list(range(self.az_steps) if steps is None else steps)
+        main = torch.cuda.current_stream()
+        if getattr(self, '_surf_stream', None) is None:
+            self._surf_stream = torch.cuda.Stream()
+        side = self._surf_stream
+        side.wait_stream(main)
+        done_surf, done_pulse = {}, {}
+        saved = self.stream
+        self.stream = main
+        try:
+            for i, a in enumerate(steps):
+                buf = i % 2
+                if i >= 2:
+                    side.wait_event(done_pulse[i - 2])          # its fields were read by pulse i-2
+                t_now = a * self.t_step
+                self.surface.set_t(t_now, stream=side, buffer=buf)
+                ev = torch.cuda.Event()
+                ev.record(side)
+                done_surf[i] = ev
+                main.wait_event(ev)
+                self.pulse(a, update_surface=False, buffer=buf)
+                evp = torch.cuda.Event()
+                evp.record(main)
+                done_pulse[i] = evp
+        finally:
+            self.stream = saved
+        main.wait_stream(side)
+
     def reset(self):
         """Clear the raw cube and NRCS accumulators and restart the Bragg refresh clock."""
         self.raw_d.zero_()
@@ -370,14 +429,18 @@ class RawGenerator(object):
         self._refreshes = []
 
     # ------------------------------------------------------------------------------------
-    def capture(self):
-        """Record reset + every pulse of the scene into one CUDA graph.
+    def capture(self, overlap=True):
+        """Record reset + every pulse of the scene into one CUDA graph (with ``overlap``,
+        the surface of the next pulse on a second stream, as ``run_overlapped``).
 
         The per-pulse host work (time, azimuth, refresh decision, launch arguments) is
         done once, at capture; ``replay()`` then re-issues the whole scene with a single
         graph launch.  One ordinary pass runs first (warm-up and lazy set-up)."""
         self.reset()
         self.run()
+        if overlap and self.can_overlap():
+            self._second_desc()                 # second field set, allocated outside the capture
+            self._surf_stream = getattr(self, '_surf_stream', None) or torch.cuda.Stream()
         torch.cuda.synchronize()
         side = torch.cuda.Stream()
         side.wait_stream(torch.cuda.current_stream())
@@ -385,7 +448,10 @@ class RawGenerator(object):
         saved, self.stream = self.stream, None
         with torch.cuda.graph(g, stream=side):
             self.reset()
-            self.run()
+            if overlap and self.can_overlap():
+                self.run_overlapped()
+            else:
+                self.run()
         self.stream = saved
         torch.cuda.current_stream().wait_stream(side)
         self._graph = g

@@ -382,11 +382,12 @@ class OceanSurface(object):
     def t(self, value):
         self.set_t(value)
 
-    def set_t(self, value, stream=None, passes=3):
+    def set_t(self, value, stream=None, passes=3, buffer=0):
         """Propagate to time ``value`` and synthesise every requested field on the GPU.
 
         ``passes`` selects the row pass (1), the column pass (2) or both (3, the default);
-        the column pass consumes what the row pass of the same time left in the workspace."""
+        the column pass consumes what the row pass of the same time left in the workspace.
+        ``buffer`` 1 writes the second field set (``second_buffer``)."""
         if not self.initialized:
             raise Exception('Surface not initialized')
         self._t = np.float32(value)
@@ -394,7 +395,7 @@ class OceanSurface(object):
         if not self._raw:
             return
         _, add, rot = self.time_terms(value)
-        desc = self.update_desc(add, rot)
+        desc = self.update_desc(add, rot, buffer)
         sp = _device.stream_ptr(stream)
         if passes == 3:
             _capi.call("ocs_surface_update", ctypes.addressof(desc), ctypes.c_float(float(self._t)), sp)
@@ -425,13 +426,28 @@ class OceanSurface(object):
             rot = np.exp(-1j * self.swell_omega * t)
         return t, add, rot
 
-    def update_desc(self, add=None, rot=np.complex64(0)):
-        """``ocs_surface_desc`` of this surface (the caller keeps it alive while in use)."""
+    def second_buffer(self):
+        """Allocate a second set of field buffers (once) so that the fields of the next time
+        can be synthesised while the current ones are still being read; returns the
+        field-name -> tensor dict of that set.  Not for choppy surfaces."""
+        if self._aux:
+            raise NotImplementedError('choppy surfaces keep a single field buffer')
+        if getattr(self, '_fields_b', None) is None:
+            shape = (self.Ny, self.Nx)
+            self._fields_b = {n: _device.empty(shape, np.float32) for n in self._fields}
+            self._dsts_b = (ctypes.c_void_p * len(self._raw))(*[self._fields_b[key].data_ptr()
+                                                                  for _, _, key, _ in self._raw])
+        return self._fields_b
+
+    def update_desc(self, add=None, rot=np.complex64(0), buffer=0):
+        """``ocs_surface_desc`` of this surface (the caller keeps it alive while in use);
+        ``buffer`` 1 writes the second field set (``second_buffer``)."""
         n = len(self._raw)
         add_c = (ctypes.c_float * n)(*(add if add is not None else [0.0] * n))
+        dsts = self._dsts if buffer == 0 else self._dsts_b
         desc = SurfaceDesc(self.Nx, self.Ny, self._coefs_d.data_ptr(), self._omega_d.data_ptr(),
                            self._kx_d.data_ptr(), self._ky_d.data_ptr(), float(self.kmin_half), n,
-                           self._codes, self._dsts, add_c, self._swm,
+                           self._codes, dsts, add_c, self._swm,
                            self._swell_d.data_ptr() if self._swell_d is not None else None,
                            float(np.real(rot)), float(np.imag(rot)), self._ws.data_ptr())
         desc._keep = add_c
