@@ -297,6 +297,15 @@ typedef struct {
 
 int ocs_field_ka(const ocs_ka_desc *desc, void *stream);
 
+/* Range-Doppler focusing (sar_focus, oceansar/radarsim/sar_processor.py:30-274): the phase
+ * multiplications between its FFTs, on complex128 data [npol][naz][nrg] in place.
+ * ocs_rd_rcmc: range-cell-migration correction in the 2-D frequency domain, data *=
+ * exp(1j (4 pi rcmc[a] / c) fr[r]) (:170-176).  ocs_rd_azfilter: azimuth compression
+ * filter, data *= h[a] with h = exp(1j ph_ac) weighting (:213-217; h complex128 [naz]). */
+int ocs_rd_rcmc(double *data_d, int64_t npol, int32_t naz, int32_t nrg, const double *rcmc_d,
+                const double *fr_d, double c, void *stream);
+int ocs_rd_azfilter(double *data_d, int64_t npol, int32_t naz, int32_t nrg, const double *h_d, void *stream);
+
 /* ---- Scene batch ----------------------------------------------------------------------
  * Many independent scenes (any mix of grid sizes, geometries and channel counts) advanced
  * together, one pulse of every scene per step, by persistent kernels that find their work

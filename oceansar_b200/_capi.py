@@ -48,6 +48,8 @@ SIGNATURES = {
     "ocs_rcs_romeiser": [c_ptr, c_ptr],
     "ocs_field_kodis": [c_ptr, c_ptr],
     "ocs_field_ka": [c_ptr, c_ptr],
+    "ocs_rd_rcmc": [c_ptr, c_i64, ctypes.c_int32, ctypes.c_int32, c_ptr, c_ptr, c_dbl, c_ptr],
+    "ocs_rd_azfilter": [c_ptr, c_i64, ctypes.c_int32, ctypes.c_int32, c_ptr, c_ptr],
     "ocs_batch_create": [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(c_ptr)],
     "ocs_batch_destroy": [c_ptr],
     "ocs_batch_set": [c_ptr, ctypes.c_int32, c_ptr, c_ptr],

@@ -16,6 +16,7 @@ reference functions on the raw-data-generation path:
 * ``closure/*.py``               ``grid_coherence`` / ``randomscat_ts``
 * ``utils/geometry.py``, ``utils/misc.py``  geometry helpers and ``optimize_fftsize``
 * ``ocs_io/cfg.py``              ``ConfigFile`` parsing of the ``.cfg`` files in ``cfg/``
+* ``radarsim/sar_processor.py``  ``sar_focus`` on a seeded raw cube
 * ``radarsim/sar_raw_nompi.py``  ``sar_raw`` end to end (noise at -300 dB), plus the
   arguments and results of its first ``chan_profile_numba`` calls.
 
@@ -250,6 +251,55 @@ def gen_ka():
         out['rcs_%s_vv' % mode] = m.rcs('v', 'v', inc, inc, az, az + np.pi, Dz, Diffx, Diffy, Diffxx, Diffyy,
                                         Diffxy)
     save("ka.npz", **out)
+
+
+PROC_CFG = """\
+[sar]
+f0=5.405e9
+prf=1000.
+num_ch=2
+alt=514e3
+v_ground=7600.
+rg_bw=50e6
+over_fs=1.1
+ant_L_tx=2.742
+ant_L_rx=2.742
+inc_angle=35.
+pol=vv
+
+[processing]
+az_weighting=0.54
+doppler_bw=100.
+plot_format=png
+plot_tex=False
+plot_save=False
+plot_path=plots
+plot_raw=False
+plot_rcmc_dopp=False
+plot_rcmc_time=False
+plot_image_valid=False
+"""
+
+
+def gen_focus():
+    """sar_focus (radarsim/sar_processor.py:30-274) on a seeded raw cube (1 pol, 2 channels,
+    500 azimuth x 40 range samples, padded by the processor to 512 x 64)."""
+    from oceansar.radarsim import sar_processor
+    path = os.path.join(OUT, "cfg", "proc.cfg")
+    with open(path, "w") as f:
+        f.write(PROC_CFG)
+    rs = np.random.RandomState(21)
+    raw = (rs.randn(1, 2, 500, 40) + 1j * rs.randn(1, 2, 500, 40)).astype(np.complex64)
+    raw_file = "/tmp/golden_focus_raw.nc"
+    rf = ocs_io.RawFile(raw_file, 'w', raw.shape)
+    rf.set('raw_data*', raw)
+    for k, v in dict(sr0=627e3, inc_angle=35., b_ati=np.array([0., 10.]), b_xti=np.zeros(2)).items():
+        rf.set(k, v)
+    rf.close()
+    out_file = "/tmp/golden_focus_slc.nc"
+    sar_processor.sar_focus(path, raw_file, out_file)
+    v = ref_shims.NC_STORE[out_file].variables
+    save("sar_focus.npz", raw=raw, slc=v['slc_r'].data + 1j * v['slc_i'].data, sr0=np.array(627e3))
 
 
 def gen_kodis():
@@ -551,6 +601,8 @@ if __name__ == "__main__":
         gen_kodis()
     if "ka" in which:
         gen_ka()
+    if "focus" in which:
+        gen_focus()
     if "closure" in which:
         gen_closure()
     if "geometry" in which:
