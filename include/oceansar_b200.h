@@ -149,6 +149,13 @@ typedef struct {
 /* Choppy-wave slopes / curvatures from the auxiliary fields (ocean.py:451-456, 468-482). */
 int ocs_surface_choppy(const ocs_choppy_desc *desc, void *stream);
 
+/* Time-interpolated fields (OceanSurfaceBalancer.t, oceansar/surfaces/balancer.py:126-297):
+ * dst[f][i] = w_l * a[f][i] + w_h * b[f][i] in float32 for nfields float32 planes of n
+ * elements (16-byte aligned); a / b hold the fields synthesised at the ends of the ocean
+ * time step.  a_d, b_d, dst_d are host arrays of device pointers. */
+int ocs_surface_blend(int64_t n, int32_t nfields, const float *const *a_d, const float *const *b_d,
+                      float *const *dst_d, float w_l, float w_h, void *stream);
+
 /* ocs_surface_update for callers that cannot allocate device memory (no counterpart in the
  * reference).  desc->workspace_d is ignored: the workspace is a 32 MiB device array
  * compiled into the library, so ocs_surface_workspace_bytes(nx, ny, nfields) must be at

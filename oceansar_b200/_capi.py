@@ -43,6 +43,7 @@ SIGNATURES = {
     "ocs_surface_update_passes": [c_ptr, c_flt, c_int, c_ptr],
     "ocs_surface_choppy": [c_ptr, c_ptr],
     "ocs_surface_update_noalloc": [c_ptr, c_flt, c_ptr],
+    "ocs_surface_blend": [c_i64, ctypes.c_int32, c_ptr, c_ptr, c_ptr, c_flt, c_flt, c_ptr],
     "ocs_pulse": [c_ptr, c_int, c_ptr],
     "ocs_pulse_workspace_bytes": [ctypes.c_int32, ctypes.c_int32],
     "ocs_rcs_romeiser": [c_ptr, c_ptr],

@@ -844,3 +844,61 @@ extern "C" int ocs_surface_update_noalloc(const ocs_surface_desc *d, float t, vo
     local.workspace_d = ws;
     return ocs_surface_update(&local, t, stream);
 }
+
+// ---------------------------------------------------------------------------------------
+// Time-interpolated surface (oceansar/surfaces/balancer.py:126-297): every field is the
+// float32 blend w_l * F(t_l) + w_h * F(t_h) of the fields synthesised at the two ends of
+// the ocean time step around t.
+namespace ocs {
+struct BlendArgs {
+    long long n;
+    int nfields;
+    const float *a[2 * kMaxPacked];
+    const float *b[2 * kMaxPacked];
+    float *dst[2 * kMaxPacked];
+    float w_l, w_h;
+};
+
+__global__ void surface_blend_kernel(const __grid_constant__ BlendArgs g) {
+    const long long n4 = g.n / 4;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (int f = 0; f < g.nfields; ++f) {
+        const float4 *a = reinterpret_cast<const float4 *>(g.a[f]);
+        const float4 *b = reinterpret_cast<const float4 *>(g.b[f]);
+        float4 *d = reinterpret_cast<float4 *>(g.dst[f]);
+        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += stride) {
+            const float4 x = a[i], y = b[i];
+            d[i] = make_float4(fadd(fmul(g.w_l, x.x), fmul(g.w_h, y.x)), fadd(fmul(g.w_l, x.y), fmul(g.w_h, y.y)),
+                               fadd(fmul(g.w_l, x.z), fmul(g.w_h, y.z)), fadd(fmul(g.w_l, x.w), fmul(g.w_h, y.w)));
+        }
+        for (long long i = 4 * n4 + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < g.n; i += stride)
+            g.dst[f][i] = fadd(fmul(g.w_l, g.a[f][i]), fmul(g.w_h, g.b[f][i]));
+    }
+}
+}  // namespace ocs
+
+extern "C" int ocs_surface_blend(int64_t n, int32_t nfields, const float *const *a_d, const float *const *b_d,
+                                 float *const *dst_d, float w_l, float w_h, void *stream) {
+    if (n < 0 || nfields < 0 || nfields > 2 * kMaxPacked) return OCS_ERR_ARG;
+    if (n == 0 || nfields == 0) return OCS_OK;
+    if (!a_d || !b_d || !dst_d) return OCS_ERR_ARG;
+    BlendArgs g;
+    memset(&g, 0, sizeof(g));
+    g.n = n;
+    g.nfields = nfields;
+    for (int f = 0; f < nfields; ++f) {
+        if (!a_d[f] || !b_d[f] || !dst_d[f]) return OCS_ERR_ARG;
+        // the vector path needs 16-byte aligned planes
+        if (((uintptr_t)a_d[f] | (uintptr_t)b_d[f] | (uintptr_t)dst_d[f]) & 15) return OCS_ERR_ARG;
+        g.a[f] = a_d[f];
+        g.b[f] = b_d[f];
+        g.dst[f] = dst_d[f];
+    }
+    g.w_l = w_l;
+    g.w_h = w_h;
+    long long blocks = (n / 4 + 255) / 256;
+    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks < 1) blocks = 1;
+    surface_blend_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(g);
+    return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
+}

@@ -65,10 +65,14 @@ class RawGenerator(object):
     ``overrides`` may fix ``az_steps`` / ``rg_samp`` / ``rg_samp_orig`` (the reference
     derives them from the geometry, ``sar_raw_nompi.py:264-278``).  ``device=False`` does
     only the host set-up (no GPU touched; the object pickles), and ``to_device()`` then
-    uploads and allocates -- scene preparation in worker processes.
+    uploads and allocates -- scene preparation in worker processes.  ``surface_dt`` (e.g. the
+    .cfg's ocean dt) selects the time-interpolated surface of the reference's MPI generator
+    (``OceanSurfaceBalancer``, ``sar_raw.py:233-353``): surfaces synthesised every
+    ``surface_dt`` seconds, fields interpolated linearly in between.
     """
 
-    def __init__(self, cfg, precision='f64', overrides=None, seed=None, stream=None, device=True):
+    def __init__(self, cfg, precision='f64', overrides=None, seed=None, stream=None, device=True,
+                 surface_dt=None):
         if precision not in PRECISIONS:
             raise ValueError('precision must be f64 or mixed')
         self.precision = precision
@@ -124,6 +128,8 @@ class RawGenerator(object):
                oc.swell_wl, compute, oc.opt_res, oc.fft_max_prime, choppy_enable=oc.choppy_enable,
                depth=oc.depth, dirspectrum_func=None, dir_swell_spec=dir_swell, device=device)
         self.frozen = bool(getattr(oc, 'frozen_ocean', False))
+        self.surface_dt = surface_dt if (surface_dt and not self.frozen) else None
+        self.balancer = None
 
         # ---- geometry (:231-278) ----------------------------------------------------------
         self.sr0 = sr0 = geo.inc_to_sr(self.inc_angle, alt)
@@ -222,6 +228,10 @@ class RawGenerator(object):
         d.nx, d.ny, d.npol, d.nch = s.Nx, s.Ny, self.npol, self.num_ch
         d.pol = nrcs.POL_CODES[self.pol]
         f = s.field
+        if self.surface_dt:
+            from ..surfaces import OceanSurfaceBalancer
+            self.balancer = OceanSurfaceBalancer(s, self.surface_dt)
+            f = self.balancer.field
         d.dx_d, d.dy_d, d.dz_d = f('Dx').data_ptr(), f('Dy').data_ptr(), f('Dz').data_ptr()
         d.diffx_d, d.diffy_d = f('Diffx').data_ptr(), f('Diffy').data_ptr()
         if self.scat_spec_enable:
@@ -290,7 +300,9 @@ class RawGenerator(object):
         surface update (default: the pulse's)."""
         t_now = az_step * self.t_step
         az_now = (t_now - self.t_span / 2.) * self.v_ground
-        if update_surface and ((not self.frozen) or az_step == 0):
+        if update_surface and self.balancer is not None:
+            self.balancer.set_t(t_now, stream=self.stream)
+        elif update_surface and ((not self.frozen) or az_step == 0):
             # a frozen ocean keeps the t = 0 surface (the reference leaves it unset)
             self.surface.set_t(t_now, stream=surface_stream if surface_stream is not None else self.stream,
                                buffer=buffer)
@@ -365,8 +377,9 @@ class RawGenerator(object):
             self.pulse(a)
 
     def can_overlap(self):
-        """Whether ``run_overlapped`` applies (not for choppy or frozen surfaces)."""
-        return not self.surface._aux and not self.frozen
+        """Whether ``run_overlapped`` applies (not for choppy, frozen or time-interpolated
+        surfaces)."""
+        return not self.surface._aux and not self.frozen and self.balancer is None
 
     def _second_desc(self):
         """The pulse descriptor reading the second field set."""
@@ -427,6 +440,8 @@ class RawGenerator(object):
         self.nrcs_bragg_d.zero_()
         self.t_last_rcs_bragg = -1.
         self._refreshes = []
+        if self.balancer is not None:
+            self.balancer.restart()
 
     # ------------------------------------------------------------------------------------
     def capture(self, overlap=True):
@@ -467,6 +482,9 @@ class RawGenerator(object):
         nout = self.npol * self.num_ch
         group = 2 if self.precision == 'f64' else 4
         pulse = 1 + (nout + group - 1) // group          # row table + pulse kernel(s)
+        if self.balancer is not None:                    # syntheses at the ends + one blend per pulse
+            times = [a * self.t_step for a in range(self.az_steps)]
+            return self.balancer.syntheses(times) * surf + self.az_steps * (1 + pulse)
         return self.az_steps * (surf + pulse)
 
     def time_stages(self, steps):
@@ -545,17 +563,18 @@ class RawGenerator(object):
 
 
 def sar_raw(cfg_file, output_file, ocean_file, reuse_ocean_file, errors_file, reuse_errors_file,
-            plot_save=True, precision='f64'):
+            plot_save=True, precision='f64', surface_dt=None):
     """Drop-in for ``sar_raw_nompi.sar_raw``: simulate and write the raw file.
 
     The raw file (``RawFile``: ``raw_data_r``/``raw_data_i`` [pol, ch, az, rg], ``NRCS_avg``,
     geometry scalars, baselines) and the ocean state file (``OceanStateFile``) are netCDF
     classic files with the reference's dimensions, variables and units; a file name ending
     in ``.npz`` gets the same variables in a numpy container instead.  ``errors_file`` /
-    ``plot_save`` are accepted and unused, as in the reference.
+    ``plot_save`` are accepted and unused, as in the reference.  ``surface_dt`` selects the
+    time-interpolated surface (``RawGenerator``).
     """
-    cfg = ConfigFile(cfg_file)
-    gen = RawGenerator(cfg, precision=precision)
+    cfg = cfg_file if isinstance(cfg_file, ConfigFile) else ConfigFile(cfg_file)
+    gen = RawGenerator(cfg, precision=precision, surface_dt=surface_dt)
     if ocean_file and not reuse_ocean_file:
         gen.surface.save(ocean_file)
     gen.run()

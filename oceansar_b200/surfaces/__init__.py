@@ -1,2 +1,4 @@
-"""Ocean surfaces (``oceansar/surfaces``): ``OceanSurface`` with fields synthesised on the GPU."""
+"""Ocean surfaces (``oceansar/surfaces``): ``OceanSurface`` with fields synthesised on the GPU,
+and ``OceanSurfaceBalancer``, its time-interpolated form."""
+from .balancer import OceanSurfaceBalancer  # noqa: F401
 from .ocean import OceanSurface  # noqa: F401

@@ -32,7 +32,7 @@ def sinc_bp(sin_angle, L, f0, field=False):
 
 
 class SarRawSim:
-    def __init__(self, cfg, overrides=None, seed=None):
+    def __init__(self, cfg, overrides=None, seed=None, surface_dt=None):
         if isinstance(cfg, str):
             cfg = ConfigFile(cfg)
         self.cfg = cfg
@@ -147,6 +147,11 @@ class SarRawSim:
                                                 az_span=az_span, use_lut=srg.use_lut)
         self.surface_area = s.dx * s.dy * s.Nx * s.Ny
         self.next_step = 0
+        # time-interpolated surface of the MPI generator (sar_raw.py:233-353)
+        self.balancer = None
+        if surface_dt and not self.frozen:
+            from .balancer import OceanSurfaceBalancer
+            self.balancer = OceanSurfaceBalancer(s, surface_dt)
 
     # ------------------------------------------------------------------------------
     def pulse(self, az_step, record=None):
@@ -155,7 +160,10 @@ class SarRawSim:
         t_now = az_step * self.t_step
         az_now = (t_now - self.t_span / 2.) * self.v_ground
         az = (s.y - az_now).reshape((s.Ny, 1))
-        if (not self.frozen) or az_step == 0:
+        if self.balancer is not None:
+            s = self.balancer
+            s.set_t(t_now)
+        elif (not self.frozen) or az_step == 0:
             s.set_t(t_now)
         sin_az = az / self.sr0
         az_proj_angle = np.arcsin(az / self.gr0)
@@ -289,9 +297,9 @@ class SarRawSim:
         return np.stack(out), np.stack(nrcs_avg)
 
 
-def sar_raw(cfg_file, seed=0, overrides=None, add_noise=True):
+def sar_raw(cfg_file, seed=0, overrides=None, add_noise=True, surface_dt=None):
     """Whole run: returns (raw[pol, ch, az, rg], NRCS_avg[pol, az], sim)."""
-    sim = SarRawSim(cfg_file, overrides=overrides, seed=seed)
+    sim = SarRawSim(cfg_file, overrides=overrides, seed=seed, surface_dt=surface_dt)
     sim.run()
     raw, nrcs_avg = sim.finish(add_noise=add_noise)
     return raw, nrcs_avg, sim

@@ -4,12 +4,13 @@ Run from the repository root, in a container where the reference tree is mounted
 
     python tests/golden/make_golden.py
 
-It imports the unmodified reference (``ref_shims.install()`` documents the five
+It imports the unmodified reference (``ref_shims.install()`` documents the
 import-time shims it needs) and records, for small seeded inputs, the outputs of the
 reference functions on the raw-data-generation path:
 
 * ``radarsim/range_profile.py``  ``calc_sinc_vec`` / ``chan_profile_numba``
 * ``surfaces/ocean.py``          ``OceanSurface.init`` and the ``t`` setter
+* ``surfaces/balancer.py``       ``OceanSurfaceBalancer`` time interpolation (one process)
 * ``nrcs/romeiser97.py``         ``RCSRomeiser97.rcs`` (numba path and LUT mode)
 * ``nrcs/kodis.py``              ``RCSKodis.field``
 * ``nrcs/ka.py``                 ``RCSKA.field`` / ``rcs`` (facet approach, stationary phase)
@@ -151,6 +152,32 @@ def gen_surfaces():
                 if hasattr(s, f):
                     out['t%d_%s' % (it, f)] = getattr(s, f).copy()
         save("surface_%s.npz" % name, **out)
+
+
+# --------------------------------------------------------------------------------------
+BALANCER_DT = 0.05
+BALANCER_TIMES = (0.0, 0.013, 0.05, 0.071, 0.12, 0.02, 0.5, 0.5371)
+BALANCER_ROW_STEP = 4                    # every 4th surface row is stored
+
+
+def gen_balancer():
+    """``OceanSurfaceBalancer`` over the deep_elf surface: pulse times inside one step, on a
+    step boundary, into the next step (upper end reused), backwards and far ahead."""
+    from oceansar.surfaces import OceanSurfaceBalancer
+    kw, seed, _ = SURFACE_CASES["deep_elf"]
+    np.random.seed(seed)
+    s = OceanSurface()
+    s.init(**kw)
+    b = OceanSurfaceBalancer(s, BALANCER_DT)
+    out = dict(wave_coefs=s.wave_coefs, dt=np.array(BALANCER_DT), times=np.array(BALANCER_TIMES),
+               row_step=np.array(BALANCER_ROW_STEP))
+    for it, t in enumerate(BALANCER_TIMES):
+        b.t = t
+        out['t%d_tl' % it] = np.array(b.t_l_last)
+        for f in FIELDS:
+            if hasattr(b, f):
+                out['t%d_%s' % (it, f)] = getattr(b, f)[::BALANCER_ROW_STEP].copy()
+    save("balancer_deep_elf.npz", **out)
 
 
 # --------------------------------------------------------------------------------------
@@ -593,6 +620,8 @@ if __name__ == "__main__":
         gen_range_profile()
     if "surfaces" in which:
         gen_surfaces()
+    if "balancer" in which:
+        gen_balancer()
     if "rcs" in which:
         gen_rcs()
     if "rcs_lut" in which:

@@ -19,6 +19,10 @@ replaces one of them without touching the reference sources:
    arrays (``or`` between boolean arrays).  Its evident intent, G = cos^2(theta)/pi inside
    |theta| <= pi/2 and 0 outside, is registered in its place; the product implements the
    same function.
+6. ``mpi4py.MPI``: a one-process communicator (rank 0 of 1) for
+   ``surfaces/balancer.py``; ``bcast`` returns its argument and ``Scatterv`` copies the
+   root's float32 buffer into the receive buffer (with one process the whole surface is
+   the root's share).
 """
 import sys
 import types
@@ -108,6 +112,24 @@ def cos2s_restated(k, theta, U_10, fetch):
     return np.where((theta < -np.pi / 2.0) | (theta > np.pi / 2.0), 0.0, g)
 
 
+class _Comm:
+    def Get_size(self):
+        return 1
+
+    def Get_rank(self):
+        return 0
+
+    def bcast(self, obj, root=0):
+        return obj
+
+    def Scatterv(self, sendbuf, recvbuf, root=0):
+        src = np.asarray(sendbuf[0])
+        if src.dtype != np.float32:
+            raise TypeError("MPI.FLOAT scatter of a %s buffer" % src.dtype)
+        dst = recvbuf[0]
+        dst.reshape(-1)[:] = src.reshape(-1)[:dst.size]
+
+
 def install():
     """Install the shims and put the reference on ``sys.path``; returns the package."""
     if "matplotlib" not in sys.modules or not isinstance(sys.modules["matplotlib"], types.ModuleType):
@@ -136,6 +158,11 @@ def install():
             setattr(np, alias, typ)
     if not hasattr(np, "trapz"):
         np.trapz = np.trapezoid
+
+    mpi = types.ModuleType("mpi4py")
+    mpi.MPI = types.SimpleNamespace(COMM_WORLD=_Comm(), FLOAT="MPI_FLOAT")
+    sys.modules["mpi4py"] = mpi
+    sys.modules["mpi4py.MPI"] = mpi.MPI
 
     if REF_ROOT not in sys.path:
         sys.path.insert(0, REF_ROOT)

@@ -105,6 +105,27 @@ def test_surface_init_and_fields(name):
                 np.testing.assert_array_equal(f[fld], d[key], err_msg="%s t=%g" % (fld, t))
 
 
+def test_balancer_interpolation():
+    """Time-interpolated surface (balancer.py:126-297) against the reference's balancer on
+    one process: bit-identical float32 fields at every time, including a step boundary, a
+    step change that reuses the upper end, a backward jump and a jump far ahead."""
+    from oracle.balancer import OceanSurfaceBalancer
+    kw, seed = SURF["deep_elf"]
+    d = load("balancer_deep_elf.npz")
+    np.random.seed(seed)
+    s = OceanSurface().init(**kw)
+    s.wave_coefs = d["wave_coefs"]
+    b = OceanSurfaceBalancer(s, float(d["dt"]))
+    rs = int(d["row_step"])
+    for it, t in enumerate(d["times"]):
+        f = b.set_t(t)
+        assert b.t_l_last == d["t%d_tl" % it]
+        for key in d.files:
+            if key.startswith("t%d_" % it) and not key.endswith("_tl"):
+                fld = key.split("_", 1)[1]
+                np.testing.assert_array_equal(f[fld][::rs], d[key], err_msg="%s t=%g" % (fld, t))
+
+
 def test_romeiser_rcs():
     d = load("rcs_romeiser.npz")
     k0 = float(d["k0"])
@@ -257,3 +278,15 @@ def test_sar_raw_end_to_end(name):
     assert err < 1e-9, err
     np.testing.assert_allclose(nrcs_avg, d["NRCS_avg"], rtol=1e-9)
     assert float(d["sr0"]) == pytest.approx(sim.sr_near, rel=1e-15)
+
+
+def test_sar_raw_interpolated_surface_one_step():
+    """With the interpolation step equal to the pulse interval, the time-interpolated run
+    reproduces the per-pulse surface of the reference's sar_raw (the blend weights are 0/1
+    up to float32 rounding of the pulse times)."""
+    d = load("sar_raw_c1small.npz")
+    cfg = os.path.join(G, "cfg", "c1small.cfg")
+    raw, _, sim = sar_raw(cfg, seed=0, surface_dt=0.001)
+    assert sim.balancer is not None and sim.t_step == 0.001
+    err = np.linalg.norm(raw - d["raw"]) / np.linalg.norm(d["raw"])
+    assert err < 1e-5, err
