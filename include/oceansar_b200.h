@@ -237,6 +237,9 @@ typedef struct {
     int32_t spec_mode;
     const float *x_d;
     double ka_dx, ka_dy, ka_K_re, ka_K_im;
+    /* Optional complex64 copies of s_m_d / s_p_d: the mixed form gathers these (half the
+     * bytes) when both are set; NULL: it reads the complex128 series. */
+    const float *s_m32_d, *s_p32_d;
 } ocs_pulse_desc;
 
 /* Workspace of ocs_pulse (per-pulse table of the row quantities); < 0 on invalid sizes. */

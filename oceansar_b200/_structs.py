@@ -36,7 +36,8 @@ class PulseDesc(ctypes.Structure):
                 ("lut_d", P), ("lut_naz", I32), ("lut_ndy", I32), ("lut_ndx", I32),
                 ("lut_az0", F64), ("lut_daz", F64), ("lut_dy0", F64), ("lut_ddy", F64),
                 ("lut_dx0", F64), ("lut_ddx", F64),
-                ("spec_mode", I32), ("x_d", P), ("ka_dx", F64), ("ka_dy", F64), ("ka_K_re", F64), ("ka_K_im", F64)]
+                ("spec_mode", I32), ("x_d", P), ("ka_dx", F64), ("ka_dy", F64), ("ka_K_re", F64), ("ka_K_im", F64),
+                ("s_m32_d", P), ("s_p32_d", P)]
 
 
 class RcsDesc(ctypes.Structure):

@@ -49,3 +49,10 @@ class randomscat_ts(object):
             self._dev = (_device.to_device(self.s, np.complex128),
                          _device.to_device(self.ind0.astype(np.int32), np.int32))
         return self._dev
+
+    def device32(self):
+        """The series as a complex64 device tensor (the mixed form's gathers), uploaded once."""
+        if getattr(self, '_dev32', None) is None:
+            from .. import _device
+            self._dev32 = _device.to_device(self.s, np.complex64)
+        return self._dev32

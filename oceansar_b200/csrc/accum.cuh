@@ -122,10 +122,12 @@ struct BinWindow {
     // Add one facet whose first tap lands on bin `first` with LUT index `lut`.
     __device__ void add(int first, int lut, const cplx<T> (&coef)[NOUT], const T *wtab,
                         const float *sinc, int taps, int ovs, CtaBins<T, NOUT> &cb) {
-        bool finite = true;
+        // one test for all coefficients: a finite sum implies finite terms; a sum that
+        // overflows with finite terms takes the exact per-tap path as well
+        T sum = (T)0;
 #pragma unroll
-        for (int o = 0; o < NOUT; ++o) finite = finite && isfinite(coef[o].re) && isfinite(coef[o].im);
-        if (!finite) {
+        for (int o = 0; o < NOUT; ++o) sum += coef[o].re + coef[o].im;
+        if (!isfinite(sum)) {
             // Non-finite coefficients touch exactly their own taps, as in the reference.
             for (int j = 0; j < taps; ++j) {
                 T w = (T)sinc[lut + j * ovs];

@@ -174,7 +174,7 @@ OCS_D cplx<T> kodis_facet(const KodisParams &kp, double sr, double sin_inc, doub
     } else {
         // mixed form: the stationary-point offsets in float32 (only the facet-window test
         // and the small range offset depend on them)
-        const float inv_j = __frcp_rn(J_abs);
+        const float inv_j = __fdividef(1.0f, J_abs);
         const float ty = diffy - (float)(tan_inc * sin_az);
         const float tx = diffx - (float)(tan_inc * cos_az);
         delta_x = (double)(inv_j * (diffxy * ty - diffyy * tx));

@@ -50,6 +50,7 @@ struct PulseArgs {
     RomeiserParams rom;
     void *scat;                             // [npol][2][ny][nx] sqrt(RCS) (T)
     const double *s_m, *s_p;                // complex128 random-scatterer series
+    const float *s_m32, *s_p32;             // complex64 copies (mixed form), or null
     int n_m, n_p;
     int tmod_m, tmod_p;                     // int(t_now * prf) mod n_m, n_p
     const int *ind0_m, *ind0_p;             // [ny][nx]
@@ -173,8 +174,11 @@ template <typename T> struct FacetIn {
             cp_async(st.ind(slot, 0), a.ind0_m + idx, 4);
             cp_async(st.ind(slot, 1), a.ind0_p + idx, 4);
         }
-        if (load_scat)
-            for (int k = 0; k < 2 * a.npol; ++k) cp_async(st.scat(slot, k), scat_buf + k * npix + idx, sizeof(T));
+        if (load_scat) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (k < 2 * a.npol) cp_async(st.scat(slot, k), scat_buf + k * npix + idx, sizeof(T));
+        }
     }
     // start the gathers of the scatterer-series values of the facet staged in `slot`
     template <typename A>
@@ -183,8 +187,13 @@ template <typename T> struct FacetIn {
         i0 = i0 >= a.n_m ? i0 - a.n_m : i0;
         int i1 = *st.ind(slot, 1) + a.tmod_p;
         i1 = i1 >= a.n_p ? i1 - a.n_p : i1;
-        cp_async(st.gather(g, 0), a.s_m + 2 * (long long)i0, 16);
-        cp_async(st.gather(g, 1), a.s_p + 2 * (long long)i1, 16);
+        if (sizeof(T) == 4 && a.s_m32) {
+            cp_async(st.gather(g, 0), a.s_m32 + 2 * (long long)i0, 8);
+            cp_async(st.gather(g, 1), a.s_p32 + 2 * (long long)i1, 8);
+        } else {
+            cp_async(st.gather(g, 0), a.s_m + 2 * (long long)i0, 16);
+            cp_async(st.gather(g, 1), a.s_p + 2 * (long long)i1, 16);
+        }
     }
     template <typename A>
     OCS_D void read(const A &a, const Stage<T> &st, int slot, bool load_scat) {
@@ -342,6 +351,16 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
         // the scatterer-series gathers of row i + 1 are in flight while row i is processed
         const Stage<T> &st = sm.stage;
         const long long idx0 = (long long)y0 * a.nx + x;
+        // outputs of this pass, 5 bits each: channel (bits 0-2), polarisation (bit 3) and
+        // whether the channel has an XTI phase (bit 4)
+        unsigned outs = 0;
+#pragma unroll
+        for (int k = 0; k < NOUT; ++k) {
+            const int o = a.out0 + k;
+            const int p = o / a.nch, c = o - p * a.nch;
+            const bool xti = k < a.nout && a.b_xti[c] != 0.0;
+            outs |= (unsigned)(c | (p << 3) | (xti ? 16 : 0)) << (5 * k);
+        }
         for (int r = 0; r < kStageRows - 1; ++r) {
             if (r < nrows) FacetIn<T>::issue(a, st, r, idx0 + (long long)r * a.nx, npix, scat, load_scat);
             cp_async_commit();
@@ -350,18 +369,23 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
         if (a.do_bragg) FacetIn<T>::issue_gather(a, st, 0, 0);
         cp_async_commit();
         FacetIn<T> cur;
+        // ring slots of rows i, i + 1 and i + kStageRows - 1
+        static_assert(kStageRows == 3, "the ring arithmetic assumes three slots");
+        int slot_i = 0;
         for (int i = 0; i < nrows; ++i) {
             const long long idx = idx0 + (long long)i * a.nx;
+            const int slot_n = slot_i == 2 ? 0 : slot_i + 1, slot_r = slot_i == 0 ? 2 : slot_i - 1;
             {
                 const int r = i + kStageRows - 1;
-                if (r < nrows) FacetIn<T>::issue(a, st, r % kStageRows, idx0 + (long long)r * a.nx, npix, scat,
+                if (r < nrows) FacetIn<T>::issue(a, st, slot_r, idx + (long long)(kStageRows - 1) * a.nx, npix, scat,
                                                  load_scat);
                 cp_async_commit();
             }
             cp_async_wait<1>();                 // rows <= i + 1 and the gathers of row i have landed
-            if (a.do_bragg && i + 1 < nrows) FacetIn<T>::issue_gather(a, st, (i + 1) % kStageRows, (i + 1) & 1);
+            if (a.do_bragg && i + 1 < nrows) FacetIn<T>::issue_gather(a, st, slot_n, (i + 1) & 1);
             cp_async_commit();
-            cur.read(a, st, i % kStageRows, load_scat);
+            cur.read(a, st, slot_i, load_scat);
+            slot_i = slot_n;
             const double az = sm.r_az[i], sin_az = sm.r_az[RCAP + i];
             // slant range: sr - cos_inc*Dz + az/2*sin_az + Dx*sin_inc + Dy*sin_az, float64,
             // left to right, no fused multiply-adds (bit-identical with numpy)
@@ -449,10 +473,18 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
                     e0 = {(T)c0, (T)s0};
                     e1 = {(T)c1, (T)s1};
                 }
-                const double2 smd = *st.gather(i & 1, 0);
-                const double2 spd = *st.gather(i & 1, 1);
-                const cplx<T> sm = {(T)smd.x, (T)smd.y};
-                const cplx<T> sp = {(T)spd.x, (T)spd.y};
+                cplx<T> sm, sp;
+                if (sizeof(T) == 4 && a.s_m32) {
+                    const float2 smf = *reinterpret_cast<const float2 *>(st.gather(i & 1, 0));
+                    const float2 spf = *reinterpret_cast<const float2 *>(st.gather(i & 1, 1));
+                    sm = {(T)smf.x, (T)smf.y};
+                    sp = {(T)spf.x, (T)spf.y};
+                } else {
+                    const double2 smd = *st.gather(i & 1, 0);
+                    const double2 spd = *st.gather(i & 1, 1);
+                    sm = {(T)smd.x, (T)smd.y};
+                    sp = {(T)spd.x, (T)spd.y};
+                }
 #pragma unroll
                 for (int p = 0; p < 2; ++p) {
                     if (p < a.npol) {
@@ -469,10 +501,10 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
 #pragma unroll
             for (int k = 0; k < NOUT; ++k) {
                 if (k < a.nout) {
-                    const int o = a.out0 + k;
-                    const int p = o / a.nch, c = o - p * a.nch;
-                    cplx<T> v = cmul(p == 0 ? scene[0] : scene[1], sm.r_fac[i * a.nch + c]);
-                    if (a.b_xti[c] != 0.0) {
+                    const unsigned ok = outs >> (5 * k);
+                    const int c = ok & 7;
+                    cplx<T> v = cmul((ok & 8) ? scene[1] : scene[0], sm.r_fac[i * a.nch + c]);
+                    if (ok & 16) {
                         const double ph = (-a.k0 * a.b_xti[c]) * (dinc0 + wave_dinc);
                         v = cmul(v, cexp_phase<T>(ph));
                     }
@@ -677,6 +709,7 @@ static int fill_pulse_args(const ocs_pulse_desc *d, PulseArgs &a) {
     r.seps_re = d->sqrt_eps_re; r.seps_im = d->sqrt_eps_im;
     r.eps2_re = 73.0 * 73.0 - 18.0 * 18.0; r.eps2_im = 2.0 * 73.0 * 18.0;
     a.scat = d->scat_d; a.s_m = d->s_m_d; a.s_p = d->s_p_d;
+    if (d->s_m32_d && d->s_p32_d) { a.s_m32 = d->s_m32_d; a.s_p32 = d->s_p32_d; }
     if (d->do_bragg) {
         if (d->n_m > (1LL << 30) || d->n_p > (1LL << 30) || d->tind < 0) return OCS_ERR_SIZE;
         a.n_m = (int)d->n_m; a.n_p = (int)d->n_p;

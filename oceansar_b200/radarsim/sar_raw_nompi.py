@@ -274,6 +274,8 @@ class RawGenerator(object):
             sp, ip = self.rndscat_p.device()
             d.s_m_d, d.s_p_d, d.n_m, d.n_p = sm.data_ptr(), sp.data_ptr(), int(self.rndscat_m.N), \
                 int(self.rndscat_p.N)
+            if self.precision == 'mixed':
+                d.s_m32_d, d.s_p32_d = self.rndscat_m.device32().data_ptr(), self.rndscat_p.device32().data_ptr()
             d.ind0_m_d, d.ind0_p_d = im.data_ptr(), ip.data_ptr()
             if self.rcs_bragg.use_lut:
                 self._lut_d = self.rcs_bragg.lut_device(self.precision)
