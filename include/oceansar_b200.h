@@ -240,6 +240,24 @@ typedef struct {
     /* Optional complex64 copies of s_m_d / s_p_d: the mixed form gathers these (half the
      * bytes) when both are set; NULL: it reads the complex128 series. */
     const float *s_m32_d, *s_p32_d;
+    /* Scatterometer mode (sca = 1; the DopSCA generator, dopscasim/dopsca_raw.py:343-520):
+     * nx = N_repeat_x * field_nx columns (range blocks, each with its own geometry
+     * columns) read the surface fields at column x mod field_nx and row (y + roll) mod ny
+     * (the azimuth shift by whole rows); the per-facet scatterer indices ind0_m/p_d are
+     * [ny][nx] and read at the rolled row too.  The scene is scaled by (sr0/(sr0 + r))^2,
+     * the range bins see r + sr_bin_offset (the sub-pulse delay), the Bragg phase uses
+     * 2 k0 c_b cap_t, and the Bragg RCS is evaluated on every call (scat_d unused).
+     * The NRCS sums are kept per range block: nrcs_spec_d[nrcs_row][nblk] and
+     * nrcs_bragg_d[npol][nrcs_rows][nblk] (float64, +=), nblk = nx / field_nx.
+     * az_f32 = 1: the azimuth residual az_now is a float32 value and the row azimuth is the
+     * float32 difference y - az_now (the reference's numpy promotion when the grid step is
+     * float32 and the residual is not a float64 scalar).
+     * Requires nch = 1, Kodis (spec_mode 0), no LUT, no hMTF.  The scene batch rejects it. */
+    int32_t sca;
+    int32_t field_nx, roll;
+    double sr_bin_offset, cap_t;
+    int32_t nrcs_row, nrcs_rows;
+    int32_t az_f32;
 } ocs_pulse_desc;
 
 /* Workspace of ocs_pulse (per-pulse table of the row quantities); < 0 on invalid sizes. */

@@ -14,6 +14,14 @@
 // register windows warm.  Per-row quantities (azimuth, antenna pattern, ATI phase) are
 // computed once per CTA into shared memory.
 //
+// Scatterometer mode (MODE = kModeSca, the DopSCA generator, oceansar/dopscasim/dopsca_raw.py:
+// 343-520): the columns are N_repeat_x range blocks side by side, each reading the same
+// surface (field column = column mod field_nx) with its rows rolled by the integer azimuth
+// shift (field row = (row + roll) mod ny); the scene is scaled by (sr0 / (sr0 + r))^2, the
+// Bragg RCS is evaluated on every launch, the Bragg phase advances with the sub-pulse time
+// cap_t, the range bins see the sub-pulse delay sr_bin_off, and the NRCS sums are kept per
+// range block.
+//
 // Precision forms (template T):
 //   double -- the drop-in: every operation in float64 in the reference's order; slant
 //             range and the bin / LUT indices bit-identical to numpy.
@@ -32,6 +40,8 @@ constexpr int kPulseRows = 64;      // rows per tile (single-scene launches)
 constexpr int kPulseRowsMax = 128;  // largest rows per tile (shared row tables)
 constexpr int kMaxCh = 8;
 constexpr int kPulseNbw = 160;      // CTA shared bin window
+
+enum { kModeStd = 0, kModeKa = 1, kModeSca = 2 };
 
 struct PulseArgs {
     int nx, ny, npol, nch;
@@ -69,11 +79,16 @@ struct PulseArgs {
     const void *lut;                        // Romeiser LUT [npol][2][naz][ndy][ndx] (T), or null
     int lut_naz, lut_ndy, lut_ndx;
     double lut_az0, lut_daz, lut_dy0, lut_ddy, lut_dx0, lut_ddx;
+    int sca;                                // scatterometer mode (see the file comment)
+    int fnx, roll;                          // field columns, azimuth roll of the field rows
+    double sr_bin_off, cap_t;               // sub-pulse range delay, Bragg phase time
+    int nblk, nrcs_row, nrcs_rows;          // range blocks; NRCS row of this call, rows in all
+    int az_f32;                             // azimuth y - az_now rounded to float32 (see pulse_row)
 };
 
 // Kirchhoff specular term of one facet and polarisation code pc (0 = hh, 1 = vv),
 // sar_raw_nompi.py:402-426: exp(-1j (2 k0 r)) (4 pi)^1.5 RCSKA.field(1, 1, ...).  Only the
-// Kirchhoff instantiations of the pulse kernel (KA = true) contain it.
+// Kirchhoff instantiations of the pulse kernel (MODE = kModeKa) contain it.
 OCS_D c128 ka_specular(const KaParams &kp, int pc, double srs, double x, double y, double st,
                                          double ct, double tt, double sp, double cp, float dz, float dx, float dy,
                                          float dxx, float dyy, float dxy) {
@@ -155,20 +170,21 @@ template <typename T> struct FacetIn {
     float dx, dy, dz, diffx, diffy, diffxx, diffyy, diffxy;
     T scat[2][2];
     // start the copies of facet idx's inputs into stage slot `slot`
+    // (fidx: index into the surface fields; idx: into the per-facet scatterer arrays)
     template <typename A>
     static OCS_D void issue(const A &a, const Stage<T> &st, int slot, long long idx, long long npix,
-                            const T *scat_buf, bool load_scat) {
-        cp_async(st.f(slot, 0), a.dx_f + idx, 4);
-        cp_async(st.f(slot, 1), a.dy_f + idx, 4);
-        cp_async(st.f(slot, 2), a.dz_f + idx, 4);
+                            const T *scat_buf, bool load_scat, long long fidx) {
+        cp_async(st.f(slot, 0), a.dx_f + fidx, 4);
+        cp_async(st.f(slot, 1), a.dy_f + fidx, 4);
+        cp_async(st.f(slot, 2), a.dz_f + fidx, 4);
         if (a.diffx) {
-            cp_async(st.f(slot, 3), a.diffx + idx, 4);
-            cp_async(st.f(slot, 4), a.diffy + idx, 4);
+            cp_async(st.f(slot, 3), a.diffx + fidx, 4);
+            cp_async(st.f(slot, 4), a.diffy + fidx, 4);
         }
         if (a.do_kodis) {
-            cp_async(st.f(slot, 5), a.diffxx + idx, 4);
-            cp_async(st.f(slot, 6), a.diffyy + idx, 4);
-            cp_async(st.f(slot, 7), a.diffxy + idx, 4);
+            cp_async(st.f(slot, 5), a.diffxx + fidx, 4);
+            cp_async(st.f(slot, 6), a.diffyy + fidx, 4);
+            cp_async(st.f(slot, 7), a.diffxy + fidx, 4);
         }
         if (a.do_bragg) {
             cp_async(st.ind(slot, 0), a.ind0_m + idx, 4);
@@ -242,7 +258,9 @@ OCS_D void block_atomic_sum(double v, double *dst, double *sred) {
 // cos / sin (q = 0..4), then rowtab[5*ny + 2*(y*nch + c)] the complex antenna-pattern x
 // ATI-phase factor of channel c.  float64, computed once per pulse for all tiles.
 OCS_D void pulse_row(const PulseArgs &a, double az_now, int y) {
-    const double az = dsub((double)a.y[y], az_now);
+    // the scatterometer's azimuth residual is float32 when the reference computes it from
+    // a float32 grid step (numpy promotion), and then y - residual is a float32 difference
+    const double az = a.az_f32 ? (double)__fsub_rn(a.y[y], (float)az_now) : dsub((double)a.y[y], az_now);
     const double sin_az = ddiv(az, a.sr0);
     const double azp = asin(az / a.gr0);
     a.rowtab[y] = az;
@@ -298,7 +316,7 @@ OCS_D PulseSmem<T> pulse_smem(unsigned char *smem, int nch) {
 // One tile of kPulseCols columns x tile_rows rows: NRCS, scene and accumulation of every
 // facet into this pulse's raw rows; the tile's NRCS sums are added to spec_sum and
 // bragg_sum.
-template <typename T, int NOUT, int S, int RCAP, bool KA = false>
+template <typename T, int NOUT, int S, int RCAP, int MODE = kModeStd>
 OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSmem<T> &sm, double &spec_sum,
                       double (&bragg_sum)[2]) {
     const int tiles_x = (a.nx + kPulseCols - 1) / kPulseCols;
@@ -328,7 +346,7 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
         // window base: bin of this CTA's first column at its first row, undisplaced
         const int xc = min((tile % tiles_x) * kPulseCols, a.nx - 1);
         const double az = (double)a.y[y0] - a.az_now;
-        const double srg = a.sr_col[xc] + az * 0.5 * (az / a.sr0);
+        const double srg = a.sr_col[xc] + az * 0.5 * (az / a.sr0) + a.sr_bin_off;
         cb.cta_base = (int)floor((srg - a.min_sr) / a.binsize) - 24;
     }
     cb.zero();
@@ -341,7 +359,11 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
         const double inc_c = a.inc[x];
         const double dinc0 = inc_c - a.inc_angle;
         const double tan_i = a.do_kodis ? a.tan_inc[x] : 0.0;
-        const double cap = a.do_bragg ? ((2.0 * a.k0) * a.t_step) * a.c_b[x] * (double)(a.az_step + 1) : 0.0;
+        double cap = 0.0;
+        if (a.do_bragg) {
+            if constexpr (MODE == kModeSca) cap = dmul(dmul(2.0 * a.k0, a.c_b[x]), a.cap_t);
+            else cap = ((2.0 * a.k0) * a.t_step) * a.c_b[x] * (double)(a.az_step + 1);
+        }
         const float cap_r = (float)reduce_2pi(cap);
         const double two_k0 = 2.0 * a.k0;
         const long long npix = (long long)a.nx * a.ny;
@@ -361,8 +383,27 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
             const bool xti = k < a.nout && a.b_xti[c] != 0.0;
             outs |= (unsigned)(c | (p << 3) | (xti ? 16 : 0)) << (5 * k);
         }
+        // indices of tile row r: per-facet arrays (ridx) and surface fields (fidx); the
+        // scatterometer mode reads the fields of the rolled row and the column mod fnx
+        int fx = x;
+        if constexpr (MODE == kModeSca) fx = x % a.fnx;
+        auto row_index = [&](int r, long long &ridx, long long &fidx) {
+            if constexpr (MODE == kModeSca) {
+                int fr = y0 + r + a.roll;
+                fr = fr >= a.ny ? fr - a.ny : fr;
+                ridx = (long long)fr * a.nx + x;
+                fidx = (long long)fr * a.fnx + fx;
+            } else {
+                ridx = idx0 + (long long)r * a.nx;
+                fidx = ridx;
+            }
+        };
         for (int r = 0; r < kStageRows - 1; ++r) {
-            if (r < nrows) FacetIn<T>::issue(a, st, r, idx0 + (long long)r * a.nx, npix, scat, load_scat);
+            if (r < nrows) {
+                long long ridx, fidx;
+                row_index(r, ridx, fidx);
+                FacetIn<T>::issue(a, st, r, ridx, npix, scat, load_scat, fidx);
+            }
             cp_async_commit();
         }
         cp_async_wait<kStageRows - 2>();
@@ -377,8 +418,11 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
             const int slot_n = slot_i == 2 ? 0 : slot_i + 1, slot_r = slot_i == 0 ? 2 : slot_i - 1;
             {
                 const int r = i + kStageRows - 1;
-                if (r < nrows) FacetIn<T>::issue(a, st, slot_r, idx + (long long)(kStageRows - 1) * a.nx, npix, scat,
-                                                 load_scat);
+                if (r < nrows) {
+                    long long ridx, fidx;
+                    row_index(r, ridx, fidx);
+                    FacetIn<T>::issue(a, st, slot_r, ridx, npix, scat, load_scat, fidx);
+                }
                 cp_async_commit();
             }
             cp_async_wait<1>();                 // rows <= i + 1 and the gathers of row i have landed
@@ -394,11 +438,21 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
             srs = dadd(srs, dmul((double)cur.dx, sin_i));
             srs = dadd(srs, dmul((double)cur.dy, sin_az));
             int bin_d, lut;
-            if (sizeof(T) == 8) bin_and_lut(srs, a.min_sr, a.binsize, kSincOvs, bin_d, lut);
-            else bin_and_lut_fast(srs, a.min_sr, a.inv_binsize, kSincOvs, bin_d, lut);
+            {
+                // the scatterometer's sub-pulses arrive later by sr_bin_off (range bins only)
+                const double srb = (MODE == kModeSca) ? dadd(srs, a.sr_bin_off) : srs;
+                if (sizeof(T) == 8) bin_and_lut(srb, a.min_sr, a.binsize, kSincOvs, bin_d, lut);
+                else bin_and_lut_fast(srb, a.min_sr, a.inv_binsize, kSincOvs, bin_d, lut);
+            }
+            // two-way spreading of the scatterometer scene, (sr0 / (sr0 + r))^2
+            T rscale = (T)1;
+            if constexpr (MODE == kModeSca) {
+                const double q = ddiv(a.sr0, dadd(a.sr0, srs));
+                rscale = (T)dmul(q, q);
+            }
 
             cplx<T> scene[2] = {{(T)0, (T)0}, {(T)0, (T)0}};      // per polarisation
-            if constexpr (KA) {
+            if constexpr (MODE == kModeKa) {
                 c128 last = {0.0, 0.0};
                 for (int p = 0; p < a.npol; ++p) {
                     const int pc = a.rom.pol == POL_DP ? p : (a.rom.pol == POL_HH ? 0 : 1);
@@ -413,9 +467,14 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
                                                  cur.diffx, cur.diffy, cur.diffxx, cur.diffyy, cur.diffxy);
                 const T s4 = (T)3.5449077018110318;                 // sqrt(4 pi)
                 const cplx<T> es = {e.re * s4, e.im * s4};
-                scene[0] = es;
-                scene[1] = es;
                 spec_sum += (double)es.re * es.re + (double)es.im * es.im;
+                if constexpr (MODE == kModeSca) {
+                    scene[0] = {es.re * rscale, es.im * rscale};
+                    scene[1] = scene[0];
+                } else {
+                    scene[0] = es;
+                    scene[1] = es;
+                }
             }
             if (a.do_bragg) {
                 T sc[2][2];                                            // [pol][line]
@@ -449,7 +508,7 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
                             bragg_sum[p] += (double)r0 + (double)r1;
                             sc[p][0] = tsqrt(r0);
                             sc[p][1] = tsqrt(r1);
-                            if (a.out0 == 0) {          // one output group stores the RCS
+                            if (MODE != kModeSca && a.out0 == 0) {   // one output group stores the RCS
                                 scat[(2 * p) * npix + idx] = sc[p][0];
                                 scat[(2 * p + 1) * npix + idx] = sc[p][1];
                             }
@@ -490,7 +549,9 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
                     if (p < a.npol) {
                         const cplx<T> l0 = cmul(cplx<T>{sc[p][0] * e0.re, sc[p][0] * e0.im}, sm);
                         const cplx<T> l1 = cmul(cplx<T>{sc[p][1] * e1.re, sc[p][1] * e1.im}, sp);
-                        scene[p] = cadd(scene[p], cadd(l0, l1));
+                        cplx<T> lb = cadd(l0, l1);
+                        if constexpr (MODE == kModeSca) lb = {lb.re * rscale, lb.im * rscale};
+                        scene[p] = cadd(scene[p], lb);
                     }
                 }
             }
@@ -518,6 +579,20 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
         }
         cp_async_wait<0>();
     }
+    if constexpr (MODE == kModeSca) {
+        // the scatterometer's NRCS sums are kept per range block: each column adds its
+        // tile's sums to its block
+        if (x < a.nx) {
+            const long long blk = x / a.fnx;
+            if (a.do_kodis && spec_sum != 0.0) atomicAdd(&a.nrcs_spec[(long long)a.nrcs_row * a.nblk + blk], spec_sum);
+            if (a.do_bragg)
+                for (int p = 0; p < a.npol; ++p)
+                    if (bragg_sum[p] != 0.0)
+                        atomicAdd(&a.nrcs_bragg[((long long)p * a.nrcs_rows + a.nrcs_row) * a.nblk + blk], bragg_sum[p]);
+        }
+        spec_sum = 0.0;
+        bragg_sum[0] = bragg_sum[1] = 0.0;
+    }
     win.flush(cb);
     __syncthreads();
     cb.flush_to_global();
@@ -534,7 +609,7 @@ OCS_D void pulse_nrcs(const PulseArgs &a, const PulseSmem<T> &sm, double spec_su
     }
 }
 
-template <typename T, int NOUT, int S, bool KA>
+template <typename T, int NOUT, int S, int MODE>
 __global__ void __launch_bounds__(kPulseCols, (sizeof(T) == 4 && NOUT < 4) ? 4 : 2)
 pulse_kernel(const __grid_constant__ PulseArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -544,7 +619,7 @@ pulse_kernel(const __grid_constant__ PulseArgs a) {
     double spec_sum = 0.0, bragg_sum[2] = {0.0, 0.0};
     // persistent CTAs: each walks tiles of kPulseCols columns x tile_rows rows
     for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x)
-        pulse_tile<T, NOUT, S, kPulseRows, KA>(a, tile, a.tile_rows, sm, spec_sum, bragg_sum);
+        pulse_tile<T, NOUT, S, kPulseRows, MODE>(a, tile, a.tile_rows, sm, spec_sum, bragg_sum);
     pulse_nrcs<T>(a, sm, spec_sum, bragg_sum);
 }
 
@@ -636,7 +711,8 @@ batch_pulse_kernel(const __grid_constant__ BatchRef b) {
 template <typename T, int NOUT, int S>
 static int launch_pulse(PulseArgs a, cudaStream_t st) {
     const size_t smem = pulse_smem_bytes<T, NOUT, S, kPulseRows>(a.nch);
-    auto k = a.spec_mode != 0 ? pulse_kernel<T, NOUT, S, true> : pulse_kernel<T, NOUT, S, false>;
+    auto k = a.sca ? pulse_kernel<T, NOUT, S, kModeSca>
+                   : (a.spec_mode != 0 ? pulse_kernel<T, NOUT, S, kModeKa> : pulse_kernel<T, NOUT, S, kModeStd>);
     if (ensure_smem((const void *)k, smem) != cudaSuccess)
         return OCS_ERR_CUDA;
     const int resident = resident_ctas((const void *)k, kPulseCols, smem);
@@ -670,7 +746,7 @@ static int fill_pulse_args(const ocs_pulse_desc *d, PulseArgs &a) {
     if (d->do_kodis && (!d->diffx_d || !d->diffy_d || !d->diffxx_d || !d->diffyy_d || !d->diffxy_d ||
                         !d->tan_inc_d || !d->nrcs_spec_d))
         return OCS_ERR_ARG;
-    if (d->do_bragg && (!d->diffx_d || !d->diffy_d || !d->c_b_d || !d->scat_d || !d->s_m_d || !d->s_p_d ||
+    if (d->do_bragg && (!d->diffx_d || !d->diffy_d || !d->c_b_d || (!d->scat_d && !d->sca) || !d->s_m_d || !d->s_p_d ||
                         !d->ind0_m_d || !d->ind0_p_d || d->n_m < 1 || d->n_p < 1 || !d->spec_k_d ||
                         !d->spec_s_d || d->spec_n < 2 || !d->nrcs_bragg_d))
         return OCS_ERR_ARG;
@@ -729,6 +805,29 @@ static int fill_pulse_args(const ocs_pulse_desc *d, PulseArgs &a) {
     a.x_f = d->x_d;
     a.ka.k0 = d->k0; a.ka.dx = d->ka_dx; a.ka.dy = d->ka_dy; a.ka.K_re = d->ka_K_re; a.ka.K_im = d->ka_K_im;
     a.ka.mode = a.spec_mode == 2 ? 1 : 0;
+    if (d->sca) {
+        // scatterometer mode: one channel, Kodis specular, direct Bragg model, no hMTF; the
+        // columns are whole range blocks of field_nx columns; the Bragg RCS is evaluated on
+        // every launch and not stored
+        if (d->nch != 1 || d->field_nx < 1 || d->nx % d->field_nx != 0 || d->roll < 0 || d->roll >= d->ny ||
+            d->use_hmtf || a.spec_mode != 0 || d->lut_d)
+            return OCS_ERR_ARG;
+        if (!(d->sr_bin_offset >= 0.0) || !(d->cap_t >= 0.0)) return OCS_ERR_ARG;
+        if (d->nrcs_rows < 1 || d->nrcs_row < 0 || d->nrcs_row >= d->nrcs_rows) return OCS_ERR_ARG;
+        a.sca = 1;
+        a.az_f32 = d->az_f32 != 0;
+        a.nblk = d->nx / d->field_nx;
+        a.nrcs_row = d->nrcs_row;
+        a.nrcs_rows = d->nrcs_rows;
+        a.fnx = d->field_nx;
+        a.roll = d->roll;
+        a.sr_bin_off = d->sr_bin_offset;
+        a.cap_t = d->cap_t;
+        a.refresh = 1;
+        a.scat = nullptr;
+    } else {
+        a.fnx = d->nx;
+    }
     a.lut = d->lut_d;
     if (a.lut) {
         if (d->lut_naz < 1 || d->lut_ndy < 1 || d->lut_ndx < 1 || !(d->lut_daz != 0.0) || !(d->lut_ddy != 0.0) ||
@@ -746,6 +845,7 @@ namespace ocs {
 size_t pulse_args_bytes() { return sizeof(PulseArgs); }
 
 int pulse_args_fill(const ocs_pulse_desc *d, void *out) {
+    if (d && d->sca) return OCS_ERR_ARG;       // the scene batch runs SAR scenes only
     PulseArgs a;
     const int st = fill_pulse_args(d, a);
     if (st == OCS_OK) memcpy(out, &a, sizeof(a));

@@ -20,6 +20,7 @@ reference functions on the raw-data-generation path:
 * ``radarsim/sar_processor.py``  ``sar_focus`` on a seeded raw cube
 * ``radarsim/sar_raw_nompi.py``  ``sar_raw`` end to end (noise at -300 dB), plus the
   arguments and results of its first ``chan_profile_numba`` calls.
+* ``dopscasim/dopsca_raw.py``    ``dopsca_raw`` end to end (range blocks, sub-pulses).
 
 The fixtures are committed; tests never import the reference.
 """
@@ -611,6 +612,117 @@ def gen_cfg_and_sar(only=None):
         save("sar_raw_%s.npz" % name, **arrs)
 
 
+# --------------------------------------------------------------------------------------
+DOPSCA_TEMPLATE = """\
+# OCEANSAR DopSCA test configuration ({name})
+[sca]
+f0=5.4e9
+inc_angle={inc}
+pol={pol}
+prf={prf}
+rg_bw={rg_bw}
+over_fs=2.0
+squint=0
+alt=817e3
+v_ground={v_ground}
+heading=-11.2
+ant_L_tx=3
+ant_L_rx=3
+num_ch=1
+n_subpulses={n_sub}
+sub_pulse_length={sub_len}
+sub_pulse_bw=1e6
+nesz=-26
+use_errors=False
+sigma_n_tx=0.12
+phase_n_tx=2.3
+sigma_beta_tx=0.2
+phase_beta_tx=0.2
+sigma_n_rx=0.04
+phase_n_rx=0.2
+sigma_beta_rx=0.04
+phase_beta_rx=0.2
+
+[acquisition]
+length={length}
+
+[ocean]
+N_repeat_x={n_rep}
+Lx={Lx}
+Ly={Ly}
+dx={dx}
+dy={dy}
+opt_res=True
+dt=0.05
+depth=500
+wind_dir={wind_dir}
+wind_U=10
+wind_fetch=500e3
+swell_dir_enable=False
+sigf=0.007
+freq_r= .068
+dir_swell_dir = 70
+sigs=8
+Hs=1
+swell_enable=False
+swell_wl=80
+swell_dir=45
+swell_ampl=0.5
+spec_model=elfouhaily
+spread_model={spread}
+cutoff_wl=auto
+current_mag=0
+current_dir=0.
+frozen_ocean=False
+fft_max_prime=3
+choppy_enable={choppy}
+use_buoy_data=False
+
+[srg]
+use_hmtf=False
+nesz=-30.
+wh_tol=2.73
+scat_spec_enable={spec}
+scat_spec_mode=kodis
+scat_bragg_enable=True
+scat_bragg_model=romeiser97
+scat_bragg_spec=elfouhaily
+scat_bragg_spread={spread}
+scat_bragg_d=0.125
+use_lut = False
+"""
+
+# The sub-pulse lengths keep the scatterer series short (N ~ 200 tau / sub_pulse_length):
+# the reference factorises N by trial division in optimize_fftsize, which takes many
+# minutes for the ~1e6-sample series of microsecond sub-pulses.
+DOPSCA_CASES = {
+    # vv, Kodis + Bragg, three range blocks, two sub-pulses
+    "dsc1": dict(inc=35., pol='vv', prf=20., rg_bw=5e6, v_ground=7000., n_sub=2, sub_len=1e-3, length=2500.,
+                 n_rep=3, Lx=512, Ly=256, dx=4, dy=4, wind_dir=30., spread='cos2s', choppy=False, spec=True),
+    # dual pol, Bragg only, choppy surface, two blocks, three sub-pulses, orbital velocity
+    "dsc2": dict(inc=30., pol='DP', prf=10., rg_bw=2e6, v_ground='auto', n_sub=3, sub_len=5e-4, length=4000.,
+                 n_rep=2, Lx=256, Ly=128, dx=4, dy=4, wind_dir=0., spread='elfouhaily', choppy=True, spec=False),
+}
+
+
+def gen_dopsca():
+    from oceansar.dopscasim import dopsca_raw as ref_dopsca
+    for name, kw in DOPSCA_CASES.items():
+        path = os.path.join(OUT, "cfg", name + ".cfg")
+        with open(path, "w") as f:
+            f.write(DOPSCA_TEMPLATE.format(name=name, **kw))
+        np.random.seed(0)
+        out_file = "/tmp/golden_%s/raw.nc" % name
+        ocean_file = "/tmp/golden_%s/ocean.nc" % name
+        os.makedirs(os.path.dirname(out_file), exist_ok=True)
+        ref_dopsca.dopsca_raw(path, out_file, ocean_file, False, None, False, plot_save=False)
+        v = ref_shims.NC_STORE[out_file].variables
+        oc = ref_shims.NC_STORE[ocean_file].variables
+        save("dopsca_%s.npz" % name, raw=v['raw_data_r'].data + 1j * v['raw_data_i'].data,
+             NRCS_avg=v['NRCS_avg'].data, sr0=v['sr0'].data, v_ground=v['v_ground'].data,
+             wave_coefs=(oc['wave_coefs_r'].data + 1j * oc['wave_coefs_i'].data))
+
+
 if __name__ == "__main__":
     which = sys.argv[1:] or ["sinc", "range_profile", "surfaces", "rcs", "kodis", "closure",
                              "geometry", "sar"]
@@ -640,5 +752,7 @@ if __name__ == "__main__":
         gen_cfg_and_sar()
     if "sar_lut" in which:
         gen_cfg_and_sar(only=["c1lut"])
+    if "dopsca" in which:
+        gen_dopsca()
     if "sar_ka" in which:
         gen_cfg_and_sar(only=["c1fa", "c1spa"])

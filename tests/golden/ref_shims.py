@@ -19,6 +19,9 @@ replaces one of them without touching the reference sources:
    arrays (``or`` between boolean arrays).  Its evident intent, G = cos^2(theta)/pi inside
    |theta| <= pi/2 and 0 outside, is registered in its place; the product implements the
    same function.
+7. ``drama.io.cfg``: the DopSCA generator reads its .cfg through the (absent) drama
+   package; the reference's own ``oceansar.ocs_io.cfg`` module parses the same format and
+   is registered as ``drama.io.cfg``.
 6. ``mpi4py.MPI``: a one-process communicator (rank 0 of 1) for
    ``surfaces/balancer.py``; ``bcast`` returns its argument and ``Scatterv`` copies the
    root's float32 buffer into the receive buffer (with one process the whole surface is
@@ -167,6 +170,14 @@ def install():
     if REF_ROOT not in sys.path:
         sys.path.insert(0, REF_ROOT)
     import oceansar  # noqa: F401
+    from oceansar.ocs_io import cfg as ocs_cfg
+    drama = types.ModuleType("drama")
+    drama_io = types.ModuleType("drama.io")
+    drama_io.cfg = ocs_cfg
+    drama.io = drama_io
+    sys.modules["drama"] = drama
+    sys.modules["drama.io"] = drama_io
+    sys.modules["drama.io.cfg"] = ocs_cfg
     from oceansar import spread
     spread.models["cos2s"] = cos2s_restated
     return oceansar

@@ -290,3 +290,18 @@ def test_sar_raw_interpolated_surface_one_step():
     assert sim.balancer is not None and sim.t_step == 0.001
     err = np.linalg.norm(raw - d["raw"]) / np.linalg.norm(d["raw"])
     assert err < 1e-5, err
+
+
+@pytest.mark.parametrize("name", ["dsc1", "dsc2"])
+def test_dopsca_end_to_end(name):
+    """DopSCA scatterometer generator (dopscasim/dopsca_raw.py) against the reference's run:
+    range blocks, rolled surface rows, sub-pulses, two-way range scaling."""
+    from oracle.dopsca_raw import dopsca_raw
+    d = load("dopsca_%s.npz" % name)
+    raw, nrcs_avg, sim = dopsca_raw(os.path.join(G, "cfg", name + ".cfg"), seed=0)
+    assert raw.shape == d["raw"].shape
+    np.testing.assert_array_equal(sim.surface.wave_coefs, d["wave_coefs"])
+    err = np.linalg.norm(raw - d["raw"]) / np.linalg.norm(d["raw"])
+    assert err < 1e-12, err
+    np.testing.assert_allclose(nrcs_avg, d["NRCS_avg"], rtol=1e-12)
+    assert float(d["sr0"]) == pytest.approx(sim.sr_near, rel=1e-15)
