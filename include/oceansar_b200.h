@@ -258,6 +258,17 @@ typedef struct {
     double sr_bin_offset, cap_t;
     int32_t nrcs_row, nrcs_rows;
     int32_t az_f32;
+    /* SKIM mode (skim = 1; the SKIM generator, radarsim/skim_raw.py:465-689): sin_az =
+     * az / sr per facet (sr_col_d holds absolute slant ranges), the two-way antenna pattern
+     * per facet (ant_l_tx / ant_l_rx: transmit / receive lengths, power units), a 10-tap
+     * pulse (sinc_d: calc_sinc_vec(10, 20, Fs)), and the facets of every skim_ny_integ rows
+     * accumulated into their own row: raw_d is [npol][az_steps][ny / skim_ny_integ][nbins]
+     * (skim_ny_integ = ny: one row per pulse).  skim_az2: az/2 sin_az is part of the phase
+     * range (the single-scale form); skim_rcm: it is added to the range bins only.
+     * skim_ny_integ must divide ny and, when below ny, be a power of two above 64.  Requires
+     * nch = 1; Kodis or Kirchhoff specular; direct or LUT Bragg model.  The scene batch
+     * rejects it. */
+    int32_t skim, skim_ny_integ, skim_az2, skim_rcm;
 } ocs_pulse_desc;
 
 /* Workspace of ocs_pulse (per-pulse table of the row quantities); < 0 on invalid sizes. */

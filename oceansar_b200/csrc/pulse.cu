@@ -22,6 +22,12 @@
 // cap_t, the range bins see the sub-pulse delay sr_bin_off, and the NRCS sums are kept per
 // range block.
 //
+// SKIM mode (MODE & kModeSkim, the SKIM generator, oceansar/radarsim/skim_raw.py:465-689):
+// sin_az = az / sr per facet (absolute slant range of the column), the two-way antenna
+// pattern evaluated per facet, 10-tap pulse, and the facets of every ny_integ rows
+// accumulated into their own output row (the two-scale Doppler's range-only profiles
+// summed over ny_integ rows; ny_integ = ny gives the single-row form).
+//
 // Precision forms (template T):
 //   double -- the drop-in: every operation in float64 in the reference's order; slant
 //             range and the bin / LUT indices bit-identical to numpy.
@@ -41,7 +47,11 @@ constexpr int kPulseRowsMax = 128;  // largest rows per tile (shared row tables)
 constexpr int kMaxCh = 8;
 constexpr int kPulseNbw = 160;      // CTA shared bin window
 
-enum { kModeStd = 0, kModeKa = 1, kModeSca = 2 };
+// Kernel modes (bits): Kirchhoff specular, scatterometer (DopSCA), SKIM; SKIM combines with
+// the Kirchhoff specular term (kModeSkim | kModeKa).
+enum { kModeStd = 0, kModeKa = 1, kModeSca = 2, kModeSkim = 4 };
+constexpr int kSkimTaps = 10;       // n_sinc_samples of the SKIM generator (skim_raw.py:164)
+template <int MODE> __host__ __device__ constexpr int mode_taps() { return (MODE & kModeSkim) ? kSkimTaps : kSincTaps; }
 
 struct PulseArgs {
     int nx, ny, npol, nch;
@@ -84,6 +94,9 @@ struct PulseArgs {
     double sr_bin_off, cap_t;               // sub-pulse range delay, Bragg phase time
     int nblk, nrcs_row, nrcs_rows;          // range blocks; NRCS row of this call, rows in all
     int az_f32;                             // azimuth y - az_now rounded to float32 (see pulse_row)
+    int skim, ny_integ, s_int;              // SKIM mode: output row per ny_integ facet rows
+    int skim_az2, skim_rcm;                 // SKIM: az/2 sin_az in the phase range / in the bins only
+    double atx, arx;                        // SKIM: antenna lengths / wavelength (tx, rx)
 };
 
 // Kirchhoff specular term of one facet and polarisation code pc (0 = hh, 1 = vv),
@@ -341,6 +354,7 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
     cb.nout = a.nout;
     cb.nbins = a.nbins;
     cb.out = reinterpret_cast<T *>(a.raw) + 2 * ((long long)a.out0 * a.raw_out_stride + a.raw_row);
+    if constexpr ((MODE & kModeSkim) != 0) cb.out += 2 * (long long)(y0 / a.ny_integ) * a.nbins;
     cb.out_stride = a.raw_out_stride;
     {
         // window base: bin of this CTA's first column at its first row, undisplaced
@@ -430,17 +444,22 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
             cp_async_commit();
             cur.read(a, st, slot_i, load_scat);
             slot_i = slot_n;
-            const double az = sm.r_az[i], sin_az = sm.r_az[RCAP + i];
+            const double az = sm.r_az[i];
+            // SKIM: sin_az = az / sr of this facet's column (skim_raw.py:486)
+            const double sin_az = (MODE & kModeSkim) ? ddiv(az, sr_c) : sm.r_az[RCAP + i];
             // slant range: sr - cos_inc*Dz + az/2*sin_az + Dx*sin_inc + Dy*sin_az, float64,
-            // left to right, no fused multiply-adds (bit-identical with numpy)
+            // left to right, no fused multiply-adds (bit-identical with numpy); the SKIM
+            // two-scale form leaves az/2*sin_az out of the phase range (skim_raw.py:494-505)
             double srs = dsub(sr_c, dmul(cos_i, (double)cur.dz));
-            srs = dadd(srs, dmul(az * 0.5, sin_az));
+            if (!(MODE & kModeSkim) || a.skim_az2) srs = dadd(srs, dmul(az * 0.5, sin_az));
             srs = dadd(srs, dmul((double)cur.dx, sin_i));
             srs = dadd(srs, dmul((double)cur.dy, sin_az));
             int bin_d, lut;
             {
-                // the scatterometer's sub-pulses arrive later by sr_bin_off (range bins only)
-                const double srb = (MODE == kModeSca) ? dadd(srs, a.sr_bin_off) : srs;
+                // the scatterometer's sub-pulses arrive later by sr_bin_off; the SKIM
+                // two-scale form with rcm adds az/2*sin_az to the bins only
+                double srb = (MODE == kModeSca) ? dadd(srs, a.sr_bin_off) : srs;
+                if ((MODE & kModeSkim) && a.skim_rcm) srb = dadd(srs, dmul(az * 0.5, sin_az));
                 if (sizeof(T) == 8) bin_and_lut(srb, a.min_sr, a.binsize, kSincOvs, bin_d, lut);
                 else bin_and_lut_fast(srb, a.min_sr, a.inv_binsize, kSincOvs, bin_d, lut);
             }
@@ -452,7 +471,7 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
             }
 
             cplx<T> scene[2] = {{(T)0, (T)0}, {(T)0, (T)0}};      // per polarisation
-            if constexpr (MODE == kModeKa) {
+            if constexpr ((MODE & kModeKa) != 0) {
                 c128 last = {0.0, 0.0};
                 for (int p = 0; p < a.npol; ++p) {
                     const int pc = a.rom.pol == POL_DP ? p : (a.rom.pol == POL_HH ? 0 : 1);
@@ -559,12 +578,33 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
             cplx<T> coef[NOUT];
             double wave_dinc = 0.0;
             if (a.any_xti) wave_dinc = ((double)cur.dz * sin_i + (double)cur.dx * sin_i) / a.sr0;
+            T bp_f = (T)1;
+            if constexpr ((MODE & kModeSkim) != 0) {
+                // two-way antenna pattern of this facet, power units for both the transmit
+                // and the receive pattern (antenna.py:28-42 passes its field flag to the
+                // positional catch-all of sinc_bp)
+                T tx, rx;
+                if constexpr (sizeof(T) == 8) {
+                    tx = np_sinc(a.atx * sin_az);
+                    rx = np_sinc(a.arx * sin_az);
+                } else {
+                    tx = np_sinc((float)(a.atx * sin_az));
+                    rx = np_sinc((float)(a.arx * sin_az));
+                }
+                bp_f = (tx * tx) * (rx * rx);
+            }
 #pragma unroll
             for (int k = 0; k < NOUT; ++k) {
                 if (k < a.nout) {
                     const unsigned ok = outs >> (5 * k);
                     const int c = ok & 7;
-                    cplx<T> v = cmul((ok & 8) ? scene[1] : scene[0], sm.r_fac[i * a.nch + c]);
+                    cplx<T> v;
+                    if constexpr ((MODE & kModeSkim) != 0) {
+                        const cplx<T> sc = (ok & 8) ? scene[1] : scene[0];
+                        v = {sc.re * bp_f, sc.im * bp_f};
+                    } else {
+                        v = cmul((ok & 8) ? scene[1] : scene[0], sm.r_fac[i * a.nch + c]);
+                    }
                     if (ok & 16) {
                         const double ph = (-a.k0 * a.b_xti[c]) * (dinc0 + wave_dinc);
                         v = cmul(v, cexp_phase<T>(ph));
@@ -575,7 +615,7 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
                 }
             }
             if (bin_d > -(1 << 29))
-                win.add(bin_d - kSincTaps / 2, lut, coef, sm.wtab, a.sinc, kSincTaps, kSincOvs, cb);
+                win.add(bin_d - mode_taps<MODE>() / 2, lut, coef, sm.wtab, a.sinc, mode_taps<MODE>(), kSincOvs, cb);
         }
         cp_async_wait<0>();
     }
@@ -614,7 +654,7 @@ __global__ void __launch_bounds__(kPulseCols, (sizeof(T) == 4 && NOUT < 4) ? 4 :
 pulse_kernel(const __grid_constant__ PulseArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     const PulseSmem<T> sm = pulse_smem<T, NOUT, S, kPulseRows>(smem, a.nch);
-    build_wtab<T, S>(sm.wtab, a.sinc, kSincTaps, kSincOvs);
+    build_wtab<T, S>(sm.wtab, a.sinc, mode_taps<MODE>(), kSincOvs);
     const int tiles = ((a.nx + kPulseCols - 1) / kPulseCols) * ((a.ny + a.tile_rows - 1) / a.tile_rows);
     double spec_sum = 0.0, bragg_sum[2] = {0.0, 0.0};
     // persistent CTAs: each walks tiles of kPulseCols columns x tile_rows rows
@@ -712,7 +752,9 @@ template <typename T, int NOUT, int S>
 static int launch_pulse(PulseArgs a, cudaStream_t st) {
     const size_t smem = pulse_smem_bytes<T, NOUT, S, kPulseRows>(a.nch);
     auto k = a.sca ? pulse_kernel<T, NOUT, S, kModeSca>
-                   : (a.spec_mode != 0 ? pulse_kernel<T, NOUT, S, kModeKa> : pulse_kernel<T, NOUT, S, kModeStd>);
+           : a.skim ? (a.spec_mode != 0 ? pulse_kernel<T, NOUT, S, kModeSkim | kModeKa>
+                                        : pulse_kernel<T, NOUT, S, kModeSkim>)
+                    : (a.spec_mode != 0 ? pulse_kernel<T, NOUT, S, kModeKa> : pulse_kernel<T, NOUT, S, kModeStd>);
     if (ensure_smem((const void *)k, smem) != cudaSuccess)
         return OCS_ERR_CUDA;
     const int resident = resident_ctas((const void *)k, kPulseCols, smem);
@@ -726,6 +768,14 @@ static int launch_pulse(PulseArgs a, cudaStream_t st) {
     if (per_col < 1) per_col = 1;
     int rows = (int)((a.ny + per_col - 1) / per_col);
     a.tile_rows = rows < 16 ? (a.ny < 16 ? a.ny : 16) : (rows > kPulseRows ? kPulseRows : rows);
+    // SKIM: a tile must not straddle two output rows (ny_integ is a power of two or ny)
+    if (a.skim && a.ny_integ < a.ny) {
+        a.tile_rows = a.ny_integ;
+        while (a.tile_rows > kPulseRows) {
+            if (a.tile_rows % 2) return OCS_ERR_ARG;
+            a.tile_rows /= 2;
+        }
+    }
     const long long tiles = (long long)tiles_x * ((a.ny + a.tile_rows - 1) / a.tile_rows);
     const long long grid = tiles < resident ? tiles : resident;
     k<<<(unsigned)grid, kPulseCols, smem, st>>>(a);
@@ -805,6 +855,24 @@ static int fill_pulse_args(const ocs_pulse_desc *d, PulseArgs &a) {
     a.x_f = d->x_d;
     a.ka.k0 = d->k0; a.ka.dx = d->ka_dx; a.ka.dy = d->ka_dy; a.ka.K_re = d->ka_K_re; a.ka.K_im = d->ka_K_im;
     a.ka.mode = a.spec_mode == 2 ? 1 : 0;
+    if (d->skim) {
+        // SKIM mode: one channel; the facets of every skim_ny_integ rows go to their
+        // own output row: raw_d holds [npol][az_steps][ny / skim_ny_integ][nbins]
+        if (d->sca || d->nch != 1 || d->skim_ny_integ < 1 || d->ny % d->skim_ny_integ != 0) return OCS_ERR_ARG;
+        if (d->skim_ny_integ > kPulseRows && d->skim_ny_integ < d->ny) {
+            for (int n = d->skim_ny_integ; n > kPulseRows; n /= 2)
+                if (n % 2) return OCS_ERR_ARG;
+        }
+        a.skim = 1;
+        a.ny_integ = d->skim_ny_integ;
+        a.s_int = d->ny / d->skim_ny_integ;
+        a.skim_az2 = d->skim_az2 != 0;
+        a.skim_rcm = d->skim_rcm != 0;
+        a.atx = a.ltx_over_l;
+        a.arx = a.lrx_over_l;
+        a.raw_out_stride = (long long)d->az_steps * a.s_int * d->nbins;
+        a.raw_row = (long long)d->az_step * a.s_int * d->nbins;
+    }
     if (d->sca) {
         // scatterometer mode: one channel, Kodis specular, direct Bragg model, no hMTF; the
         // columns are whole range blocks of field_nx columns; the Bragg RCS is evaluated on
@@ -845,7 +913,7 @@ namespace ocs {
 size_t pulse_args_bytes() { return sizeof(PulseArgs); }
 
 int pulse_args_fill(const ocs_pulse_desc *d, void *out) {
-    if (d && d->sca) return OCS_ERR_ARG;       // the scene batch runs SAR scenes only
+    if (d && (d->sca || d->skim)) return OCS_ERR_ARG;   // the scene batch runs SAR scenes only
     PulseArgs a;
     const int st = fill_pulse_args(d, a);
     if (st == OCS_OK) memcpy(out, &a, sizeof(a));

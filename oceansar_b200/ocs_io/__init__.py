@@ -3,5 +3,5 @@ ocean-state files in the netCDF classic format (``netcdf3``)."""
 from .cfg import ConfigFile  # noqa: F401
 from .netcdf import NETCDFHandler  # noqa: F401
 from .processed import ProcFile  # noqa: F401
-from .raw import DopscaRawFile, RawFile  # noqa: F401
+from .raw import DopscaRawFile, RawFile, SkimRawFile  # noqa: F401
 from .state import OceanStateFile  # noqa: F401

@@ -35,6 +35,22 @@ def max_look_angle(orbit_alt, r_planet=R_EARTH):
     return np.arcsin(r_planet / (r_planet + orbit_alt))
 
 
+def sr_to_geo(slant_range, orbit_alt, r_planet=R_EARTH, m_planet=M_EARTH):
+    """Ground range, incidence, look angle and b = v_orb^2 r_track / (r_planet + h) at the
+    given slant ranges (geometry.py:101-133): quadratic splines through 2500 look angles."""
+    theta_l = np.linspace(0, max_look_angle(orbit_alt, r_planet=r_planet), 2500)
+    theta_i = look_to_inc(theta_l, orbit_alt, r_planet=r_planet)
+    delta_theta = theta_i - theta_l
+    r_track = np.cos(delta_theta) * r_planet
+    v_orb = orbit_to_vel(orbit_alt, r_planet=r_planet, m_planet=m_planet)
+    b = v_orb ** 2 * r_track / (r_planet + orbit_alt)
+    gr = r_planet * delta_theta
+    sr = np.sqrt((orbit_alt + r_planet - r_planet * np.cos(delta_theta)) ** 2 + (r_planet * np.sin(delta_theta)) ** 2)
+    spl = interpolate.InterpolatedUnivariateSpline
+    return (spl(sr, gr, k=2)(slant_range), spl(sr, theta_i, k=2)(slant_range),
+            spl(sr, theta_l, k=2)(slant_range), spl(sr, b, k=2)(slant_range))
+
+
 def gr_to_geo(ground_range, orbit_alt, r_planet=R_EARTH):
     theta_l = np.linspace(0, max_look_angle(orbit_alt), 500)
     theta_i = look_to_inc(theta_l, orbit_alt, r_planet=r_planet)

@@ -21,6 +21,7 @@ reference functions on the raw-data-generation path:
 * ``radarsim/sar_raw_nompi.py``  ``sar_raw`` end to end (noise at -300 dB), plus the
   arguments and results of its first ``chan_profile_numba`` calls.
 * ``dopscasim/dopsca_raw.py``    ``dopsca_raw`` end to end (range blocks, sub-pulses).
+* ``radarsim/skim_raw.py``       ``skimraw`` end to end on one process (two-scale Doppler).
 
 The fixtures are committed; tests never import the reference.
 """
@@ -723,6 +724,124 @@ def gen_dopsca():
              wave_coefs=(oc['wave_coefs_r'].data + 1j * oc['wave_coefs_i'].data))
 
 
+# --------------------------------------------------------------------------------------
+SKIM_TEMPLATE = """\
+# OCEANSAR SKIM test configuration ({name})
+[sim]
+verbosity=0
+
+[radar]
+f0=35e9
+inc_angle={inc}
+pol={pol}
+prf=32e3
+rg_bw=200e6
+Fs = 250e6
+n_pulses = {n_pulses}
+n_rg = 128
+over_fs=1.1
+azimuth = {azimuth}
+alt=690e3
+v_ground=auto
+heading=-11.2
+ant_L={ant_L}
+L_total={L_total}
+Spacing=50
+num_ch={num_ch}
+use_errors=False
+sigma_n_tx=0.12
+phase_n_tx=2.3
+sigma_beta_tx=0.2
+phase_beta_tx=0.2
+sigma_n_rx=0.04
+phase_n_rx=0.2
+sigma_beta_rx=0.04
+phase_beta_rx=0.2
+
+[ocean]
+Lx=64.
+Ly=64.
+dx=1
+dy=1
+opt_res=True
+depth=100
+wind_dir=45.
+wind_U={wind_U}
+wind_fetch=500e3
+swell_enable=False
+swell_wl=12.5
+swell_dir=90
+swell_ampl=1
+swell_dir_enable={dir_swell}
+sigf=0.007
+freq_r= .068
+dir_swell_dir=90
+sigs=8
+Hs=1.45
+spec_model=elfouhaily
+spread_model=elfouhaily
+cutoff_wl=auto
+current_mag=0.2
+current_dir=90.
+dt=0.002
+fft_max_prime=3
+choppy_enable={choppy}
+use_buoy_data=False
+
+[srg]
+use_hmtf=False
+nesz=-300.
+wh_tol=5.
+scat_spec_enable={spec}
+scat_spec_mode={spec_mode}
+scat_bragg_enable=True
+scat_bragg_model=romeiser97
+scat_bragg_spec=elfouhaily
+scat_bragg_spread=elfouhaily
+scat_bragg_d=0.125
+two_scale_Doppler={two_scale}
+surface_coh_time=2e-3
+phase_err_tol=0.5
+rcm = {rcm}
+"""
+
+# The antenna lengths keep at least two samples in the calibration's azimuth axis (step
+# sr0 c / (pi f0 L 10)) over these short acquisitions; with one sample the reference's
+# calibration factor is 1/sqrt(0).
+SKIM_CASES = {
+    # the shipped SKIM set-up, scaled down: vv, stationary-phase specular + Bragg, choppy,
+    # directional swell, two-scale Doppler (8 simulated steps, groups of 16 rows)
+    "skim1": dict(inc=12., pol='vv', n_pulses=256, azimuth=90, ant_L=10, L_total=False, num_ch=1, wind_U=3.,
+                  dir_swell=True, choppy=True, spec=True, spec_mode='spa', two_scale=True, rcm=False),
+    # dual pol, facet-approach specular + Bragg, squinted beam, L_total with two channels,
+    # rcm in the bins (the reference's Kodis field fails on [Ny, 1] azimuth angles as soon
+    # as a stationary point lies outside column 0, kodis.py:61)
+    "skim2": dict(inc=10., pol='DP', n_pulses=256, azimuth=60, ant_L=10, L_total=True, num_ch=2, wind_U=7.,
+                  dir_swell=False, choppy=False, spec=True, spec_mode='fa', two_scale=True, rcm=True),
+    # single-scale form: every pulse simulated, all rows in one profile
+    "skim3": dict(inc=12., pol='vv', n_pulses=64, azimuth=90, ant_L=30, L_total=False, num_ch=1, wind_U=5.,
+                  dir_swell=False, choppy=False, spec=False, spec_mode='kodis', two_scale=False, rcm=False),
+}
+
+
+def gen_skim():
+    from oceansar.radarsim import skim_raw as ref_skim
+    for name, kw in SKIM_CASES.items():
+        path = os.path.join(OUT, "cfg", name + ".cfg")
+        with open(path, "w") as f:
+            f.write(SKIM_TEMPLATE.format(name=name, **kw))
+        np.random.seed(0)
+        out_file = "/tmp/golden_%s/raw.nc" % name
+        ocean_file = "/tmp/golden_%s/ocean.nc" % name
+        os.makedirs(os.path.dirname(out_file), exist_ok=True)
+        ref_skim.skimraw(path, out_file, ocean_file, False, None, False, plot_save=False)
+        v = ref_shims.NC_STORE[out_file].variables
+        oc = ref_shims.NC_STORE[ocean_file].variables
+        save("skim_%s.npz" % name, raw=v['raw_data_r'].data + 1j * v['raw_data_i'].data,
+             NRCS_avg=v['NRCS_avg'].data, dop_ref=v['dop_ref'].data, sr0=v['sr0'].data,
+             wave_coefs=(oc['wave_coefs_r'].data + 1j * oc['wave_coefs_i'].data))
+
+
 if __name__ == "__main__":
     which = sys.argv[1:] or ["sinc", "range_profile", "surfaces", "rcs", "kodis", "closure",
                              "geometry", "sar"]
@@ -754,5 +873,7 @@ if __name__ == "__main__":
         gen_cfg_and_sar(only=["c1lut"])
     if "dopsca" in which:
         gen_dopsca()
+    if "skim" in which:
+        gen_skim()
     if "sar_ka" in which:
         gen_cfg_and_sar(only=["c1fa", "c1spa"])

@@ -25,7 +25,7 @@ replaces one of them without touching the reference sources:
 6. ``mpi4py.MPI``: a one-process communicator (rank 0 of 1) for
    ``surfaces/balancer.py``; ``bcast`` returns its argument and ``Scatterv`` copies the
    root's float32 buffer into the receive buffer (with one process the whole surface is
-   the root's share).
+   the root's share); ``Reduce`` copies (the sum over one process).
 """
 import sys
 import types
@@ -132,6 +132,9 @@ class _Comm:
         dst = recvbuf[0]
         dst.reshape(-1)[:] = src.reshape(-1)[:dst.size]
 
+    def Reduce(self, sendbuf, recvbuf, op=None, root=0):
+        recvbuf[...] = sendbuf
+
 
 def install():
     """Install the shims and put the reference on ``sys.path``; returns the package."""
@@ -163,7 +166,7 @@ def install():
         np.trapz = np.trapezoid
 
     mpi = types.ModuleType("mpi4py")
-    mpi.MPI = types.SimpleNamespace(COMM_WORLD=_Comm(), FLOAT="MPI_FLOAT")
+    mpi.MPI = types.SimpleNamespace(COMM_WORLD=_Comm(), FLOAT="MPI_FLOAT", SUM="MPI_SUM")
     sys.modules["mpi4py"] = mpi
     sys.modules["mpi4py.MPI"] = mpi.MPI
 
