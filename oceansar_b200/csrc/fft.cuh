@@ -151,7 +151,32 @@ OCS_D void fft_stage_pow2(float2 *buf, int vstride, const float2 *tw, const Ld &
     constexpr int in_step = nb + nb / 8;                       // padded stride of the reads
     constexpr int out_step = (NS % 8 == 0) ? NS + NS / 8 : NS; // padded stride of the writes
     static_assert(NS == 1 || NS % 8 == 0, "stage spans must be 1 or multiples of 8");
-    if constexpr (FIRST || LAST) {
+    if constexpr (FIRST && !LAST && NS == 1) {
+        // first stage from a loader: every load of the thread's butterflies is issued
+        // before the first transform (NS == 1: no twiddles)
+        float2 v[IT][R];
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int b = threadIdx.x + it * blockDim.x;
+            if (b < nb * NVEC) {
+                const int vec = b % NVEC, j = b / NVEC;
+#pragma unroll
+                for (int r = 0; r < R; ++r) v[it][r] = ld(vec, j + r * nb);
+            }
+        }
+#pragma unroll
+        for (int it = 0; it < IT; ++it) {
+            const int b = threadIdx.x + it * blockDim.x;
+            if (b < nb * NVEC) {
+                const int vec = b % NVEC, j = b / NVEC;
+                dft_inv<R>(v[it]);
+                float2 *y = buf + vec * vstride + pad_idx(j * R);
+#pragma unroll
+                for (int r = 0; r < R; ++r) y[r * out_step] = v[it][r];
+            }
+        }
+        __syncthreads();
+    } else if constexpr (FIRST || LAST) {
         // independent butterflies: nothing else in shared memory is read (FIRST) or
         // written (LAST) in this stage, so each result is written out immediately
 #pragma unroll

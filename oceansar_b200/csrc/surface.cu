@@ -110,6 +110,14 @@ OCS_D float2 phased(const SurfaceArgs &a, int y, int x) {
     return make_float2(fsub(fmul(c.x, co), fmul(c.y, s)), fadd(fmul(c.x, s), fmul(c.y, co)));
 }
 
+// c exp(-i fl(omega t)) from values already loaded (the same arithmetic as phased).
+OCS_D float2 phased_v(float2 c, float om, float t) {
+    float ph = -fmul(om, t);
+    float s, co;
+    sincosf(ph, &s, &co);
+    return make_float2(fsub(fmul(c.x, co), fmul(c.y, s)), fadd(fmul(c.x, s), fmul(c.y, co)));
+}
+
 // Threads per CTA of the two passes for a power-of-two length N (0 = any length).
 template <int N> __host__ __device__ constexpr int rows_threads() {
     return N == 0 ? 256 : (N / 4 < 64 ? 64 : (N / 4 > 1024 ? 1024 : N / 4));
@@ -275,9 +283,30 @@ OCS_D void rows_item(const SurfaceArgs &a, int r, float2 *sbuf, bool load_tw) {
     const float kyr = a.ky[r], kymr = a.ky[mr];
     const float *omA = a.omega + (size_t)r * nx, *omB = a.omega + (size_t)mr * nx;
 
-    for (int x = threadIdx.x; x < nx; x += blockDim.x) {
-        cA[x] = phased(a, r, x);
-        cB[x] = phased(a, mr, x);
+    if constexpr (N > 0 && N % rows_threads<N>() == 0) {
+        // all loads of the thread's columns first, then the phase rotations
+        constexpr int T = rows_threads<N>(), J = N / T;
+        float2 c0[J], c1[J];
+        float o0[J], o1[J];
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+            const int x = threadIdx.x + j * T;
+            c0[j] = a.coefs[(size_t)r * nx + x];
+            c1[j] = a.coefs[(size_t)mr * nx + x];
+            o0[j] = a.omega[(size_t)r * nx + x];
+            o1[j] = a.omega[(size_t)mr * nx + x];
+        }
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+            const int x = threadIdx.x + j * T;
+            cA[x] = phased_v(c0[j], o0[j], a.t);
+            cB[x] = phased_v(c1[j], o1[j], a.t);
+        }
+    } else {
+        for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+            cA[x] = phased(a, r, x);
+            cB[x] = phased(a, mr, x);
+        }
     }
     __syncthreads();
 
