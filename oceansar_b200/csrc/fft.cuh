@@ -1,10 +1,11 @@
-// Shared-memory mixed-radix (2, 3, 4, 5, 7, 8) inverse FFT used by the surface kernels.
+// Shared-memory mixed-radix (2, 3, 4, 5, 7, 8, 16) inverse FFT used by the surface kernels.
 //
 // A CTA transforms `nvec` vectors of length n held in shared memory with the
 // self-sorting Stockham formulation: at a stage of radix R after radices of product Ns,
 // butterfly j reads x[j + r*n/R] (r < R), multiplies by w^(r*(j mod Ns)*n/(Ns*R)),
 // takes an R-point DFT and writes x[(j/Ns)*Ns*R + j mod Ns + r*Ns].  Power-of-two lengths
-// are compiled per length (radix 8, then one 4 or 2): each thread keeps its butterflies in
+// are compiled per length (radix 16 while it divides, then 8, then one 4 or 2;
+// pow2_stage_radix): each thread keeps its butterflies in
 // registers between a read phase and a write phase separated by a barrier, so one buffer
 // suffices.  Other lengths (primes 3, 5, 7) run a runtime plan out of place between two
 // buffers.  Element i of a vector lives at smem index
@@ -122,6 +123,47 @@ template <> OCS_D void dft_inv<7>(float2 *v) {
     }
 }
 
+// Radix-16 inverse DFT as 4 x 4: A[n2][k1] = DFT4 over n1 of v[4 n1 + n2], then
+// X[k1 + 4 k2] = DFT4 over n2 of w16^(n2 k1) A[n2][k1], w16 = exp(+2 pi i / 16).
+template <> OCS_D void dft_inv<16>(float2 *v) {
+    const float c1 = 0.92387953251128674f, s1 = 0.38268343236508977f, h = 0.70710678118654752f;
+    float2 a[4][4];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) {
+        float2 t[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
+        dft_inv<4>(t);
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) a[n2][k1] = t[k1];
+    }
+    // twiddles w16^(n2 k1): m = 0, 1, 2, 3 (n2 = 1), 0, 2, 4, 6 (n2 = 2), 0, 3, 6, 9 (n2 = 3)
+    const float2 w1 = make_float2(c1, s1), w2 = make_float2(h, h), w3 = make_float2(s1, c1);
+    const float2 w6 = make_float2(-h, h), w9 = make_float2(-c1, -s1);
+    a[1][1] = c_mul(a[1][1], w1);
+    a[1][2] = c_mul(a[1][2], w2);
+    a[1][3] = c_mul(a[1][3], w3);
+    a[2][1] = c_mul(a[2][1], w2);
+    a[2][2] = c_ipos(a[2][2]);
+    a[2][3] = c_mul(a[2][3], w6);
+    a[3][1] = c_mul(a[3][1], w3);
+    a[3][2] = c_mul(a[3][2], w6);
+    a[3][3] = c_mul(a[3][3], w9);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+        float2 t[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+        dft_inv<4>(t);
+#pragma unroll
+        for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = t[k2];
+    }
+}
+
+// Radix of the stage of a power-of-two transform of length n that follows radices of
+// product ns: 16 while 16 divides the rest (for n a multiple of 128, so that every stage
+// has a multiple of 8 butterflies per vector), then 8, then the remaining 4 or 2.  The
+// stage-major twiddle table is built with the same sequence.
+OCS_HD constexpr int pow2_stage_radix(int n, int ns) {
+    return ((n / ns) % 16 == 0 && n % 128 == 0) ? 16 : (((n / ns) % 8 == 0) ? 8 : n / ns);
+}
+
 // Power-of-two lengths: NVEC vectors of compile-time length N, T threads.  Butterfly b
 // of a stage maps to vector b % NVEC and index b / NVEC (vector fastest), and vectors sit
 // pow2_vstride(N, NVEC) slots apart, so that the 16 lanes of a half-warp always hit 16
@@ -149,7 +191,9 @@ OCS_D void fft_stage_pow2(float2 *buf, int vstride, const float2 *tw, const Ld &
     constexpr int nb = N / R;
     static_assert(nb % 8 == 0, "power-of-two stages need N/R to be a multiple of 8");
     constexpr int in_step = nb + nb / 8;                       // padded stride of the reads
-    constexpr int out_step = (NS % 8 == 0) ? NS + NS / 8 : NS; // padded stride of the writes
+    // padded offset of output r from output 0: the writes go to d + r*NS; with NS a multiple
+    // of 8 that is r*(NS + NS/8) slots, with NS == 1 (d a multiple of 8) it is pad_idx(r)
+    auto out_off = [](int r) { return (NS % 8 == 0) ? r * (NS + NS / 8) : r + (r >> 3); };
     static_assert(NS == 1 || NS % 8 == 0, "stage spans must be 1 or multiples of 8");
     if constexpr (FIRST && !LAST && NS == 1) {
         // first stage from a loader: every load of the thread's butterflies is issued
@@ -172,7 +216,7 @@ OCS_D void fft_stage_pow2(float2 *buf, int vstride, const float2 *tw, const Ld &
                 dft_inv<R>(v[it]);
                 float2 *y = buf + vec * vstride + pad_idx(j * R);
 #pragma unroll
-                for (int r = 0; r < R; ++r) y[r * out_step] = v[it][r];
+                for (int r = 0; r < R; ++r) y[out_off(r)] = v[it][r];
             }
         }
         __syncthreads();
@@ -202,7 +246,7 @@ OCS_D void fft_stage_pow2(float2 *buf, int vstride, const float2 *tw, const Ld &
                 } else {
                     float2 *y = buf + vec * vstride + pad_idx(d);
 #pragma unroll
-                    for (int r = 0; r < R; ++r) y[r * out_step] = v[r];
+                    for (int r = 0; r < R; ++r) y[out_off(r)] = v[r];
                 }
             }
         }
@@ -234,21 +278,21 @@ OCS_D void fft_stage_pow2(float2 *buf, int vstride, const float2 *tw, const Ld &
                 const int jm = j % NS;
                 float2 *y = buf + vec * vstride + pad_idx((j - jm) * R + jm);
 #pragma unroll
-                for (int r = 0; r < R; ++r) y[r * out_step] = v[it][r];
+                for (int r = 0; r < R; ++r) y[out_off(r)] = v[it][r];
             }
         }
         __syncthreads();
     }
 }
 
-// The whole transform: radix-8 stages, then one radix-4 or -2 stage.  Without a loader
+// The whole transform: the stages of pow2_stage_radix.  Without a loader
 // the inputs are read from buf (and must be complete before the call); without a storer
 // the results are left in buf (complete when the call returns).
 template <int N, int NVEC, int T, bool HAS_LD, bool HAS_ST, int NS = 1, class Ld = NoLoad, class St = NoStore>
 OCS_D void ifft_pow2(float2 *buf, int vstride, const float2 *tw, const Ld &ld = Ld(), const St &st = St()) {
     if constexpr (NS < N) {
         constexpr int REM = N / NS;
-        constexpr int R = (REM % 8 == 0) ? 8 : REM;
+        constexpr int R = pow2_stage_radix(N, NS);
         constexpr int IT = ((N / R) * NVEC + T - 1) / T;
         constexpr bool first = HAS_LD && NS == 1;
         constexpr bool last = HAS_ST && NS * R == N;

@@ -424,7 +424,7 @@ static bool make_plan(int n, FftPlan &pl) {
 }
 
 
-// Stage-major twiddles of the power-of-two transform (radix 8, then 4 or 2): stage s with
+// Stage-major twiddles of the power-of-two transform (radices of pow2_stage_radix): stage s with
 // radix R after radices of product ns holds w^(r*j*n/(ns*R)) at [(r-1)*ns + j],
 // 1 <= r < R, 0 <= j < ns, so that the lanes of a warp (consecutive j) read consecutive
 // entries.  Total length < n.
@@ -432,7 +432,7 @@ __global__ void staged_twiddle_kernel(float2 *tw, int n) {
     int base = 0;
     for (int ns = 1; ns < n;) {
         const int rem = n / ns;
-        const int R = (rem % 8 == 0) ? 8 : rem;
+        const int R = pow2_stage_radix(n, ns);
         const int cnt = (R - 1) * ns;
         const int tstep = n / (ns * R);
         for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += gridDim.x * blockDim.x) {
