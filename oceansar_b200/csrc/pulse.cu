@@ -147,16 +147,19 @@ OCS_D void cp_async(void *dst, const void *src, int bytes) {
 OCS_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N> OCS_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// Staging of the per-facet inputs in shared memory: kStageRows rows of every input array
+// Staging of the per-facet inputs in shared memory: stage_rows rows of every input array
 // ([8] float32 fields, [4] sqrt(RCS) of type T, [2] int32 scatterer offsets, kPulseCols
-// columns each) in a ring, filled kStageRows - 1 rows ahead of use, and two slots of the
+// columns each) in a ring of stage_rows slots, and two slots of the
 // gathered scatterer-series values (complex128 of both Bragg lines), filled one row ahead.
-constexpr int kStageRows = 3;
+// Ring slots: the mixed form keeps two rows in flight while it processes one (four
+// slots); the float64 form, limited to two CTAs per SM by its registers, one (three slots,
+// measured faster there).
+template <typename T> OCS_HD constexpr int stage_rows() { return sizeof(T) == 4 ? 4 : 3; }
 template <typename T> OCS_HD constexpr size_t stage_slot_bytes() {
     return (8 * 4 + 4 * sizeof(T) + 2 * 4) * (size_t)kPulseCols;
 }
 template <typename T> OCS_HD constexpr size_t stage_bytes() {
-    return kStageRows * stage_slot_bytes<T>() + 2 * 2 * 16 * (size_t)kPulseCols + 16;
+    return stage_rows<T>() * stage_slot_bytes<T>() + 2 * 2 * 16 * (size_t)kPulseCols + 16;
 }
 
 template <typename T> struct Stage {
@@ -173,7 +176,7 @@ template <typename T> struct Stage {
                k * kPulseCols + threadIdx.x;
     }
     OCS_D double2 *gather(int g, int k) const {
-        return reinterpret_cast<double2 *>(base + kStageRows * stage_slot_bytes<T>()) + (2 * g + k) * kPulseCols +
+        return reinterpret_cast<double2 *>(base + stage_rows<T>() * stage_slot_bytes<T>()) + (2 * g + k) * kPulseCols +
                threadIdx.x;
     }
 };
@@ -383,7 +386,7 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
         const long long npix = (long long)a.nx * a.ny;
         T *scat = reinterpret_cast<T *>(a.scat);
         const bool load_scat = a.do_bragg && !a.refresh;
-        // software pipeline through shared memory: the inputs of row i + kStageRows - 1 and
+        // software pipeline through shared memory: the inputs of the next rows and
         // the scatterer-series gathers of row i + 1 are in flight while row i is processed
         const Stage<T> &st = sm.stage;
         const long long idx0 = (long long)y0 * a.nx + x;
@@ -412,36 +415,51 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
                 fidx = ridx;
             }
         };
-        for (int r = 0; r < kStageRows - 1; ++r) {
+        auto issue_row = [&](int r, int slot) {
             if (r < nrows) {
                 long long ridx, fidx;
                 row_index(r, ridx, fidx);
-                FacetIn<T>::issue(a, st, r, ridx, npix, scat, load_scat, fidx);
+                FacetIn<T>::issue(a, st, slot, ridx, npix, scat, load_scat, fidx);
             }
             cp_async_commit();
-        }
-        cp_async_wait<kStageRows - 2>();
-        if (a.do_bragg) FacetIn<T>::issue_gather(a, st, 0, 0);
-        cp_async_commit();
+        };
         FacetIn<T> cur;
-        // ring slots of rows i, i + 1 and i + kStageRows - 1
-        static_assert(kStageRows == 3, "the ring arithmetic assumes three slots");
+        if constexpr (stage_rows<T>() == 4) {
+            // Commit order: rows 0, 1; gathers of row 0; row 2; then per row i the gathers of
+            // row i + 1 and row i + 3.  Waiting for all groups but the newest at the top of
+            // row i completes rows <= i + 1 and the gathers of row i and leaves row i + 2 in
+            // flight, so two rows of inputs are on their way while a row is processed.
+            issue_row(0, 0);
+            issue_row(1, 1);
+            cp_async_wait<1>();
+            if (a.do_bragg) FacetIn<T>::issue_gather(a, st, 0, 0);
+            cp_async_commit();
+            issue_row(2, 2);
+        } else {
+            // rows 0, 1, then gathers of row 0; per row i: row i + 2, gathers of row i + 1
+            issue_row(0, 0);
+            issue_row(1, 1);
+            cp_async_wait<1>();
+            if (a.do_bragg) FacetIn<T>::issue_gather(a, st, 0, 0);
+            cp_async_commit();
+        }
         int slot_i = 0;
         for (int i = 0; i < nrows; ++i) {
             const long long idx = idx0 + (long long)i * a.nx;
-            const int slot_n = slot_i == 2 ? 0 : slot_i + 1, slot_r = slot_i == 0 ? 2 : slot_i - 1;
-            {
-                const int r = i + kStageRows - 1;
-                if (r < nrows) {
-                    long long ridx, fidx;
-                    row_index(r, ridx, fidx);
-                    FacetIn<T>::issue(a, st, slot_r, ridx, npix, scat, load_scat, fidx);
-                }
+            int slot_n;
+            if constexpr (stage_rows<T>() == 4) {
+                slot_n = (i + 1) & 3;
+                cp_async_wait<1>();             // rows <= i + 1 and the gathers of row i have landed
+                if (a.do_bragg && i + 1 < nrows) FacetIn<T>::issue_gather(a, st, slot_n, (i + 1) & 1);
+                cp_async_commit();
+                issue_row(i + 3, (i + 3) & 3);  // into the slot of row i - 1
+            } else {
+                slot_n = slot_i == 2 ? 0 : slot_i + 1;
+                issue_row(i + 2, slot_i == 0 ? 2 : slot_i - 1);
+                cp_async_wait<1>();             // rows <= i + 1 and the gathers of row i have landed
+                if (a.do_bragg && i + 1 < nrows) FacetIn<T>::issue_gather(a, st, slot_n, (i + 1) & 1);
                 cp_async_commit();
             }
-            cp_async_wait<1>();                 // rows <= i + 1 and the gathers of row i have landed
-            if (a.do_bragg && i + 1 < nrows) FacetIn<T>::issue_gather(a, st, slot_n, (i + 1) & 1);
-            cp_async_commit();
             cur.read(a, st, slot_i, load_scat);
             slot_i = slot_n;
             const double az = sm.r_az[i];
