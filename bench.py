@@ -9,8 +9,21 @@ the surface synthesis and the fused pulse kernel for all 4096 pulses, replayed f
 graph.  The working set (coefficients, scratch planes, fields, RCS, raw cube) is ~0.5 GB,
 far above the 126 MB L2, so no L2 flush is needed between steps.
 
+The default run also reports, in the same JSON line:
+* ``fp64``: the float64 drop-in form on the same scene;
+* ``parity``: the raw rows of the first pulses of both forms against the oracle (the CPU
+  restatement of the reference) run on the same seed -- relative L2 and masked maximum
+  phase error;
+* ``accumulation``: the standalone facet-to-bin accumulation kernel's roofline;
+* ``batched``: 64 scenes drawn from seed 1 (256^2..2048^2, 1-3 channels, 512-4096 pulses)
+  in one scene batch, device and end-to-end echoes/s;
+* ``serving``: Poisson request streams with continuous batching -- a stable-rate window and
+  a window of the configured 20 req/s stream -- with p50 / p99 latency;
+* ``cpu_baseline``: the oracle on all host cores over a window that amortises one Bragg
+  refresh per ocean time step.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision mixed|f64] [--small]
+                    [--precision mixed|f64] [--small] [--workload c2|c3|batched|serving]
 
 ``--impl reference`` times the CPU restatement of the reference's numba path (the oracle)
 on the host cores, on a bounded window of pulses of the same workload, and prints the same
@@ -20,6 +33,7 @@ simulates its own scene (seed + rank); value = all ranks' echoes / max-over-rank
 import argparse
 import json
 import os
+import platform
 import subprocess
 import sys
 import tempfile
@@ -32,13 +46,21 @@ sys.path.insert(0, ROOT)
 
 METRIC = "raw echoes/s (facet*pulse*chan)"
 UNIT = "echoes/s"
+SEED = 0                      # surface / scatterer seed of the scene (rank r: SEED + r)
 
 C2 = dict(name="C-band 2-channel ATI, 2048x2048 surface, 4096 pulses, 2048 bins",
           L=2048, d=1.0, wind_U=7.0, wind_dir=45.0, prf=1500.0, pulses=4096, bins=2048, num_ch=2,
-          b_ati=10.0, b_xti=0.0, ant_l=2.742, pol="vv", inc=35.0)
+          b_ati="10.0", b_xti="0", ant_l=2.742, pol="vv", inc=35.0, swell_dir_enable=False)
 C1 = dict(name="C-band 1-channel, 512x512 surface, 256 pulses, 512 bins",
           L=512, d=1.0, wind_U=10.0, wind_dir=0.0, prf=1000.0, pulses=256, bins=512, num_ch=1,
-          b_ati=0.0, b_xti=0.0, ant_l=35.7, pol="vv", inc=35.0)
+          b_ati="0.0", b_xti="0", ant_l=35.7, pol="vv", inc=35.0, swell_dir_enable=False)
+# 4096^2 facets at 0.5 m, wind sea + directional swell (250 m, Hs 0.8 m, from 120 deg),
+# four channels: along-track 0 / 5 / 10 m and a 2 m cross-track baseline on the fourth
+C3 = dict(name="C-band 4-channel ATI+XTI, 4096x4096 surface at 0.5 m with swell, 8192 pulses, 4096 bins",
+          L=2048, d=0.5, wind_U=15.0, wind_dir=30.0, prf=2000.0, pulses=8192, bins=4096, num_ch=4,
+          b_ati="[0., 5., 10., 0.]", b_xti="[0., 0., 0., 2.]", ant_l=1.7633, pol="vv", inc=35.0,
+          swell_dir_enable=True)
+SCENES = {"c1": C1, "c2": C2, "c3": C3}
 
 CFG = """[sar]
 f0=5.405e9
@@ -77,9 +99,9 @@ depth=1e5
 wind_dir={wind_dir}
 wind_U={wind_U}
 wind_fetch=500e3
-swell_dir_enable=False
+swell_dir_enable={swell_dir_enable}
 sigf=0.007
-freq_r=0.079
+freq_r=0.07901333615718642
 dir_swell_dir=120
 sigs=8
 Hs=0.8
@@ -120,8 +142,33 @@ def overrides(c):
     return dict(az_steps=c["pulses"], rg_samp=c["bins"], rg_samp_orig=c["bins"])
 
 
+def facets(c):
+    return float(round(c["L"] / c["d"])) ** 2
+
+
 def echoes(c, pulses=None):
-    return float(c["L"] / c["d"]) ** 2 * (c["pulses"] if pulses is None else pulses) * c["num_ch"]
+    return facets(c) * (c["pulses"] if pulses is None else pulses) * c["num_ch"]
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def max_phase(a, b):
+    """Maximum phase error [rad] over samples with |b| >= 1e-3 rms(b)."""
+    mask = np.abs(b) >= 1e-3 * np.sqrt(np.mean(np.abs(b) ** 2))
+    return float(np.max(np.abs(np.angle(a[mask] * np.conj(b[mask])))))
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return platform.processor() or "unknown"
 
 
 # ----------------------------------------------------------------------------------------
@@ -182,47 +229,105 @@ def dist_info():
     return world, rank, local
 
 
-def cpu_baseline(c, cfg_path, pulses, seed=0):
-    """Oracle (CPU restatement of the reference's numba path) over a bounded pulse window."""
-    from oracle.sar_raw import SarRawSim
-    sim = SarRawSim(cfg_path, overrides=overrides(c), seed=seed)
-    sim.pulse(0)                               # JIT-free warm-up (FFT plans, first refresh)
-    t0 = time.perf_counter()
-    for a in range(1, 1 + pulses):
-        sim.pulse(a)
-    dt = time.perf_counter() - t0
-    return echoes(c, pulses) / dt, dt
+class OracleLeg:
+    """The oracle (CPU restatement of the reference's numba path) on the host cores, set up
+    once for a scene: pulse 0 (the first Bragg refresh, also the warm-up) runs untimed.
+
+    ``measure`` times ``regular`` ordinary pulses and one pulse with a forced Bragg refresh
+    and amortises over one ocean time step: P = floor(ocean_dt * PRF) + 1 pulses share one
+    refresh, so seconds per pulse = (t_refresh + (P - 1) t_regular) / P."""
+
+    def __init__(self, c, cfg_path, seed=SEED, threads=None):
+        from oracle.sar_raw import SarRawSim
+        self.c = c
+        self.seed = seed
+        self.threads = threads or os.cpu_count() or 1
+        self.sim = SarRawSim(cfg_path, overrides=overrides(c), seed=seed)
+        self.sim.set_threads(self.threads)
+        self.sim.pulse(0)
+        self.next = 1
+        self.cpu_s = 0.0
+
+    def measure(self, regular):
+        sim = self.sim
+        t_reg = []
+        for _ in range(regular):
+            t0 = time.perf_counter()
+            sim.pulse(self.next % sim.az_steps)
+            t_reg.append(time.perf_counter() - t0)
+            self.next += 1
+        sim.t_last_rcs_bragg = -1.0              # force the refresh of the next pulse
+        t0 = time.perf_counter()
+        sim.pulse(self.next % sim.az_steps)
+        t_ref = time.perf_counter() - t0
+        self.next += 1
+        self.cpu_s += sum(t_reg) + t_ref
+        P = int(np.floor(sim.ocean_dt * sim.prf)) + 1
+        per_pulse = (t_ref + (P - 1) * float(np.mean(t_reg))) / P
+        return per_pulse, float(np.mean(t_reg)), t_ref, P
+
+    def raw_rows(self, n):
+        """The oracle's raw rows of pulses 0..n-1, [pol][ch][pulse][bin]."""
+        return np.stack([r[:, :n].copy() for r in (getattr(self.sim, "proc_raw_hh", None),
+                                                   getattr(self.sim, "proc_raw_vv", None)) if r is not None])
+
+    def report(self, per_pulse, t_reg, t_ref, P, regular, steps=1):
+        n = int(round(self.c["L"] / self.c["d"]))
+        return {"value": facets(self.c) * self.c["num_ch"] / per_pulse, "unit": UNIT, "cores": self.threads,
+                "kind": "port", "cpu_model": cpu_model(), "cpu_count": os.cpu_count(),
+                "seconds_per_pulse": per_pulse, "regular_pulse_s": t_reg, "refresh_pulse_s": t_ref,
+                "sample": ("per measurement %d ordinary pulses + 1 Bragg-refresh pulse of the %dx%d scene "
+                           "(seed %d), after one warm-up pulse, amortised over one refresh per %d pulses "
+                           "(ocean_dt x PRF); %d measurement(s); oracle on %d threads (row blocks, "
+                           "threaded FFT); %.1f s of timed CPU work" %
+                           (regular, n, n, self.seed, P, steps, self.threads, self.cpu_s))}
+
+    def close(self):
+        self.sim.set_threads(1)
+
+
+def cpu_baseline(c, cfg_path, regular=4, seed=SEED, threads=None):
+    """One amortised measurement of the oracle on all host cores; returns the report and
+    the oracle's raw rows of pulses 0..regular (the parity reference of the GPU arm)."""
+    leg = OracleLeg(c, cfg_path, seed=seed, threads=threads)
+    per, t_reg, t_ref, P = leg.measure(regular)
+    rows = leg.raw_rows(1 + regular)
+    rep = leg.report(per, t_reg, t_ref, P, regular)
+    leg.close()
+    return rep, rows
 
 
 def run_reference(args, c, cfg_path):
     world, rank, _ = dist_info()
     if rank != 0:
         return
-    from oracle.sar_raw import SarRawSim
-    sim = SarRawSim(cfg_path, overrides=overrides(c), seed=0)
+    leg = OracleLeg(c, cfg_path)
+    regular = 2
     steps = []
-    pulses = 2 if args.small else 3
-    a = 0
     for i in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        for _ in range(pulses):
-            sim.pulse(a % sim.az_steps)
-            a += 1
-        dt = time.perf_counter() - t0
+        m = leg.measure(regular)
         if i >= args.warmup:
-            steps.append((echoes(c, pulses) / dt, dt))
-    value = float(np.mean([v for v, _ in steps]))
+            steps.append(m)
+    per = float(np.mean([m[0] for m in steps]))
+    rep = leg.report(per, float(np.mean([m[1] for m in steps])), float(np.mean([m[2] for m in steps])),
+                     steps[0][3], regular, steps=len(steps))
+    leg.close()
+    value = rep["value"]
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": float(np.mean([d for _, d in steps]) * 1e3),
+            "warmup": args.warmup, "ms_per_step": per * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": c["name"], "sample": "%d pulses per step" % pulses},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
-                             "sample": "%d pulses of the %dx%d scene per step, after one warm-up pulse; "
-                                       "numpy FFT (single thread) + serial C accumulation" %
-                                       (pulses, c["L"], c["L"])},
+            "config": {"workload": c["name"], "step": "one amortised pulse (see cpu_baseline.sample)"},
+            "cpu_baseline": rep,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def peak_hbm():
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(peaks_path):
+        return json.load(open(peaks_path))["hbm_gbs"], "measured"
+    return 6650.0, "fallback"
 
 
 def accumulation_roofline(peak, peak_src, n=4096, nbins=2048, reps=10):
@@ -278,43 +383,125 @@ def accumulation_roofline(peak, peak_src, n=4096, nbins=2048, reps=10):
 
 # ----------------------------------------------------------------------------------------
 # Batched and serving workloads (one GPU; replicas for N > 1 as for the default workload)
-def _workload_reference(args, specs, what):
+def _workload_reference(specs, what):
     """CPU oracle on a bounded sample of the workload's scenes (2 pulses of each of the
-    first three), as echoes/s."""
-    from oceansar_b200.serving import prepare_scene  # noqa: F401  (same cfg writer)
+    first three, all host cores), as echoes/s."""
     from oracle.sar_raw import SarRawSim
     tot_e, tot_t = 0.0, 0.0
+    threads = os.cpu_count() or 1
     tmpd = tempfile.mkdtemp(prefix="ocs_ref_")
     for k, sp in enumerate(specs[:3]):
         path = os.path.join(tmpd, "s%d.cfg" % k)
         with open(path, "w") as f:
             f.write(sp["cfg"])
         sim = SarRawSim(path, overrides=sp["overrides"], seed=sp["seed"])
+        sim.set_threads(threads)
         sim.pulse(0)
         t0 = time.perf_counter()
         for a in (1, 2):
             sim.pulse(a)
         tot_t += time.perf_counter() - t0
         tot_e += 2.0 * sim.surface.Nx * sim.surface.Ny * sim.num_ch
+        sim.set_threads(1)
     v = tot_e / tot_t
-    return {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": "2 pulses of each of the first 3 scenes of the %s workload (%.1f s)" % (what, tot_t)}
+    return {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "cpu_model": cpu_model(),
+            "sample": "2 pulses of each of the first 3 scenes of the %s workload after one warm-up pulse "
+                      "(%.1f s, %d threads)" % (what, tot_t, threads)}
+
+
+def batched_report(prep, tuner, precision, n_scenes=64, seed=1):
+    """The batched workload: scenes prepared on the host, tuned, then one timed run with
+    the host inputs uploaded first and every raw cube read back last (CUDA events:
+    device time of the steps alone, and the whole upload-run-readback span)."""
+    import torch
+    from oceansar_b200.radarsim.batch import SceneBatch
+    from oceansar_b200.serving import batched_specs, scene_echoes
+    specs = batched_specs(n_scenes, seed=seed)
+    t0 = time.perf_counter()
+    gens = [f.result() for f in [prep.submit(sp, precision) for sp in specs]]
+    host_prep = time.perf_counter() - t0
+    batch = SceneBatch(max_slots=len(gens), precision=precision)
+    ins, outs = [], []
+    for g in gens:
+        batch.add(g)
+        s = g.surface
+        pairs = [(torch.from_numpy(s.wave_coefs).pin_memory(), s._coefs_d),
+                 (torch.from_numpy(s.omega).pin_memory(), s._omega_d)]
+        if g.scat_bragg_enable:
+            pairs.append((torch.from_numpy(g.rndscat_m.ind0.astype(np.int32)).pin_memory(), g.rndscat_m.device()[1]))
+            pairs.append((torch.from_numpy(g.rndscat_p.ind0.astype(np.int32)).pin_memory(), g.rndscat_p.device()[1]))
+        ins.extend(pairs)
+        outs.append((g.raw_d, torch.empty(g.raw_d.shape, dtype=g.raw_d.dtype).pin_memory()))
+    t0 = time.perf_counter()
+    rows, block = tuner.tune(batch)
+    t_tune = time.perf_counter() - t0
+    launches0 = batch.launches_per_step()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    kernel_launches = 0
+    ev[0].record()
+    for h, d in ins:
+        d.copy_(h, non_blocking=True)
+    ev[1].record()
+    steps = 0
+    while True:
+        for sl in batch.finished():
+            batch.remove(sl)
+        live = batch.live()
+        if not live:
+            break
+        k = min(block, min(batch.remaining(sl) for sl in live))
+        kernel_launches += k * batch.launches_per_step()
+        batch.graph_step(k)
+        steps += k
+    ev[2].record()
+    for d, h in outs:
+        h.copy_(d, non_blocking=True)
+    ev[3].record()
+    torch.cuda.synchronize()
+    dev_s = ev[1].elapsed_time(ev[2]) * 1e-3
+    e2e_s = ev[0].elapsed_time(ev[3]) * 1e-3
+    batch.close()
+    ech = sum(scene_echoes(g) for g in gens)
+    h2d = sum(h.numel() * h.element_size() for h, _ in ins)
+    d2h = sum(h.numel() * h.element_size() for _, h in outs)
+    del gens, ins, outs
+    torch.cuda.empty_cache()
+    return {"scenes": len(specs), "seed": seed, "echoes": ech, "device_s": dev_s, "value": ech / dev_s,
+            "unit": UNIT, "steps": steps, "pulse_block": block,
+            "tile_rows": {"%dx%d/%d" % k: v for k, v in rows.items()}, "tune_s": t_tune,
+            "host_prep_s": host_prep, "launches_per_step_first": launches0, "gpu_launches": kernel_launches,
+            "e2e": {"value": ech / e2e_s, "unit": UNIT, "h2d_bytes": int(h2d), "d2h_bytes": int(d2h),
+                    "seconds": e2e_s}}
+
+
+def serving_report(prep, tuner, precision, rate, duration, seed=2):
+    from oceansar_b200.serving import ServingLoop, serving_requests
+    specs = serving_requests(rate=rate, duration=duration, seed=seed)
+    loop = ServingLoop(precision=precision, hbm_budget=150e9, max_slots=64, pulse_block=16, preparer=prep,
+                       tuner=tuner)
+    rep = loop.run(specs)
+    keys = ("requests", "echoes", "span_s", "echoes_per_s", "offered_echoes_per_s", "latency_p50_s",
+            "latency_p99_s", "latency_max_s", "peak_reserved_bytes", "max_backlog", "gpu_busy_frac",
+            "capacity_echoes_per_s", "queue_stable")
+    out = {k: rep[k] for k in keys}
+    out.update(rate_per_s=rate, arrival_window_s=duration, seed=seed)
+    return out
 
 
 def run_workload(args):
+    """``--workload batched|serving``: that workload alone, as the line's headline."""
     import torch
     from oceansar_b200 import replicas
-    from oceansar_b200.serving import ScenePreparer, ServingLoop, batched_specs, run_batched, serving_requests
+    from oceansar_b200.serving import ScenePreparer, batched_specs, serving_requests
     from oceansar_b200.tune import Autotuner
     world, rank, local = dist_info()
     what = args.workload
-    if what == "batched":
-        specs = batched_specs(args.scenes, seed=1 + 1000 * rank)
-    else:
-        specs = serving_requests(rate=args.rate, duration=args.duration, seed=2 + 1000 * rank)
     if args.impl == "reference":
         if rank == 0:
-            cpu = _workload_reference(args, specs, what)
+            specs = (batched_specs(args.scenes, seed=1) if what == "batched" else
+                     serving_requests(rate=args.rate, duration=args.duration, seed=2))
+            cpu = _workload_reference(specs, what)
             print(json.dumps({"metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": args.gpus,
                               "steps": 1, "warmup": 0, "higher_is_better": True, "scaling": "weak",
                               "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
@@ -331,107 +518,89 @@ def run_workload(args):
     clocks = ClockSampler(local)
     tuner = Autotuner()
     try:
+        clocks.start()
         if what == "batched":
-            t0 = time.perf_counter()
-            futs = [prep.submit(sp, args.precision) for sp in specs]
-            gens = [f.result() for f in futs]
-            host_prep = time.perf_counter() - t0
-            clocks.start()
-            rep = run_batched(gens, precision=args.precision, tuner=tuner)
-            clk = clocks.stop()
-            # end to end: spectra and scatterer indices from pinned host memory, the run,
-            # every raw cube back to pinned host memory
-            e2e = _batched_e2e(gens, args.precision, tuner, rep["pulse_block"])
+            rep = batched_report(prep, tuner, args.precision, args.scenes, seed=1 + 1000 * rank)
             sec = replicas.max_over_ranks(rep["device_s"], device="cuda")
-            ms = sec * 1e3
-            value = replicas.sum_over_ranks(rep["echoes"], device="cuda") / sec
-            line_extra = {"batched": {k: rep[k] for k in ("scenes", "echoes", "steps", "pulse_block", "tile_rows",
-                                                          "tune_s", "launches_first_step")},
-                          "host_prep_s": host_prep}
-            launches = rep["kernel_launches"]
-            e2e_d = e2e
+            e2e_sec = replicas.max_over_ranks(rep["e2e"]["seconds"], device="cuda")
+            total = replicas.sum_over_ranks(rep["echoes"], device="cuda")
+            value = total / sec
+            e2e_d = {"value": total / e2e_sec, "unit": UNIT, "h2d_bytes_per_step": rep["e2e"]["h2d_bytes"],
+                     "d2h_bytes_per_step": rep["e2e"]["d2h_bytes"], "ms_per_step": e2e_sec * 1e3}
+            launches = rep["gpu_launches"]
         else:
-            clocks.start()
-            loop = ServingLoop(precision=args.precision, hbm_budget=150e9, max_slots=64, pulse_block=16,
-                               preparer=prep, tuner=tuner)
-            rep = loop.run(specs)
-            clk = clocks.stop()
+            rep = serving_report(prep, tuner, args.precision, args.rate, args.duration, seed=2 + 1000 * rank)
             sec = replicas.max_over_ranks(rep["span_s"], device="cuda")
-            ms = sec * 1e3
             value = replicas.sum_over_ranks(rep["echoes"], device="cuda") / sec
             e2e_d = {"value": value, "unit": UNIT, "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
                      "note": "arrival to raw cube in host memory for every request (wall clock)"}
-            line_extra = {"serving": {k: rep[k] for k in ("requests", "echoes", "span_s", "offered_echoes_per_s",
-                                                          "latency_p50_s", "latency_p99_s", "latency_max_s",
-                                                          "peak_reserved_bytes", "max_backlog",
-                                                          "gpu_busy_frac", "capacity_echoes_per_s",
-                                                          "queue_stable")},
-                          "rate_per_s": args.rate, "arrival_window_s": args.duration}
             launches = None
+        clk = clocks.stop()
     finally:
         prep.close()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = _workload_reference(args, specs, what)
+        specs = (batched_specs(args.scenes, seed=1) if what == "batched" else
+                 serving_requests(rate=args.rate, duration=args.duration, seed=2))
+        cpu = _workload_reference(specs, what)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": 1, "warmup": 0,
-                "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
                 "config": {"workload": what, "precision": args.precision,
                            "parallelism": "replicas" if world > 1 else "single-gpu",
                            "l2": "working set of many scenes far above L2"},
                 "clocks": clk, "e2e": e2e_d, "gpu_launches": launches, "roofline": None,
-                "cpu_baseline": cpu}
-        line.update(line_extra)
+                "cpu_baseline": cpu, what: rep}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
 
 
-def _batched_e2e(gens, precision, tuner, pulse_block):
-    """Echoes/s of the whole batch with host inputs and outputs inside the timed region."""
-    import torch
-    from oceansar_b200.radarsim.batch import SceneBatch
-    from oceansar_b200.serving import scene_echoes
-    batch = SceneBatch(max_slots=len(gens), precision=precision)
-    ins, outs = [], []
-    for g in gens:
-        cls = (g.surface.Nx, g.surface.Ny, g.npol * g.num_ch)
-        batch.add(g, tile_rows=tuner.tile_rows_for(precision, cls))
-        s = g.surface
-        pairs = [(torch.from_numpy(s.wave_coefs).pin_memory(), s._coefs_d),
-                 (torch.from_numpy(s.omega).pin_memory(), s._omega_d)]
-        if g.scat_bragg_enable:
-            pairs.append((torch.from_numpy(g.rndscat_m.ind0.astype(np.int32)).pin_memory(), g.rndscat_m.device()[1]))
-            pairs.append((torch.from_numpy(g.rndscat_p.ind0.astype(np.int32)).pin_memory(), g.rndscat_p.device()[1]))
-        ins.extend(pairs)
-        outs.append((g.raw_d, torch.empty(g.raw_d.shape, dtype=g.raw_d.dtype).pin_memory()))
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for h, d in ins:
-        d.copy_(h, non_blocking=True)
-    while True:
-        for sl in batch.finished():
-            batch.remove(sl)
-        live = batch.live()
-        if not live:
-            break
-        batch.graph_step(min(pulse_block, min(batch.remaining(sl) for sl in live)))
-    for d, h in outs:
-        h.copy_(d, non_blocking=True)
-    e1.record()
-    torch.cuda.synchronize()
-    sec = e0.elapsed_time(e1) * 1e-3
-    batch.close()
-    echoes = sum(scene_echoes(g) for g in gens)
-    h2d = sum(h.numel() * h.element_size() for h, _ in ins)
-    d2h = sum(h.numel() * h.element_size() for _, h in outs)
-    return {"value": echoes / sec, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-            "ms_per_step": sec * 1e3}
-
-
 # ----------------------------------------------------------------------------------------
+def kernel_roofline(gen, precision, peak, peak_src, ms_per_step, pulses):
+    """Per-kernel CUDA-event timing (each launch bracketed alone on its stream; 3 windows of
+    128 pulses, median) and the dominant kernel's roofline; plus a consistency check of the
+    per-kernel sum against the scene's step time."""
+    kt = gen.time_kernels(range(64, 64 + 128), repeats=3)
+    nf = float(gen.surface.Nx * gen.surface.Ny)
+    fields_pulse = 5 + (3 if gen.scat_spec_enable else 0)
+    scat_b = ((8 if precision == "f64" else 4) * 2 * gen.npol) if gen.scat_bragg_enable else 0
+    ind_b = 8 if gen.scat_bragg_enable else 0
+    nfields = len(gen.surface._raw)
+    npair = (nfields + 1) // 2
+    # algorithmic bytes per launch: row pass reads c and omega and writes the packed row
+    # transforms (one complex64 plane per field pair); column pass reads those planes and
+    # writes the float32 fields; pulse kernel reads the fields it uses, sqrt(RCS) (m, p per
+    # polarisation) and the two Bragg index maps.
+    alg = {"surface_rows": nf * (8 + 4 + 8 * npair),
+           "surface_cols": nf * (8 * npair + 4 * nfields),
+           "pulse": nf * (4 * fields_pulse + scat_b + ind_b)}
+    kern = {}
+    for k, b in alg.items():
+        ms = kt[k]
+        gbs = b / (ms * 1e-3) / 1e9
+        kern[k] = {"ms": round(ms, 5), "GBps": round(gbs, 1), "frac": round(gbs / peak, 4), "alg_bytes": b,
+                   "ms_spread": [round(v, 5) for v in kt["windows"][k]]}
+    dom = max(kern, key=lambda k: kern[k]["ms"])
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(precision, {}).get(dom)
+        except (ValueError, OSError):
+            traffic = None
+    ksum = sum(kt[k] for k in alg) * pulses
+    ratio = ksum / ms_per_step
+    return {"bound": "hbm", "achieved": kern[dom]["GBps"], "peak": peak, "unit": "GB/s",
+            "frac": kern[dom]["frac"], "traffic": traffic, "kernel": dom, "peak_source": peak_src,
+            "per_kernel": kern,
+            # the scene graph overlaps the next pulse's surface with this pulse's kernels,
+            # so the per-kernel sum may exceed the step time somewhat, never fall below it
+            "consistency": {"kernel_sum_ms_per_step": round(ksum, 3), "step_ms": round(ms_per_step, 3),
+                            "ratio": round(ratio, 3), "ok": bool(0.95 <= ratio <= 1.6)}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -442,9 +611,12 @@ def main():
     ap.add_argument("--small", action="store_true", help="512^2 single-channel case (quick check)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=["c2", "batched", "serving"],
-                    help="c2: the two-channel 2048^2 scene (default); batched: many scenes in one "
-                         "scene batch; serving: a Poisson request stream with continuous batching")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched / serving / accumulation objects of the default line")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "batched", "serving"],
+                    help="c2: the two-channel 2048^2 scene (default); c3: the four-channel 4096^2 "
+                         "stress scene; batched: many scenes in one scene batch; serving: a Poisson "
+                         "request stream with continuous batching")
     ap.add_argument("--scenes", type=int, default=64, help="batched: number of scenes")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: requests per second")
     ap.add_argument("--duration", type=float, default=5.0, help="serving: seconds of arrivals")
@@ -454,18 +626,15 @@ def main():
     ap.add_argument("--profile-pulses", type=int, default=0,
                     help="run this many pulses with plain launches (for ncu) and exit")
     args = ap.parse_args()
-    if args.workload != "c2":
+    if args.workload in ("batched", "serving"):
         run_workload(args)
         return
     if args.accumulation_only:
         import torch
         torch.cuda.set_device(dist_info()[2])
-        peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-        peak, src = ((json.load(open(peaks_path))["hbm_gbs"], "measured") if os.path.exists(peaks_path)
-                     else (6650.0, "fallback"))
-        print(json.dumps({"accumulation": accumulation_roofline(peak, src)}), flush=True)
+        print(json.dumps({"accumulation": accumulation_roofline(*peak_hbm())}), flush=True)
         return
-    c = C1 if args.small else C2
+    c = C1 if args.small else SCENES[args.workload]
     tmpd = tempfile.mkdtemp(prefix="ocs_bench_")
     cfg_path = write_cfg(c, os.path.join(tmpd, "scene.cfg"))
     if args.impl == "reference":
@@ -481,6 +650,12 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", init_method="env://",
                                 timeout=__import__("datetime").timedelta(seconds=120))
+    # host set-up workers for the batched / serving objects, spawned before the GPU work
+    extras = not (args.no_extras or args.small or world > 1 or args.workload != "c2")
+    prep = None
+    if extras:
+        from oceansar_b200.serving import ScenePreparer
+        prep = ScenePreparer(workers=args.workers)
 
     def barrier():
         if world > 1:
@@ -506,9 +681,16 @@ def main():
         barrier()
         return max_over_ranks(e0.elapsed_time(e1) / steps)
 
-    # ---- main arm ---------------------------------------------------------------------
-    gen = RawGenerator(cfg_path, precision=args.precision, overrides=overrides(c),
-                       seed=replicas.replica_seed(1000, rank))
+    # ---- CPU oracle on the same seed (before the GPU arm: its raw rows are the parity
+    # reference; the threads end before any GPU work) ----------------------------------
+    cpu, ref_rows = None, None
+    nparity = 2 if args.small else 4
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu, ref_rows = cpu_baseline(c, cfg_path, regular=nparity)
+
+    # ---- main arm -----------------------------------------------------------------------
+    seed = replicas.replica_seed(SEED, rank)
+    gen = RawGenerator(cfg_path, precision=args.precision, overrides=overrides(c), seed=seed)
     if args.profile_pulses:
         gen.run(range(args.profile_pulses))
         torch.cuda.synchronize()
@@ -521,49 +703,13 @@ def main():
     clk = clocks.stop()
     value = echoes(c) * world / (ms * 1e-3)
     launches = gen.kernel_launches_per_scene() * args.steps
+    parity = {}
+    if ref_rows is not None:
+        got = gen.raw()[:, :, :ref_rows.shape[2]]
+        parity[args.precision] = {"rel_l2": rel_l2(got, ref_rows), "max_phase_rad": max_phase(got, ref_rows)}
 
-    # ---- per-kernel timing and roofline (dominant kernel) -----------------------------
-    # Each kernel is bracketed alone by CUDA events on its launching stream, 64 pulses.
-    npl = 64
-    kt = gen.time_kernels(range(64, 64 + npl))
-    nf = float(gen.surface.Nx * gen.surface.Ny)
-    fields_pulse = 5 + (3 if gen.scat_spec_enable else 0)
-    scat_b = ((8 if args.precision == "f64" else 4) * 2 * gen.npol) if gen.scat_bragg_enable else 0
-    ind_b = 8 if gen.scat_bragg_enable else 0
-    nfields = len(gen.surface._raw)
-    npair = (nfields + 1) // 2
-    # algorithmic bytes per launch: row pass reads c and omega and writes the packed row
-    # transforms (one complex64 plane per field pair); column pass reads those planes and
-    # writes the float32 fields; pulse kernel reads the fields it uses, sqrt(RCS) (m, p per
-    # polarisation) and the two Bragg index maps.
-    surf_rows_bytes = nf * (8 + 4 + 8 * npair)
-    surf_cols_bytes = nf * (8 * npair + 4 * nfields)
-    pulse_bytes = nf * (4 * fields_pulse + scat_b + ind_b)
-    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(peaks_path):
-        peak = json.load(open(peaks_path))["hbm_gbs"]
-        peak_src = "measured"
-    else:
-        peak, peak_src = 6650.0, "fallback"
-    kern = {"surface_rows": {"ms": kt["surface_rows"], "bytes": surf_rows_bytes},
-            "surface_cols": {"ms": kt["surface_cols"], "bytes": surf_cols_bytes},
-            "pulse": {"ms": kt["pulse"], "bytes": pulse_bytes}}
-    for k in kern.values():
-        k["GBps"] = k["bytes"] / (k["ms"] * 1e-3) / 1e9
-        k["frac"] = k["GBps"] / peak
-    dom = max(kern, key=lambda k: kern[k]["ms"])
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        try:
-            traffic = json.load(open(tpath)).get(args.precision, {}).get(dom)
-        except (ValueError, OSError):
-            traffic = None
-    roofline = {"bound": "hbm", "achieved": kern[dom]["GBps"], "peak": peak, "unit": "GB/s",
-                "frac": kern[dom]["frac"], "traffic": traffic, "kernel": dom, "peak_source": peak_src,
-                "per_kernel": {k: {"ms": round(v["ms"], 5), "GBps": round(v["GBps"], 1),
-                                   "frac": round(v["frac"], 4), "alg_bytes": v["bytes"]}
-                               for k, v in kern.items()}}
+    peak, peak_src = peak_hbm()
+    roofline = kernel_roofline(gen, args.precision, peak, peak_src, ms, c["pulses"])
 
     # ---- end to end through the public API with host buffers ---------------------------
     s = gen.surface
@@ -606,40 +752,48 @@ def main():
     if not args.no_fp64 and args.precision == "mixed":
         del gen
         torch.cuda.empty_cache()
-        g64 = RawGenerator(cfg_path, precision="f64", overrides=overrides(c),
-                           seed=replicas.replica_seed(1000, rank))
+        g64 = RawGenerator(cfg_path, precision="f64", overrides=overrides(c), seed=seed)
         g64.capture()
         ms64 = timed(g64, 1, 1)
-        fp64 = {"value": echoes(c) * world / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64}
+        fp64 = {"value": echoes(c) * world / (ms64 * 1e-3), "unit": UNIT, "ms_per_step": ms64,
+                "mixed_over_f64": ms64 / ms}
+        if ref_rows is not None:
+            got = g64.raw()[:, :, :ref_rows.shape[2]]
+            parity["f64"] = {"rel_l2": rel_l2(got, ref_rows), "max_phase_rad": max_phase(got, ref_rows)}
         del g64
         torch.cuda.empty_cache()
+    if parity:
+        parity.update(pulses=list(range(ref_rows.shape[2])), reference="oracle (CPU restatement of the "
+                      "reference), same seed; end to end: both sides synthesise their own float32 surface",
+                      bars={"mixed": {"rel_l2": 1e-4, "max_phase_rad": 1e-3}, "f64": {"rel_l2": 1e-4}})
 
-    # ---- standalone accumulation (chan_profile drop-in, [ny][nx] layout) -------------------
-    accum = None
-    if not args.small:
+    # ---- standalone accumulation, batched and serving workloads -----------------------------
+    accum = batched = serving = None
+    if extras:
+        from oceansar_b200.tune import Autotuner
         accum = accumulation_roofline(peak, peak_src)
-
-    # ---- CPU baseline (oracle port) -------------------------------------------------------
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        pulses = 2 if args.small else 3
-        v, dt = cpu_baseline(c, cfg_path, pulses)
-        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": "%d pulses of the %dx%d scene (%.1f s), after one warm-up pulse; numpy FFT "
-                         "(single thread) + serial C accumulation" % (pulses, c["L"], c["L"], dt)}
+        tuner = Autotuner()
+        try:
+            batched = batched_report(prep, tuner, args.precision)
+            serving = {"stable": serving_report(prep, tuner, args.precision, rate=2.0, duration=10.0),
+                       "configured": serving_report(prep, tuner, args.precision, rate=20.0, duration=2.0)}
+        finally:
+            prep.close()
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f64",
                 "data": "synthetic",
-                "config": {"workload": c["name"], "grid": [c["L"], c["L"]], "pulses": c["pulses"],
-                           "channels": c["num_ch"], "range_bins": c["bins"], "precision": args.precision,
+                "config": {"workload": c["name"], "grid": [int(round(c["L"] / c["d"]))] * 2,
+                           "pulses": c["pulses"], "channels": c["num_ch"], "range_bins": c["bins"],
+                           "precision": args.precision, "seed": seed,
                            "parallelism": "replicas" if world > 1 else "single-gpu",
                            "l2": "inputs larger than L2 (~0.5 GB working set)",
                            "graph": "whole scene replayed from one CUDA graph"},
                 "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
-                "cpu_baseline": cpu, "fp64": fp64, "accumulation": accum}
+                "cpu_baseline": cpu, "parity": parity or None, "fp64": fp64, "accumulation": accum,
+                "batched": batched, "serving": serving}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()

@@ -159,10 +159,12 @@ int ocs_surface_blend(int64_t n, int32_t nfields, const float *const *a_d, const
 /* ocs_surface_update for callers that cannot allocate device memory (no counterpart in the
  * reference).  desc->workspace_d is ignored: the workspace is a 32 MiB device array
  * compiled into the library, so ocs_surface_workspace_bytes(nx, ny, nfields) must be at
- * most 32 MiB (else OCS_ERR_SIZE).  The first call on a device resolves that array's
- * address (make it before any stream capture); all calls on a device share the array, so
- * calls that overlap on the GPU race and must be serialised by the caller.  Allocates
- * nothing. */
+ * most 32 MiB (else OCS_ERR_SIZE).  The descriptor is checked before anything is
+ * launched.  Every call resolves the array's address on the current device; with lazy
+ * module loading the first call on a device also loads the module, so make one warm-up
+ * call before any latency-critical loop or stream capture.  All calls on a device share
+ * the array, so calls that overlap on the GPU race and must be serialised by the caller.
+ * Allocates nothing. */
 int ocs_surface_update_noalloc(const ocs_surface_desc *desc, float t, void *stream);
 
 /* ------------------------------------------------------------------------------------

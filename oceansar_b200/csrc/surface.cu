@@ -835,9 +835,13 @@ extern "C" int ocs_surface_choppy(const ocs_choppy_desc *d, void *stream) {
 //   nx, ny, nfields) must not exceed it (for example 1024 x 1024 with up to 6 fields or
 //   512 x 512 with up to 24); larger requests return OCS_ERR_SIZE.  The array is part of
 //   the loaded module, so every GPU that loads the library holds it until exit.
-// * Set-up: the first call on a device, with that device current, resolves the array's
-//   device address (cudaGetSymbolAddress) and caches it; make that first call before any
-//   stream capture.
+// * Set-up: every call resolves the array's device address on the current device
+//   (cudaGetSymbolAddress; cheap once the module is loaded, and never stale after a
+//   context reset).  With lazy module loading the first call on a device also loads the
+//   module and its 32 MiB array, so make one warm-up call before any latency-critical
+//   loop or stream capture.
+// * Errors: the descriptor is checked completely before anything is launched, so a bad
+//   descriptor returns OCS_ERR_ARG / OCS_ERR_SIZE with the array untouched.
 // * Sharing: every call on a device uses the same array, which keeps the last call's
 //   contents.  Each call rewrites the twiddle tables and overwrites the scratch planes
 //   completely before reading them, so nothing needs clearing, but calls that overlap on
@@ -847,30 +851,20 @@ extern "C" int ocs_surface_choppy(const ocs_choppy_desc *d, void *stream) {
 constexpr size_t kNoAllocScratchBytes = 32u << 20;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-static std::mutex g_noalloc_mu;
-static void *g_noalloc_ptr[64] = {nullptr};
-
 extern "C" int ocs_surface_update_noalloc(const ocs_surface_desc *d, float t, void *stream) {
     if (!d) return OCS_ERR_ARG;
     const int64_t need = ocs_surface_workspace_bytes(d->nx, d->ny, d->nfields);
     if (need < 0) return OCS_ERR_ARG;
     if ((size_t)need > kNoAllocScratchBytes) return OCS_ERR_SIZE;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return OCS_ERR_CUDA;
     void *ws = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {
-            void *p = nullptr;
-            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return OCS_ERR_CUDA;
-            g_noalloc_ptr[dev] = p;
-        }
-        ws = g_noalloc_ptr[dev];
-    }
-    int st = ocs_surface_prepare(d->nx, d->ny, ws, stream);
-    if (st != OCS_OK) return st;
+    if (cudaGetSymbolAddress(&ws, g_noalloc_scratch) != cudaSuccess || !ws) return OCS_ERR_CUDA;
     ocs_surface_desc local = *d;
     local.workspace_d = ws;
+    SurfaceArgs check;                     // full argument check before the array is touched
+    const int fst = fill_surface_args(&local, t, check);
+    if (fst != OCS_OK) return fst;
+    const int st = ocs_surface_prepare(d->nx, d->ny, ws, stream);
+    if (st != OCS_OK) return st;
     return ocs_surface_update(&local, t, stream);
 }
 

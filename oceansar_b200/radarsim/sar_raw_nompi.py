@@ -495,28 +495,38 @@ class RawGenerator(object):
         t = self.time_kernels(steps)
         return t['surface_rows'] + t['surface_cols'], t['pulse'], None, None
 
-    def time_kernels(self, steps):
+    def time_kernels(self, steps, repeats=1):
         """Average device time [ms] per pulse of each kernel of the scene loop over ``steps``
         pulses: 'surface_rows' (row pass), 'surface_cols' (column pass) and 'pulse' (the
         per-pulse row table and the fused NRCS / scene / accumulation kernel(s)), each from
-        CUDA events recorded on the launching stream around that launch alone."""
+        CUDA events recorded on the launching stream around that launch alone.  The window
+        runs ``repeats`` times (same pulses, same Bragg refresh decisions); the result is the
+        median of the windows' averages, and 'windows' holds every window's average."""
         st = torch.cuda.current_stream()
         mk = lambda: torch.cuda.Event(enable_timing=True)  # noqa: E731
-        ev = [[mk() for _ in range(4)] for _ in steps]
-        saved_last = self.t_last_rcs_bragg
-        for e, a in zip(ev, steps):
-            t_now = a * self.t_step
-            e[0].record(st)
-            self.surface.set_t(t_now, passes=1)
-            e[1].record(st)
-            self.surface.set_t(t_now, passes=2)
-            e[2].record(st)
-            self.pulse(a, update_surface=False)
-            e[3].record(st)
-        torch.cuda.synchronize()
-        self.t_last_rcs_bragg = saved_last
+        steps = list(steps)
         names = ('surface_rows', 'surface_cols', 'pulse')
-        return {n: float(np.mean([e[i].elapsed_time(e[i + 1]) for e in ev])) for i, n in enumerate(names)}
+        saved_last = self.t_last_rcs_bragg
+        wins = {n: [] for n in names}
+        for _ in range(max(1, int(repeats))):
+            self.t_last_rcs_bragg = saved_last
+            ev = [[mk() for _ in range(4)] for _ in steps]
+            for e, a in zip(ev, steps):
+                t_now = a * self.t_step
+                e[0].record(st)
+                self.surface.set_t(t_now, passes=1)
+                e[1].record(st)
+                self.surface.set_t(t_now, passes=2)
+                e[2].record(st)
+                self.pulse(a, update_surface=False)
+                e[3].record(st)
+            torch.cuda.synchronize()
+            for i, n in enumerate(names):
+                wins[n].append(float(np.mean([e[i].elapsed_time(e[i + 1]) for e in ev])))
+        self.t_last_rcs_bragg = saved_last
+        out = {n: float(np.median(wins[n])) for n in names}
+        out['windows'] = wins
+        return out
 
     # ------------------------------------------------------------------------------------
     def nrcs_avg(self):

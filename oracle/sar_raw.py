@@ -154,6 +154,23 @@ class SarRawSim:
             self.balancer = OceanSurfaceBalancer(s, surface_dt)
 
     # ------------------------------------------------------------------------------
+    def set_threads(self, threads):
+        """Run the per-facet work of each pulse on ``threads`` host threads (row blocks in a
+        thread pool; numpy and the C accumulator release the GIL) and the surface FFTs with
+        ``threads`` workers.  Only the CPU baseline uses more than one thread: with one
+        thread (the default) every operation is the whole-array operation of the reference,
+        bit for bit; with several, the NRCS sums and the range profiles are summed block by
+        block (rounding order differs)."""
+        import concurrent.futures
+        import functools
+        self.threads = max(1, int(threads))
+        self._pool = (concurrent.futures.ThreadPoolExecutor(self.threads) if self.threads > 1 else None)
+        if self.threads > 1:
+            import scipy.fft
+            self.surface.fft_ifft2 = functools.partial(scipy.fft.ifft2, workers=self.threads)
+        else:
+            self.surface.fft_ifft2 = None
+
     def pulse(self, az_step, record=None):
         """One iteration of ``sar_raw_nompi.py:349-535``."""
         s = self.surface
@@ -167,16 +184,71 @@ class SarRawSim:
             s.set_t(t_now)
         sin_az = az / self.sr0
         az_proj_angle = np.arcsin(az / self.gr0)
-        sr_surface = (self.sr - self.cos_inc * s.Dz + az / 2 * sin_az
-                      + s.Dx * self.sin_inc + s.Dy * sin_az)
-        wave_dinc = (s.Dz * self.sin_inc + s.Dx * self.sin_inc) / self.sr0
+        refresh = self.scat_bragg_enable and (t_now - self.t_last_rcs_bragg) > self.ocean_dt
+        if refresh:
+            self.t_last_rcs_bragg = t_now
+            if record is not None:
+                record['rcs_refresh'] = True
+        if self.scat_bragg_enable:
+            scats = (self.rndscat_m.scats(t_now), self.rndscat_p.scats(t_now))
+        else:
+            scats = None
+        threads = getattr(self, 'threads', 1)
+        ny = s.Ny
+        kirchhoff = self.scat_spec_enable and self.scat_spec_mode != 'kodis'   # needs whole rows of x, y
+        if threads == 1 or record is not None or kirchhoff:
+            blocks = [(0, ny)]
+        else:
+            nb = 4 * threads
+            edges = [ny * i // nb for i in range(nb + 1)]
+            blocks = [(edges[i], edges[i + 1]) for i in range(nb) if edges[i + 1] > edges[i]]
+        if refresh and len(blocks) > 1:
+            shape = (2, s.Ny, s.Nx)
+            if self.do_hh:
+                self.RCS_bragg_hh = np.empty(shape)
+            if self.do_vv:
+                self.RCS_bragg_vv = np.empty(shape)
+        args = (s, az_step, t_now, az, sin_az, az_proj_angle, refresh, scats, record, len(blocks) == 1)
+        if len(blocks) == 1:
+            parts = [self._pulse_rows(0, ny, *args)]
+        else:
+            parts = list(self._pool.map(lambda blk: self._pulse_rows(blk[0], blk[1], *args), blocks))
+        spec = [p[0] for p in parts]
+        if self.scat_spec_enable:
+            self.NRCS_avg_hh[az_step] += (spec[0] if len(spec) == 1 else sum(spec)) / self.surface_area
+            self.NRCS_avg_vv[az_step] += self.NRCS_avg_hh[az_step]
+        if self.scat_bragg_enable:
+            for k, (do, attr) in enumerate(((self.do_hh, 'NRCS_avg_hh'), (self.do_vv, 'NRCS_avg_vv'))):
+                if do:
+                    rs = [p[1][k] for p in parts]
+                    getattr(self, attr)[az_step] += (rs[0] if len(rs) == 1 else sum(rs)) / self.surface_area
+        if len(parts) > 1:
+            for key in parts[0][2]:
+                pol, ch = key
+                raw = self.proc_raw_hh if pol == 'hh' else self.proc_raw_vv
+                for p in parts:
+                    raw[ch][az_step] += p[2][key]
+
+    def _pulse_rows(self, r0, r1, s, az_step, t_now, az, sin_az, az_proj_angle, refresh, scats, record, whole):
+        """The per-facet part of a pulse for facet rows r0:r1.  ``whole``: the block is the
+        whole surface (whole-array operations, profiles accumulated in place)."""
+        rows = slice(r0, r1)
+        az, sin_az, az_proj_angle = az[rows], sin_az[rows], az_proj_angle[rows]
+        Dx, Dy, Dz = s.Dx[rows], s.Dy[rows], s.Dz[rows]
+        Diffx, Diffy = s.Diffx[rows], s.Diffy[rows]
+        ny = r1 - r0
+        sr_surface = (self.sr - self.cos_inc * Dz + az / 2 * sin_az
+                      + Dx * self.sin_inc + Dy * sin_az)
+        wave_dinc = (Dz * self.sin_inc + Dx * self.sin_inc) / self.sr0
         if self.do_hh:
-            scene_hh = np.zeros([s.Ny, s.Nx], dtype=complex)
+            scene_hh = np.zeros([ny, s.Nx], dtype=complex)
         if self.do_vv:
-            scene_vv = np.zeros([s.Ny, s.Nx], dtype=complex)
+            scene_vv = np.zeros([ny, s.Nx], dtype=complex)
+        spec_sum = 0.
         if self.scat_spec_enable and self.scat_spec_mode == 'kodis':
-            Esn_sp = np.sqrt(4. * np.pi) * self.rcs_spec.field(az_proj_angle, sr_surface, s.Diffx,
-                                                                s.Diffy, s.Diffxx, s.Diffyy, s.Diffxy)
+            Esn_sp = np.sqrt(4. * np.pi) * self.rcs_spec.field(az_proj_angle, sr_surface, Diffx,
+                                                                Diffy, s.Diffxx[rows], s.Diffyy[rows],
+                                                                s.Diffxy[rows])
             if self.do_hh:
                 scene_hh += Esn_sp
             if self.do_vv:
@@ -189,51 +261,66 @@ class SarRawSim:
                     continue
                 Esn_sp = (np.exp(-1j * (2. * self.k0 * sr_surface)) * (4. * np.pi) ** 1.5 *
                           self.rcs_spec.field(1, 1, pol_tmp[0], pol_tmp[1], self.inc, self.inc, az_proj_angle,
-                                              az_proj_angle + np.pi, s.Dz, s.Diffx, s.Diffy, s.Diffxx, s.Diffyy,
-                                              s.Diffxy))
+                                              az_proj_angle + np.pi, Dz, Diffx, Diffy, s.Diffxx[rows],
+                                              s.Diffyy[rows], s.Diffxy[rows]))
                 if pol_tmp == 'hh':
                     scene_hh += Esn_sp
                 else:
                     scene_vv += Esn_sp
         if self.scat_spec_enable:
-            self.NRCS_avg_hh[az_step] += (np.sum(np.abs(Esn_sp) ** 2) / self.surface_area)
-            self.NRCS_avg_vv[az_step] += self.NRCS_avg_hh[az_step]
+            spec_sum = np.sum(np.abs(Esn_sp) ** 2)
+        bragg_sums = [0., 0.]
         if self.scat_bragg_enable:
-            if (t_now - self.t_last_rcs_bragg) > self.ocean_dt:
-                r = self.rcs_bragg.rcs(az_proj_angle, s.Diffx, s.Diffy)
+            if refresh:
+                r = self.rcs_bragg.rcs(az_proj_angle, Diffx, Diffy)
                 if self.pol == 'DP':
-                    self.RCS_bragg_hh, self.RCS_bragg_vv = r
+                    r_hh, r_vv = r
                 elif self.pol == 'hh':
-                    self.RCS_bragg_hh = r
+                    r_hh, r_vv = r, None
                 else:
-                    self.RCS_bragg_vv = r
+                    r_hh, r_vv = None, r
                 if self.use_hmtf:
-                    s.hMTF[np.where(s.hMTF < -1)] = -1
+                    hm = s.hMTF[rows]
+                    hm[np.where(hm < -1)] = -1
                     if self.do_hh:
-                        self.RCS_bragg_hh[0] *= (1 + s.hMTF)
-                        self.RCS_bragg_hh[1] *= (1 + s.hMTF)
+                        r_hh[0] *= (1 + hm)
+                        r_hh[1] *= (1 + hm)
                     if self.do_vv:
-                        self.RCS_bragg_vv[0] *= (1 + s.hMTF)
-                        self.RCS_bragg_vv[1] *= (1 + s.hMTF)
-                self.t_last_rcs_bragg = t_now
-                if record is not None:
-                    record['rcs_refresh'] = True
+                        r_vv[0] *= (1 + hm)
+                        r_vv[1] *= (1 + hm)
+                if whole:
+                    if self.do_hh:
+                        self.RCS_bragg_hh = r_hh
+                    if self.do_vv:
+                        self.RCS_bragg_vv = r_vv
+                else:
+                    if self.do_hh:
+                        self.RCS_bragg_hh[:, rows] = r_hh
+                    if self.do_vv:
+                        self.RCS_bragg_vv[:, rows] = r_vv
             if self.do_hh:
-                scat_bragg_hh = np.sqrt(self.RCS_bragg_hh)
-                self.NRCS_avg_hh[az_step] += np.sum(self.RCS_bragg_hh) / self.surface_area
+                rcs = self.RCS_bragg_hh if whole else self.RCS_bragg_hh[:, rows]
+                scat_bragg_hh = np.sqrt(rcs)
+                bragg_sums[0] = np.sum(rcs)
             if self.do_vv:
-                scat_bragg_vv = np.sqrt(self.RCS_bragg_vv)
-                self.NRCS_avg_vv[az_step] += np.sum(self.RCS_bragg_vv) / self.surface_area
+                rcs = self.RCS_bragg_vv if whole else self.RCS_bragg_vv[:, rows]
+                scat_bragg_vv = np.sqrt(rcs)
+                bragg_sums[1] = np.sum(rcs)
             surf_phase = - (2 * self.k0) * sr_surface
             cap_phase = (2 * self.k0) * self.t_step * self.c_b * (az_step + 1)
-            self.phase_bragg[0] = surf_phase - cap_phase
-            self.phase_bragg[1] = surf_phase + cap_phase
-            self.bragg_scats[0] = self.rndscat_m.scats(t_now)
-            self.bragg_scats[1] = self.rndscat_p.scats(t_now)
+            if whole:
+                phase_bragg, bragg_scats = self.phase_bragg, self.bragg_scats
+            else:
+                phase_bragg = np.zeros([2, ny, s.Nx])
+                bragg_scats = np.zeros([2, ny, s.Nx], dtype=complex)
+            phase_bragg[0] = surf_phase - cap_phase
+            phase_bragg[1] = surf_phase + cap_phase
+            bragg_scats[0] = scats[0][rows]
+            bragg_scats[1] = scats[1][rows]
             if self.do_hh:
-                scene_hh += np.sum(scat_bragg_hh * np.exp(1j * self.phase_bragg) * self.bragg_scats, axis=0)
+                scene_hh += np.sum(scat_bragg_hh * np.exp(1j * phase_bragg) * bragg_scats, axis=0)
             if self.do_vv:
-                scene_vv += np.sum(scat_bragg_vv * np.exp(1j * self.phase_bragg) * self.bragg_scats, axis=0)
+                scene_vv += np.sum(scat_bragg_vv * np.exp(1j * phase_bragg) * bragg_scats, axis=0)
         beam_pattern = (sinc_bp(sin_az, self.ant_l_tx, self.f0, field=True) *
                         sinc_bp(sin_az, self.ant_l_rx, self.f0, field=True))
         if record is not None:
@@ -242,20 +329,24 @@ class SarRawSim:
                 record['scene_vv'] = scene_vv.copy()
             if self.do_hh:
                 record['scene_hh'] = scene_hh.copy()
+        profiles = {}
         for ch in np.arange(self.num_ch, dtype=int):
             tot_dinc = (self.inc - self.inc_angle) + wave_dinc
-            for do, scene, raw in ((self.do_hh, scene_hh if self.do_hh else None,
-                                    self.proc_raw_hh if self.do_hh else None),
-                                   (self.do_vv, scene_vv if self.do_vv else None,
-                                    self.proc_raw_vv if self.do_vv else None)):
+            for do, pol, scene, raw in ((self.do_hh, 'hh', scene_hh if self.do_hh else None,
+                                         self.proc_raw_hh if self.do_hh else None),
+                                        (self.do_vv, 'vv', scene_vv if self.do_vv else None,
+                                         self.proc_raw_vv if self.do_vv else None)):
                 if not do:
                     continue
                 scene_bp = scene * beam_pattern
                 scene_bp *= np.exp(-1j * self.k0 * self.b_ati[ch] * sin_az)
                 scene_bp *= np.exp(-1j * self.k0 * self.b_xti[ch] * tot_dinc)
+                out = raw[ch][az_step] if whole else np.zeros(self.rg_samp, dtype=complex)
                 rp.chan_profile(sr_surface.flatten(), scene_bp.flatten(), self.sr_res / self.over_fs,
-                                self.min_sr, self.chan_sinc_vec, self.n_sinc_samples, self.sinc_ovs,
-                                raw[ch][az_step])
+                                self.min_sr, self.chan_sinc_vec, self.n_sinc_samples, self.sinc_ovs, out)
+                if not whole:
+                    profiles[(pol, int(ch))] = out
+        return spec_sum, bragg_sums, profiles
 
     def run(self, steps=None, record_steps=()):
         recs = {}

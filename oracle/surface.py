@@ -151,7 +151,8 @@ class OceanSurface:
         kx, ky, kxn, kyn, kinv, om = self.kx, self.ky, self.kxn, self.kyn, self.kinv, self.omega
         if precision != 'f32':
             kx, ky, kxn, kyn, kinv, om = (a.astype(np.float64) for a in (kx, ky, kxn, kyn, kinv, om))
-        ifft2 = np.fft.ifft2
+        # numpy's transform (as the reference); a threaded one only for the CPU baseline
+        ifft2 = getattr(self, 'fft_ifft2', None) or np.fft.ifft2
         cur = self.current if precision == 'f32' else self.current.astype(np.float64)
         tt = t if precision == 'f32' else np.float64(t)
         if self.swell_enable:

@@ -27,12 +27,14 @@ replaces one of them without touching the reference sources:
    root's float32 buffer into the receive buffer (with one process the whole surface is
    the root's share); ``Reduce`` copies (the sum over one process).
 """
+import os
 import sys
 import types
 
 import numpy as np
 
-REF_ROOT = "/root/reference"
+# where the reference source tree is checked out (read-only); set OCEANSAR_REF_ROOT
+REF_ROOT = os.environ.get("OCEANSAR_REF_ROOT", "/root/reference")
 
 NC_STORE = {}
 

@@ -64,13 +64,15 @@ def test_golden_surfaces(name):
     (1024, ['D', 'Diff'], False),
     (256, ['D', 'Diff', 'Diff2', 'V', 'A'], True),
     (96, ['D', 'Diff', 'Diff2'], False),
+    (4096, ['D', 'Diff', 'Diff2'], False),
+    (2400, ['D', 'Diff', 'Diff2'], False),
 ])
 def test_against_oracle(n, compute, choppy):
     from oceansar_b200.surfaces import OceanSurface
     kw = dict(Lx=float(n), Ly=float(n), dx=1., dy=1., cutoff_wl='auto', spec_model='elfouhaily',
               spread_model='elfouhaily', wind_dir=0.3, wind_fetch=500e3, wind_U=10.,
               current_mag=0.2, current_dir=1.0, compute=compute, opt_res=True,
-              fft_max_prime=2 if n != 96 else 3, choppy_enable=choppy, depth=None)
+              fft_max_prime={96: 3, 2400: 5}.get(n, 2), choppy_enable=choppy, depth=None)
     np.random.seed(7)
     o = OracleSurface().init(**kw)
     np.random.seed(7)
@@ -78,6 +80,7 @@ def test_against_oracle(n, compute, choppy):
     s.init(**kw)
     s.wave_coefs = o.wave_coefs
     s._upload()
+    assert (s.Nx, s.Ny) == (n, n)
     for t in (0.0, 2.37):
         ref = o.set_t(t)
         s.t = t
