@@ -78,6 +78,11 @@ int ocs_chan_profile_2d_c64(const double *srg_d, const float *scene_d, int64_t n
                             int n_sinc_samples, int sinc_ovs, float *output_d, int64_t nbins,
                             void *stream);
 
+/* OCS_ERR_TIMEOUT if a bounded device-side wait of the bulk-staged 2-D accumulation gave up
+ * since the last call (the flag is then cleared), else OCS_OK.  Synchronises with the
+ * device. */
+int ocs_chan_profile_status(void);
+
 
 /* ------------------------------------------------------------------------------------
  * Per-pulse surface synthesis.
@@ -271,14 +276,52 @@ typedef struct {
      * nch = 1; Kodis or Kirchhoff specular; direct or LUT Bragg model.  The scene batch
      * rejects it. */
     int32_t skim, skim_ny_integ, skim_az2, skim_rcm;
+    /* Mixed form only, optional: complex64 [npol*nch][nbins] compensation row.  The
+     * rounding errors of the compensated adds into the raw row collect here and are folded
+     * into the raw row by the next pulse's launch or by ocs_pulse_flush.  NULL: the raw row
+     * is accumulated with plain float32 atomics. */
+    void *raw_lo_d;
 } ocs_pulse_desc;
 
-/* Workspace of ocs_pulse (per-pulse table of the row quantities); < 0 on invalid sizes. */
+/* Workspace of ocs_pulse (per-pulse float64 and float32 tables of the row quantities and
+ * a 16-byte header); < 0 on invalid sizes.  Reset it with ocs_pulse_reset before the
+ * first pulse of a scene. */
 int64_t ocs_pulse_workspace_bytes(int32_t ny, int32_t nch);
 
-/* Accumulate one pulse into raw_d (OCS_PREC_F64: the float64 drop-in; OCS_PREC_MIXED:
- * float64 range / phase reduction, float32 elsewhere). */
+/* Accumulate one pulse into raw_d.
+ * OCS_PREC_F64: the float64 drop-in (every facet's slant range, bins and phase in float64
+ * in the reference's order).
+ * OCS_PREC_MIXED: for SAR scenes with Kodis specular and / or Bragg scattering, nx a
+ * multiple of 4 and 16-byte aligned inputs, the split-range form: float64 only for each
+ * pulse row's and each column's reference range (reduced 2 k0 R mod 2 pi and the range-bin
+ * position, split into float32 hi + lo); each facet's range offset, bin, phase, NRCS and
+ * scene in float32, with the float64 decision only for facets within the float32 error
+ * bound of a rounding boundary (so bins, LUT indices and specular facet selection equal the
+ * float64 form's); compensated float32 accumulation (see raw_lo_d).  Other mixed-precision
+ * pulses (Kirchhoff specular, DopSCA, SKIM) keep the facet's slant range, bins and phase
+ * reduction in float64. */
 int ocs_pulse(const ocs_pulse_desc *desc, int precision, void *stream);
+
+/* Reset the workspace header (pending compensation row, error flag) and zero raw_lo_d;
+ * enqueued on `stream`. */
+int ocs_pulse_reset(const ocs_pulse_desc *desc, void *stream);
+
+/* Fold the compensation row of the last mixed-precision pulse into its raw row; call
+ * after a scene's last pulse (or before reading raw_d).  Enqueued on `stream`. */
+int ocs_pulse_flush(const ocs_pulse_desc *desc, void *stream);
+
+/* OCS_ERR_TIMEOUT if a bounded device-side wait of the mixed kernel gave up since the last
+ * reset, else OCS_OK.  Synchronises with the device. */
+int ocs_pulse_error(const ocs_pulse_desc *desc);
+
+/* SKIM two-scale Doppler (upsample_and_dopplerize, oceansar/radarsim/skim_raw.py:51-81):
+ * the step profiles x_d (complex128 [N][G][R]: N simulated steps, G row groups, R range
+ * bins) up-sampled by n_up as the reference's zero-padded spectrum does (band-limited
+ * interpolation with the period-M Dirichlet kernel, M = N n_up) and modulated by each
+ * group's Doppler dop_d (float64 [G][R]) at t = m / prf, summed over the groups into y_d
+ * (complex128 [M][R]).  D_d: complex128 [M] scratch.  Float64 throughout. */
+int ocs_skim_upsample(const double *x_d, const double *dop_d, double *y_d, double *D_d, int32_t N, int32_t G,
+                      int32_t R, int32_t n_up, double prf, void *stream);
 
 /* ------------------------------------------------------------------------------------
  * Standalone NRCS models (float64).

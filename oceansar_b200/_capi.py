@@ -45,10 +45,16 @@ SIGNATURES = {
     "ocs_surface_update_noalloc": [c_ptr, c_flt, c_ptr],
     "ocs_surface_blend": [c_i64, ctypes.c_int32, c_ptr, c_ptr, c_ptr, c_flt, c_flt, c_ptr],
     "ocs_pulse": [c_ptr, c_int, c_ptr],
+    "ocs_pulse_reset": [c_ptr, c_ptr],
+    "ocs_pulse_flush": [c_ptr, c_ptr],
+    "ocs_pulse_error": [c_ptr],
     "ocs_pulse_workspace_bytes": [ctypes.c_int32, ctypes.c_int32],
     "ocs_rcs_romeiser": [c_ptr, c_ptr],
     "ocs_field_kodis": [c_ptr, c_ptr],
     "ocs_field_ka": [c_ptr, c_ptr],
+    "ocs_chan_profile_status": [],
+    "ocs_skim_upsample": [c_ptr, c_ptr, c_ptr, c_ptr, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                          ctypes.c_int32, c_dbl, c_ptr],
     "ocs_rd_rcmc": [c_ptr, c_i64, ctypes.c_int32, ctypes.c_int32, c_ptr, c_ptr, c_dbl, c_ptr],
     "ocs_rd_azfilter": [c_ptr, c_i64, ctypes.c_int32, ctypes.c_int32, c_ptr, c_ptr],
     "ocs_batch_create": [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(c_ptr)],

@@ -39,7 +39,8 @@ class PulseDesc(ctypes.Structure):
                 ("spec_mode", I32), ("x_d", P), ("ka_dx", F64), ("ka_dy", F64), ("ka_K_re", F64), ("ka_K_im", F64),
                 ("s_m32_d", P), ("s_p32_d", P), ("sca", I32), ("field_nx", I32), ("roll", I32),
                 ("sr_bin_offset", F64), ("cap_t", F64), ("nrcs_row", I32), ("nrcs_rows", I32),
-                ("az_f32", I32), ("skim", I32), ("skim_ny_integ", I32), ("skim_az2", I32), ("skim_rcm", I32)]
+                ("az_f32", I32), ("skim", I32), ("skim_ny_integ", I32), ("skim_az2", I32), ("skim_rcm", I32),
+                ("raw_lo_d", P)]
 
 
 class RcsDesc(ctypes.Structure):

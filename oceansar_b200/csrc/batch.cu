@@ -96,6 +96,7 @@ extern "C" int ocs_batch_set(ocs_batch *b, int32_t slot, const ocs_scene_desc *s
     if (sd->nx != pd->nx || sd->ny != pd->ny) return OCS_ERR_ARG;
     const int tile_rows = sc->tile_rows == 0 ? 64 : sc->tile_rows;
     if (tile_rows < 1 || tile_rows > 128) return OCS_ERR_ARG;
+    if (b->precision == OCS_PREC_MIXED && !pulse_split_ok(pd)) return OCS_ERR_UNSUPPORTED;
     HostSlot h;
     h.rows_key = surface_key(sd->nx);
     h.cols_key = surface_key(sd->ny);
@@ -232,7 +233,7 @@ extern "C" int ocs_batch_step(ocs_batch *b, int32_t pulses, void *stream) {
         for (const auto &c : p.cols)
             if ((st = batch_launch_cols(ref, c.first, (int)c.second.items, (size_t)c.second.smem, cs)) != OCS_OK)
                 return st;
-        if ((st = batch_launch_pulse_rows(ref, cs)) != OCS_OK) return st;
+        if ((st = batch_launch_pulse_rows(ref, b->precision, cs)) != OCS_OK) return st;
         for (const auto &w : p.widths)
             if ((st = batch_launch_pulse(ref, b->precision, w.first, (int)w.second, cs)) != OCS_OK) return st;
         batch_advance_kernel<<<1, 256, 0, cs>>>(ref);

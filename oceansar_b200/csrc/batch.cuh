@@ -97,7 +97,10 @@ int pulse_args_fill(const ocs_pulse_desc *d, void *out);
 // class, one item per CTA (finished slots leave CTAs that return at once).
 int batch_launch_rows(const BatchRef &b, int key, int prog, int grid, size_t smem, cudaStream_t st);
 int batch_launch_cols(const BatchRef &b, int key, int grid, size_t smem, cudaStream_t st);
-int batch_launch_pulse_rows(const BatchRef &b, cudaStream_t st);
+int batch_launch_pulse_rows(const BatchRef &b, int precision, cudaStream_t st);
+// Whether a scene's pulse descriptor takes the split-range mixed kernel (required of every
+// scene of a mixed-precision batch).
+bool pulse_split_ok(const ocs_pulse_desc *d);
 int batch_launch_pulse(const BatchRef &b, int precision, int width, int grid, cudaStream_t st);
 // Pulse-kernel items (groups of a width class x facet tiles) of one scene.
 int batch_pulse_items(int nx, int ny, int tile_rows, int nout, int precision, int width);

@@ -8,6 +8,7 @@
 // accumulates them through the register window of accum.cuh.  Output is accumulated in
 // place (+=), never cleared, exactly like the reference.
 #include "accum.cuh"
+#include "bulk.cuh"
 
 namespace ocs {
 
@@ -213,10 +214,166 @@ static int launch_chan_profile_2d(const double *srg, const void *scene, long lon
     return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
 }
 
+// Bulk-staged form of the two-dimensional accumulation (the default when nx is even and the
+// inputs are 16-byte aligned).  Persistent CTAs walk tiles of kC2Cols columns x tile_rows
+// rows; each warp moves its 32 columns' slant ranges and scene values of a row into a
+// four-row shared-memory ring with two one-dimensional bulk copies (cp.async.bulk, issued by
+// lane 0, completing on the slot's mbarrier), so the per-facet work is two shared loads,
+// the bin / LUT index and the register-window update.  Waits are bounded: a wait that
+// gives up sets g_chan_profile_err (read by ocs_chan_profile_status), lets the warp's
+// copies in flight land and ends the warp's work.
+constexpr int kB2Slots = 4;
+__device__ int g_chan_profile_err = 0;
+
+template <typename T> OCS_HD constexpr size_t b2_slot_bytes() { return 32 * (sizeof(double) + sizeof(cplx<T>)); }
+
+template <typename T, int S> OCS_HD size_t b2_smem_bytes(int taps, int ovs) {
+    return (size_t)((wtab_len<T, S>(taps, ovs) + 3) & ~3) * sizeof(T) + (size_t)kC2Nbw * 2 * sizeof(T) + 128 +
+           (size_t)4 * kB2Slots * b2_slot_bytes<T>() + 4 * kB2Slots * 8;
+}
+
+template <typename T, int S>
+__global__ void __launch_bounds__(kC2Cols, 4)
+chan_profile_2d_bulk_kernel(const double *__restrict__ srg, const cplx<T> *__restrict__ scene, int ny, int nx,
+                            double binsize, double min_sr, const float *__restrict__ sinc, int taps, int ovs,
+                            T *__restrict__ out, int nbins, int tile_rows) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem_raw);            // [4][kB2Slots]
+    unsigned char *stage = smem_raw + 128;                                                   // [4][kB2Slots] slots
+    T *wtab = reinterpret_cast<T *>(stage + 4 * kB2Slots * b2_slot_bytes<T>());
+    const int wlen = wtab_len<T, S>(taps, ovs);
+    T *acc = wtab + ((wlen + 3) & ~3);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    build_wtab<T, S>(wtab, sinc, taps, ovs);
+    if (lane == 0)
+        for (int k = 0; k < kB2Slots; ++k) mbar_init(bars + warp * kB2Slots + k, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    __syncthreads();
+
+    const int tiles_x = (nx + kC2Cols - 1) / kC2Cols;
+    const int tiles = tiles_x * ((ny + tile_rows - 1) / tile_rows);
+    const double inv_binsize = 1.0 / binsize;
+    const int half = taps / 2;
+    unsigned rseq = 0;
+    bool bad = false;
+    unsigned char *wst = stage + (size_t)warp * kB2Slots * b2_slot_bytes<T>();
+    unsigned long long *wbar = bars + warp * kB2Slots;
+    for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const int x0 = (tile % tiles_x) * kC2Cols;
+        const int y0 = (tile / tiles_x) * tile_rows;
+        const int nrows = min(tile_rows, ny - y0);
+        __syncthreads();                  // the previous tile's bins are flushed
+        CtaBins<T, 1> cb;
+        cb.acc = acc;
+        cb.nbw = kC2Nbw;
+        cb.nout = 1;
+        cb.nbins = nbins;
+        cb.out = out;
+        cb.out_stride = 0;
+        {
+            int b0, l0;
+            bin_and_lut(srg[(long long)y0 * nx + x0], min_sr, binsize, ovs, b0, l0);
+            cb.cta_base = (b0 > -(1 << 29)) ? b0 - kC2Nbw / 4 : 0;
+        }
+        cb.zero();
+        __syncthreads();
+        BinWindow<T, S, 1> win;
+        win.reset();
+        const int xw = x0 + 32 * warp;
+        if (xw < nx && !bad) {
+            const int ncw = min(32, nx - xw);
+            const bool col_ok = xw + lane < nx;
+            const unsigned first = rseq;
+            unsigned issued = 0, waited = 0;
+            auto issue = [&](int r) {
+                if (lane == 0 && r < nrows) {
+                    const unsigned q = first + (unsigned)r;
+                    unsigned char *dst = wst + (size_t)(q % kB2Slots) * b2_slot_bytes<T>();
+                    unsigned long long *bar = wbar + (q % kB2Slots);
+                    const long long g = (long long)(y0 + r) * nx + xw;
+                    fence_proxy_async();
+                    mbar_expect_tx(bar, (unsigned)ncw * (unsigned)(sizeof(double) + sizeof(cplx<T>)));
+                    bulk_g2s(dst, srg + g, (unsigned)ncw * 8u, bar);
+                    bulk_g2s(dst + 32 * sizeof(double), scene + g, (unsigned)ncw * (unsigned)sizeof(cplx<T>), bar);
+                    issued = (unsigned)r + 1;
+                }
+            };
+            auto wait_row = [&](int r) -> bool {
+                const unsigned q = first + (unsigned)r;
+                return mbar_wait(wbar + (q % kB2Slots), (q / kB2Slots) & 1u);
+            };
+            issue(0);
+            issue(1);
+            issue(2);
+            bool ok = true;
+            for (int i = 0; i < nrows; ++i) {
+                ok = __all_sync(0xffffffffu, wait_row(i));
+                if (!ok) break;
+                waited = (unsigned)i + 1;
+                const unsigned char *src = wst + (size_t)((first + (unsigned)i) % kB2Slots) * b2_slot_bytes<T>();
+                const double sr = reinterpret_cast<const double *>(src)[lane];
+                const cplx<T> c = reinterpret_cast<const cplx<T> *>(src + 32 * sizeof(double))[lane];
+                __syncwarp();
+                issue(i + 3);             // into the slot of row i - 1
+                if (!col_ok) continue;
+                int bin_d, lut;
+                // FP64: IEEE division, bin / LUT bit-identical with numpy; single precision:
+                // reciprocal multiply (a one-ulp difference in the bin coordinate)
+                if (sizeof(T) == 8) bin_and_lut(sr, min_sr, binsize, ovs, bin_d, lut);
+                else bin_and_lut_fast(sr, min_sr, inv_binsize, ovs, bin_d, lut);
+                if (bin_d < -(1 << 29)) continue;
+                cplx<T> cc[1] = {c};
+                win.add(bin_d - half, lut, cc, wtab, sinc, taps, ovs, cb);
+            }
+            if (!ok) {
+                bad = true;
+                if (lane == 0) {
+                    atomicOr(&g_chan_profile_err, 1);
+                    for (unsigned r = waited; r < issued; ++r) wait_row((int)r);
+                }
+                __syncwarp();
+            }
+            rseq = first + (unsigned)nrows;
+        }
+        win.flush(cb);
+        __syncthreads();
+        cb.flush_to_global();
+    }
+}
+
+template <typename T, int S>
+static int launch_chan_profile_2d_bulk(const double *srg, const void *scene, long long ny, long long nx,
+                                       double binsize, double min_sr, const float *sinc, int taps, int ovs, T *out,
+                                       int nbins, cudaStream_t stream) {
+    if (taps < 1 || taps > S || ovs < 1) return OCS_ERR_ARG;
+    if (ny > 0x7fffffffLL || nx > 0x7fffffffLL) return OCS_ERR_SIZE;
+    const size_t smem = b2_smem_bytes<T, S>(taps, ovs);
+    auto kern = chan_profile_2d_bulk_kernel<T, S>;
+    if (ensure_smem((const void *)kern, smem) != cudaSuccess) return OCS_ERR_CUDA;
+    const int resident = resident_ctas((const void *)kern, kC2Cols, smem);
+    if (resident <= 0) return OCS_ERR_CUDA;
+    // tile height: the tallest (<= kC2Rows) that fills the last wave of resident CTAs
+    const long long tiles_x = (nx + kC2Cols - 1) / kC2Cols;
+    const long long want = (long long)resident * ((tiles_x * ((ny + kC2Rows - 1) / kC2Rows) + resident - 1) / resident);
+    long long per_col = want / tiles_x;
+    if (per_col < 1) per_col = 1;
+    long long rows = (ny + per_col - 1) / per_col;
+    rows = rows < 8 ? (ny < 8 ? ny : 8) : (rows > kC2Rows ? kC2Rows : rows);
+    const long long tiles = tiles_x * ((ny + rows - 1) / rows);
+    const long long grid = tiles < resident ? tiles : resident;
+    kern<<<(unsigned)grid, kC2Cols, smem, stream>>>(srg, reinterpret_cast<const cplx<T> *>(scene), (int)ny, (int)nx,
+                                                      binsize, min_sr, sinc, taps, ovs, out, nbins, (int)rows);
+    return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
+}
+
 template <typename T>
 static int launch_chan_profile_2d_any(const double *srg, const void *scene, long long ny, long long nx,
                                       double binsize, double min_sr, const float *sinc, int taps, int ovs, T *out,
                                       int nbins, cudaStream_t stream) {
+    const bool bulk_ok = nx % 2 == 0 && ((((uintptr_t)srg) | ((uintptr_t)scene)) & 15) == 0;
+    if (bulk_ok && taps <= 8)
+        return launch_chan_profile_2d_bulk<T, 12>(srg, scene, ny, nx, binsize, min_sr, sinc, taps, ovs, out, nbins,
+                                                  stream);
     if (taps <= 8)
         return launch_chan_profile_2d<T, 12>(srg, scene, ny, nx, binsize, min_sr, sinc, taps, ovs, out, nbins,
                                              stream);
@@ -284,4 +441,11 @@ extern "C" int ocs_chan_profile_2d_c64(const double *srg, const float *scene, in
     if (nbins > 0x3fffffff) return OCS_ERR_SIZE;
     return ocs::launch_chan_profile_2d_any<float>(srg, scene, ny, nx, binsize, min_sr, sinc_vec, n_sinc_samples,
                                                   sinc_ovs, output, (int)nbins, (cudaStream_t)stream);
+}
+
+extern "C" int ocs_chan_profile_status(void) {
+    int flag = 0, zero = 0;
+    if (cudaMemcpyFromSymbol(&flag, ocs::g_chan_profile_err, sizeof(int)) != cudaSuccess) return OCS_ERR_CUDA;
+    if (flag && cudaMemcpyToSymbol(ocs::g_chan_profile_err, &zero, sizeof(int)) != cudaSuccess) return OCS_ERR_CUDA;
+    return flag ? OCS_ERR_TIMEOUT : OCS_OK;
 }

@@ -681,6 +681,12 @@ pulse_kernel(const __grid_constant__ PulseArgs a) {
     pulse_nrcs<T>(a, sm, spec_sum, bragg_sum);
 }
 
+}  // namespace ocs
+
+#include "pulse_mixed.cuh"
+
+namespace ocs {
+
 // ---------------------------------------------------------------------------------------
 // Scene batch (batch.cuh).  Output groups: a slot's npol*nch outputs are taken G at a time
 // (G = 4 in the mixed form, 2 in FP64); a group of w outputs runs in the kernel of width
@@ -705,6 +711,7 @@ OCS_D int slot_pulse_tiles(const SlotState &g) {
     return ((g.nx + kPulseCols - 1) / kPulseCols) * ((g.ny + g.tile_rows - 1) / g.tile_rows);
 }
 
+template <bool MIXED>
 __global__ void batch_pulse_rows_kernel(const __grid_constant__ BatchRef b) {
     __shared__ int pref[kMaxSlots + 1];
     const int total = scan_slots(b, pref, [](const SlotState &g) {
@@ -715,7 +722,10 @@ __global__ void batch_pulse_rows_kernel(const __grid_constant__ BatchRef b) {
         const SlotState &g = b.slots[s];
         const PulseArgs &a = *static_cast<const PulseArgs *>(g.pargs);
         const int y = (item - pref[s]) * blockDim.x + threadIdx.x;
-        if (y < a.ny) pulse_row(a, g.aznow_tab[g.counter], y);
+        if (y < a.ny) {
+            if (MIXED) mix_row(a, g.aznow_tab[g.counter], y);
+            else pulse_row(a, g.aznow_tab[g.counter], y);
+        }
     }
 }
 
@@ -766,6 +776,65 @@ batch_pulse_kernel(const __grid_constant__ BatchRef b) {
     pulse_nrcs<T>(pa, sm, spec_sum, bragg_sum);
 }
 
+// The mixed form of the batch: every slot's scene passes pulse_split_ok (checked when the
+// slot is set) and its tile runs the split-range kernel's tile (mix_tile); the raw rows
+// take the CTA's compensated bins through plain float32 atomics (no compensation row).
+template <int NOUT>
+__global__ void __launch_bounds__(kMixCols, NOUT < 4 ? 3 : 2)
+batch_pulse_mixed_kernel(const __grid_constant__ BatchRef b) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ PulseArgs pa;
+    __shared__ int pref[kMaxSlots + 1];
+    constexpr int G = 4;
+    const int total = scan_slots(b, pref, [](const SlotState &g) {
+        int o, w;
+        return slot_live(g) ? groups_of_class(g.nout, G, NOUT, -1, o, w) * slot_pulse_tiles(g) : 0;
+    });
+    const int item = blockIdx.x;
+    if (item >= total) return;
+    const int s = find_slot(pref, b.nslots, item);
+    const SlotState &g = b.slots[s];
+    const int tiles = slot_pulse_tiles(g);
+    const int j = item - pref[s];
+    const int grp = j / tiles, tile = j - grp * tiles;
+    {
+        const int *src = static_cast<const int *>(g.pargs);
+        int *dst = reinterpret_cast<int *>(&pa);
+        for (int i = threadIdx.x; i < (int)(sizeof(PulseArgs) / 4); i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int c = g.counter;
+        int o = 0, w = 0;
+        groups_of_class(g.nout, G, NOUT, grp, o, w);
+        pa.out0 = o;
+        pa.nout = w;
+        pa.az_step = c;
+        pa.az_now = g.aznow_tab[c];
+        pa.refresh = (g.flags_tab[c] & kFlagRefresh) ? 1 : 0;
+        pa.tmod_m = g.tmod_tab[2 * c];
+        pa.tmod_p = g.tmod_tab[2 * c + 1];
+        pa.raw_row = (long long)c * pa.nbins;
+        pa.tile_rows = g.tile_rows;
+    }
+    const MixSmem<NOUT> sm = mix_smem<NOUT>(smem, kMaxCh, kPulseRowsMax);
+    build_wtab<float, kMixS>(sm.wtab, pa.sinc, kSincTaps, kSincOvs);
+    if ((threadIdx.x & 31) == 0)
+        for (int k = 0; k < kMixSlots; ++k) mbar_init(sm.bar + (threadIdx.x >> 5) * kMixSlots + k, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    __syncthreads();
+    double spec_sum = 0.0, bragg_sum[2] = {0.0, 0.0};
+    unsigned rseq = 0;
+    bool bad = false;
+    mix_tile<NOUT, true>(pa, nullptr, tile, g.tile_rows, sm, rseq, bad, spec_sum, bragg_sum);
+    if (pa.out0 == 0) {
+        if (pa.do_kodis) block_atomic_sum(spec_sum, &pa.nrcs_spec[pa.az_step], sm.sred);
+        if (pa.do_bragg && pa.refresh)
+            for (int p = 0; p < pa.npol; ++p)
+                block_atomic_sum(bragg_sum[p], &pa.nrcs_bragg[(long long)p * pa.az_steps + pa.az_step], sm.sred);
+    }
+}
+
 template <typename T, int NOUT, int S>
 static int launch_pulse(PulseArgs a, cudaStream_t st) {
     const size_t smem = pulse_smem_bytes<T, NOUT, S, kPulseRows>(a.nch);
@@ -798,6 +867,39 @@ static int launch_pulse(PulseArgs a, cudaStream_t st) {
     const long long grid = tiles < resident ? tiles : resident;
     k<<<(unsigned)grid, kPulseCols, smem, st>>>(a);
     return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
+}
+
+// Tile height for a persistent launch: the tallest (<= kPulseRows) that still gives every
+// resident CTA slot a tile in the last wave.
+static int tile_rows_for(int nx, int ny, int cols, int resident) {
+    const int tiles_x = (nx + cols - 1) / cols;
+    const long long want = (long long)resident * (((long long)tiles_x * ((ny + kPulseRows - 1) / kPulseRows) +
+                                                   resident - 1) / resident);
+    long long per_col = want / tiles_x;
+    if (per_col < 1) per_col = 1;
+    const int rows = (int)((ny + per_col - 1) / per_col);
+    return rows < 16 ? (ny < 16 ? ny : 16) : (rows > kPulseRows ? kPulseRows : rows);
+}
+
+template <int NOUT, bool KODIS>
+static int launch_pulse_mixed(PulseArgs a, float *lo_row, cudaStream_t st) {
+    const size_t smem = mix_smem_bytes<NOUT>(a.nch, kPulseRows);
+    auto k = pulse_mixed_kernel<NOUT, KODIS>;
+    if (ensure_smem((const void *)k, smem) != cudaSuccess) return OCS_ERR_CUDA;
+    const int resident = resident_ctas((const void *)k, kMixCols, smem);
+    if (resident <= 0) return OCS_ERR_CUDA;
+    a.tile_rows = tile_rows_for(a.nx, a.ny, kMixCols, resident);
+    const long long tiles = (long long)((a.nx + kMixCols - 1) / kMixCols) * ((a.ny + a.tile_rows - 1) / a.tile_rows);
+    const long long grid = tiles < resident ? tiles : resident;
+    k<<<(unsigned)grid, kMixCols, smem, st>>>(a, lo_row);
+    return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
+}
+
+template <bool KODIS>
+static int launch_pulse_mixed_n(const PulseArgs &a, float *lo_row, cudaStream_t st) {
+    if (a.nout == 1) return launch_pulse_mixed<1, KODIS>(a, lo_row, st);
+    if (a.nout == 2) return launch_pulse_mixed<2, KODIS>(a, lo_row, st);
+    return launch_pulse_mixed<4, KODIS>(a, lo_row, st);
 }
 
 }  // namespace ocs
@@ -938,12 +1040,22 @@ int pulse_args_fill(const ocs_pulse_desc *d, void *out) {
     return st;
 }
 
-int batch_launch_pulse_rows(const BatchRef &b, cudaStream_t st) {
+int batch_launch_pulse_rows(const BatchRef &b, int precision, cudaStream_t st) {
     int sms = 0, dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
         return OCS_ERR_CUDA;
-    batch_pulse_rows_kernel<<<sms * 4, 128, 0, st>>>(b);
+    if (precision == OCS_PREC_MIXED) batch_pulse_rows_kernel<true><<<sms * 4, 128, 0, st>>>(b);
+    else batch_pulse_rows_kernel<false><<<sms * 4, 128, 0, st>>>(b);
+    return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
+}
+
+template <int NOUT>
+static int batch_pulse_mixed_n(const BatchRef &b, int grid, cudaStream_t st) {
+    const size_t smem = mix_smem_bytes<NOUT>(kMaxCh, kPulseRowsMax);
+    auto k = batch_pulse_mixed_kernel<NOUT>;
+    if (ensure_smem((const void *)k, smem) != cudaSuccess) return OCS_ERR_CUDA;
+    k<<<grid, kMixCols, smem, st>>>(b);
     return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
 }
 
@@ -971,9 +1083,9 @@ int batch_launch_pulse(const BatchRef &b, int precision, int width, int grid, cu
         return OCS_ERR_ARG;
     }
     if (precision == OCS_PREC_MIXED) {
-        if (width == 1) return batch_pulse_n<float, 1, 12>(b, grid, st);
-        if (width == 2) return batch_pulse_n<float, 2, 12>(b, grid, st);
-        if (width == 4) return batch_pulse_n<float, 4, 12>(b, grid, st);
+        if (width == 1) return batch_pulse_mixed_n<1>(b, grid, st);
+        if (width == 2) return batch_pulse_mixed_n<2>(b, grid, st);
+        if (width == 4) return batch_pulse_mixed_n<4>(b, grid, st);
         return OCS_ERR_ARG;
     }
     return OCS_ERR_ARG;
@@ -983,7 +1095,68 @@ int batch_launch_pulse(const BatchRef &b, int precision, int width, int grid, cu
 
 extern "C" int64_t ocs_pulse_workspace_bytes(int32_t ny, int32_t nch) {
     if (ny < 1 || nch < 1 || nch > kMaxCh) return -1;
-    return (int64_t)ny * (5 + 2 * nch) * (int64_t)sizeof(double);
+    return (int64_t)(mix_hdr_offset(ny, nch) + kMixHdrBytes);
+}
+
+// Whether the split-range mixed kernel takes this pulse: SAR mode with Kodis and / or
+// direct / LUT Bragg scattering, the float32 scatterer series, column counts and base
+// pointers that allow 16-byte bulk copies of every input row.
+static bool mixed_split_ok(const ocs_pulse_desc *d);
+namespace ocs {
+bool pulse_split_ok(const ocs_pulse_desc *d) { return mixed_split_ok(d); }
+}  // namespace ocs
+static bool mixed_split_ok(const ocs_pulse_desc *d) {
+    if (d->sca || d->skim || (d->do_kodis && d->spec_mode != 0) || !(d->do_kodis || d->do_bragg)) return false;
+    if (d->nx % 4 != 0) return false;
+    if (d->do_bragg && (!d->s_m32_d || !d->s_p32_d)) return false;
+    if (!d->diffx_d || !d->diffy_d) return false;
+    const void *ptrs[] = {d->dx_d, d->dy_d, d->dz_d, d->diffx_d, d->diffy_d,
+                          d->do_kodis ? d->diffxx_d : nullptr, d->do_kodis ? d->diffyy_d : nullptr,
+                          d->do_kodis ? d->diffxy_d : nullptr, d->do_bragg ? d->ind0_m_d : nullptr,
+                          d->do_bragg ? d->ind0_p_d : nullptr, d->do_bragg ? d->scat_d : nullptr};
+    for (const void *p : ptrs)
+        if (((uintptr_t)p) & 15) return false;
+    return ((uintptr_t)d->rowtab_d & 15) == 0;
+}
+
+// Compensation row of the mixed kernel (complex64 [npol*nch][nbins]) and the workspace
+// header: reset before a scene (pending row -1, error flag 0, row zeroed).
+extern "C" int ocs_pulse_reset(const ocs_pulse_desc *d, void *stream) {
+    if (!d || !d->rowtab_d || d->ny < 1 || d->nch < 1 || d->nch > kMaxCh) return OCS_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned char *hdr = (unsigned char *)d->rowtab_d + mix_hdr_offset(d->ny, d->nch);
+    if (cudaMemsetAsync(hdr, 0xff, 4, s) != cudaSuccess) return OCS_ERR_CUDA;
+    if (cudaMemsetAsync(hdr + 4, 0, kMixHdrBytes - 4, s) != cudaSuccess) return OCS_ERR_CUDA;
+    if (d->raw_lo_d) {
+        const size_t n = (size_t)d->npol * d->nch * d->nbins * 2 * sizeof(float);
+        if (cudaMemsetAsync(d->raw_lo_d, 0, n, s) != cudaSuccess) return OCS_ERR_CUDA;
+    }
+    return OCS_OK;
+}
+
+// Fold the last pulse's compensation row into its raw row (the scene's final step, or
+// before the raw cube is read); no-op when nothing is pending.
+extern "C" int ocs_pulse_flush(const ocs_pulse_desc *d, void *stream) {
+    PulseArgs a;
+    int st = fill_pulse_args(d, a);
+    if (st != OCS_OK) return st;
+    if (!d->raw_lo_d) return OCS_OK;
+    const int nout = d->npol * d->nch;
+    const long long n = (long long)nout * d->nbins;
+    long long blocks = (n + 255) / 256;
+    if (blocks > 1024) blocks = 1024;
+    pulse_flush_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(a, (float *)d->raw_lo_d, nout);
+    return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
+}
+
+// Status of the mixed kernel's bounded waits since the last reset (synchronises with the
+// device): OCS_OK, or OCS_ERR_TIMEOUT if a wait gave up.
+extern "C" int ocs_pulse_error(const ocs_pulse_desc *d) {
+    if (!d || !d->rowtab_d || d->ny < 1 || d->nch < 1 || d->nch > kMaxCh) return OCS_ERR_ARG;
+    int flag = 0;
+    const unsigned char *hdr = (const unsigned char *)d->rowtab_d + mix_hdr_offset(d->ny, d->nch);
+    if (cudaMemcpy(&flag, hdr + 4, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return OCS_ERR_CUDA;
+    return flag ? OCS_ERR_TIMEOUT : OCS_OK;
 }
 
 extern "C" int ocs_pulse(const ocs_pulse_desc *d, int precision, void *stream) {
@@ -992,8 +1165,10 @@ extern "C" int ocs_pulse(const ocs_pulse_desc *d, int precision, void *stream) {
     if (st != OCS_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
     const int nout = d->npol * d->nch;
-    pulse_rows_kernel<<<(d->ny + 127) / 128, 128, 0, s>>>(a);
-    if (cudaGetLastError() != cudaSuccess) return OCS_ERR_CUDA;
+    if (!(precision == OCS_PREC_MIXED && mixed_split_ok(d))) {
+        pulse_rows_kernel<<<(d->ny + 127) / 128, 128, 0, s>>>(a);
+        if (cudaGetLastError() != cudaSuccess) return OCS_ERR_CUDA;
+    }
     if (precision == OCS_PREC_F64) {
         for (int o = 0; o < nout; o += 2) {
             a.out0 = o;
@@ -1001,6 +1176,22 @@ extern "C" int ocs_pulse(const ocs_pulse_desc *d, int precision, void *stream) {
             st = (a.nout == 1) ? launch_pulse<double, 1, 12>(a, s) : launch_pulse<double, 2, 12>(a, s);
             if (st != OCS_OK) return st;
             a.refresh = 0;                  // later groups read the refreshed RCS
+        }
+        return OCS_OK;
+    }
+    if (precision == OCS_PREC_MIXED && mixed_split_ok(d)) {
+        float *lo_row = (float *)d->raw_lo_d;
+        const int rows = d->ny > nout * d->nbins ? d->ny : nout * d->nbins;
+        long long blocks = (rows + 127) / 128;
+        if (blocks > 4096) blocks = 4096;
+        pulse_rows_mixed_kernel<<<(unsigned)blocks, 128, 0, s>>>(a, lo_row, nout);
+        if (cudaGetLastError() != cudaSuccess) return OCS_ERR_CUDA;
+        for (int o = 0; o < nout; o += 4) {
+            a.out0 = o;
+            a.nout = nout - o < 4 ? nout - o : 4;
+            st = d->do_kodis ? launch_pulse_mixed_n<true>(a, lo_row, s) : launch_pulse_mixed_n<false>(a, lo_row, s);
+            if (st != OCS_OK) return st;
+            a.refresh = 0;
         }
         return OCS_OK;
     }

@@ -290,6 +290,11 @@ class RawGenerator(object):
         nb = _capi.load().ocs_pulse_workspace_bytes(s.Ny, self.num_ch)
         self._rowtab = torch.empty(int(nb), dtype=torch.uint8, device=_device.device())
         d.rowtab_d = self._rowtab.data_ptr()
+        if self.precision == 'mixed':
+            # compensation row of the raw cube's compensated float32 accumulation
+            self._raw_lo = _device.zeros((nout, self.rg_samp), cdt)
+            d.raw_lo_d = self._raw_lo.data_ptr()
+        _capi.call("ocs_pulse_reset", ctypes.addressof(d), _device.stream_ptr(self.stream))
         self._refreshes = []
 
     # ------------------------------------------------------------------------------------
@@ -377,6 +382,19 @@ class RawGenerator(object):
     def run(self, steps=None):
         for a in (range(self.az_steps) if steps is None else steps):
             self.pulse(a)
+        self.flush()
+
+    def flush(self, stream=None):
+        """Fold the last pulse's compensation row into the raw cube (mixed form; a no-op
+        otherwise).  ``run``, ``run_overlapped`` and ``raw`` call it."""
+        _capi.call("ocs_pulse_flush", ctypes.addressof(self.desc),
+                   _device.stream_ptr(stream if stream is not None else self.stream))
+
+    def check(self):
+        """Raise if a bounded device-side wait of the pulse kernel gave up (synchronises)."""
+        st = _capi.load().ocs_pulse_error(ctypes.addressof(self.desc))
+        if st != 0:
+            raise RuntimeError('ocs_pulse: a device-side wait gave up (status %d)' % st)
 
     def can_overlap(self):
         """Whether ``run_overlapped`` applies (not for choppy, frozen or time-interpolated
@@ -431,6 +449,7 @@ class RawGenerator(object):
                 evp = torch.cuda.Event()
                 evp.record(main)
                 done_pulse[i] = evp
+            self.flush(stream=main)
         finally:
             self.stream = saved
         main.wait_stream(side)
@@ -440,6 +459,7 @@ class RawGenerator(object):
         self.raw_d.zero_()
         self.nrcs_spec_d.zero_()
         self.nrcs_bragg_d.zero_()
+        _capi.call("ocs_pulse_reset", ctypes.addressof(self.desc), _device.stream_ptr(self.stream))
         self.t_last_rcs_bragg = -1.
         self._refreshes = []
         if self.balancer is not None:
@@ -550,6 +570,8 @@ class RawGenerator(object):
 
     def raw(self):
         """Accumulated raw cube [pol, ch, az, rg_samp] before calibration (host copy)."""
+        self.flush()
+        self.check()
         r = self.raw_d.cpu().numpy()
         return r.reshape(self.npol, self.num_ch, self.az_steps, self.rg_samp)
 

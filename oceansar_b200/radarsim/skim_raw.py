@@ -17,8 +17,8 @@ azimuth.  Compared with ``sar_raw`` its loop differs in these ways, all reproduc
 
 The device does the surface, the row table and one pulse-kernel launch per simulated step
 (the SKIM mode of ``ocs_pulse``, which writes the row-group profiles directly); the host
-does the set-up in the reference's order (same RNG stream), the up-sampling (numpy FFTs in
-complex64, as the reference), calibration and noise.  Not built: calibration targets
+does the set-up in the reference's order (same RNG stream), calibration and noise; the
+up-sampling and Doppler of the two-scale form run on the device (``ocs_skim_upsample``).  Not built: calibration targets
 (``sim.cal_targets``) and buoy-spectrum input, which raise ``NotImplementedError``.
 """
 import ctypes
@@ -42,24 +42,29 @@ from .sar_raw_nompi import C_LIGHT, G, PRECISIONS
 N_SINC, SINC_OVS = 10, 20
 
 
-def upsample_and_dopplerize(ssraw, dop, n_up, prf):
-    """Up-sample the step profiles [steps, groups, rg] by ``n_up`` and apply the geometric
-    Doppler ``dop`` [groups, rg] of each row group (``skim_raw.py:51-81``): per group, the
-    azimuth spectrum is zero-padded, brought back to time and modulated; complex64 as in
-    the reference."""
-    dims = ssraw.shape
+def upsample_and_dopplerize(ssraw, dop, n_up, prf, stream=None):
+    """Up-sample the step profiles ``ssraw`` [steps, groups, rg] by ``n_up`` and apply the
+    geometric Doppler ``dop`` [groups, rg] of each row group, summed over the groups
+    (``skim_raw.py:51-81``); returns complex128 [steps * n_up, rg].
+
+    On the device (``ocs_skim_upsample``): the reference's zero-padded azimuth spectrum
+    transformed back is the band-limited (Dirichlet-kernel) interpolation of the step
+    samples, which the kernel evaluates directly for every output sample and range bin, with
+    the Doppler ramp applied in the same pass.  ``ssraw`` may be a numpy array or a device
+    tensor (the generator passes its device profiles)."""
+    dev = _device.device()
+    x = torch.as_tensor(ssraw).to(device=dev, dtype=torch.complex128).contiguous()
+    if x.dim() != 3:
+        raise ValueError('ssraw must be [steps, groups, rg]')
+    N, G, R = (int(v) for v in x.shape)
     n_up = int(n_up)
-    out = np.zeros((dims[0] * n_up, dims[2]), dtype=np.complex64)
-    t = (np.arange(dims[0] * n_up) / prf).reshape((dims[0] * n_up, 1))
-    t2pi = t * (np.pi * 2)
-    for ind in range(dims[1]):
-        raw_zp = np.zeros((dims[0] * n_up, dims[2]), dtype=np.complex64)
-        raw_zp[0:dims[0]] = np.fft.fftshift(np.fft.fft(ssraw[:, ind, :], axis=0), axes=(0,))
-        raw_zp = np.roll(raw_zp, int(-dims[0] / 2), axis=0)
-        raw_zp = np.conj(np.fft.fft(np.conj(raw_zp), axis=0)) / dims[0]
-        dop_phase = t2pi * (dop[ind]).reshape((1, dims[2]))
-        out = out + raw_zp * np.exp(1j * dop_phase)
-    return out
+    d = torch.as_tensor(np.ascontiguousarray(np.broadcast_to(np.asarray(dop, dtype=np.float64), (G, R))),
+                        device=dev)
+    y = torch.empty((N * n_up, R), dtype=torch.complex128, device=dev)
+    D = torch.empty((N * n_up,), dtype=torch.complex128, device=dev)
+    _capi.call("ocs_skim_upsample", x.data_ptr(), d.data_ptr(), y.data_ptr(), D.data_ptr(), N, G, R, n_up,
+               float(prf), _device.stream_ptr(stream))
+    return y.cpu().numpy()
 
 
 class SkimGenerator(object):
@@ -372,12 +377,12 @@ class SkimGenerator(object):
     def finish(self, add_noise=True):
         """(raw [pol, az, n_rg], NRCS_avg [pol, n_pulses]): up-sampling and Doppler of the
         two-scale form, truncation, calibration and noise (:661-677)."""
-        prof = self.profiles()
+        prof = None if self.two_scale else self.profiles()
         out = []
         cal = self.cal_factor()
         for p in range(self.npol):
             if self.two_scale:
-                r = upsample_and_dopplerize(prof[p], self.dop0, self.n_pulses_b, self.prf)
+                r = upsample_and_dopplerize(self.raw_d[p], self.dop0, self.n_pulses_b, self.prf, stream=self.stream)
             else:
                 r = prof[p][:, 0, :]
             r = r[:, :self.n_rg]

@@ -49,6 +49,8 @@ def _cfg(c):
 
 
 def _rows(gen, steps):
+    gen.flush()
+    gen.check()
     r = gen.raw_d[:, list(steps)].cpu().numpy()
     return r.reshape(gen.npol, gen.num_ch, len(steps), gen.rg_samp)
 
