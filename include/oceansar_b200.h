@@ -78,11 +78,6 @@ int ocs_chan_profile_2d_c64(const double *srg_d, const float *scene_d, int64_t n
                             int n_sinc_samples, int sinc_ovs, float *output_d, int64_t nbins,
                             void *stream);
 
-/* OCS_ERR_TIMEOUT if a bounded device-side wait of the bulk-staged 2-D accumulation gave up
- * since the last call (the flag is then cleared), else OCS_OK.  Synchronises with the
- * device. */
-int ocs_chan_profile_status(void);
-
 
 /* ------------------------------------------------------------------------------------
  * Per-pulse surface synthesis.

@@ -52,7 +52,6 @@ SIGNATURES = {
     "ocs_rcs_romeiser": [c_ptr, c_ptr],
     "ocs_field_kodis": [c_ptr, c_ptr],
     "ocs_field_ka": [c_ptr, c_ptr],
-    "ocs_chan_profile_status": [],
     "ocs_skim_upsample": [c_ptr, c_ptr, c_ptr, c_ptr, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                           ctypes.c_int32, c_dbl, c_ptr],
     "ocs_rd_rcmc": [c_ptr, c_i64, ctypes.c_int32, ctypes.c_int32, c_ptr, c_ptr, c_dbl, c_ptr],

@@ -43,3 +43,24 @@ OCS_D void bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long lo
 OCS_D void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
 }  // namespace ocs
+
+namespace ocs {
+
+// Tiled tensor copies global -> shared (cp.async.bulk.tensor) completing on `bar`; `map` is
+// the generic address of a CUtensorMap in parameter or global memory, (x, y[, z]) the
+// box origin in elements (x times the element size a multiple of 16 bytes).  Boxes that
+// reach past the tensor are filled with zeros and count their full size.
+OCS_D void tma_load_2d(void *dst, const void *map, int x, int y, unsigned long long *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n"
+        ::"r"(smem_u32(dst)), "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+OCS_D void tma_load_3d(void *dst, const void *map, int x, int y, int z, unsigned long long *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n"
+        ::"r"(smem_u32(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+}  // namespace ocs

@@ -33,7 +33,10 @@
 //             range and the bin / LUT indices bit-identical to numpy.
 //   float  -- mixed: slant range, bin / LUT indices and the 2 k0 r phase reduction in
 //             float64, everything else (NRCS, scene, accumulation) in float32.
+#include <cudaTypedefs.h>
 #include <string.h>
+
+#include <mutex>
 
 #include "accum.cuh"
 #include "batch.cuh"
@@ -819,14 +822,12 @@ batch_pulse_mixed_kernel(const __grid_constant__ BatchRef b) {
     }
     const MixSmem<NOUT> sm = mix_smem<NOUT>(smem, kMaxCh, kPulseRowsMax);
     build_wtab<float, kMixS>(sm.wtab, pa.sinc, kSincTaps, kSincOvs);
-    if ((threadIdx.x & 31) == 0)
-        for (int k = 0; k < kMixSlots; ++k) mbar_init(sm.bar + (threadIdx.x >> 5) * kMixSlots + k, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    __syncthreads();
+    mix_init<NOUT>(sm);
     double spec_sum = 0.0, bragg_sum[2] = {0.0, 0.0};
     unsigned rseq = 0;
     bool bad = false;
-    mix_tile<NOUT, true>(pa, nullptr, tile, g.tile_rows, sm, rseq, bad, spec_sum, bragg_sum);
+    mix_tile<NOUT, true>(pa, static_cast<const MixMaps *>(g.maps), nullptr, tile, g.tile_rows, sm, rseq, bad,
+                         spec_sum, bragg_sum);
     if (pa.out0 == 0) {
         if (pa.do_kodis) block_atomic_sum(spec_sum, &pa.nrcs_spec[pa.az_step], sm.sred);
         if (pa.do_bragg && pa.refresh)
@@ -882,7 +883,7 @@ static int tile_rows_for(int nx, int ny, int cols, int resident) {
 }
 
 template <int NOUT, bool KODIS>
-static int launch_pulse_mixed(PulseArgs a, float *lo_row, cudaStream_t st) {
+static int launch_pulse_mixed(PulseArgs a, const MixMaps &maps, float *lo_row, cudaStream_t st) {
     const size_t smem = mix_smem_bytes<NOUT>(a.nch, kPulseRows);
     auto k = pulse_mixed_kernel<NOUT, KODIS>;
     if (ensure_smem((const void *)k, smem) != cudaSuccess) return OCS_ERR_CUDA;
@@ -891,15 +892,74 @@ static int launch_pulse_mixed(PulseArgs a, float *lo_row, cudaStream_t st) {
     a.tile_rows = tile_rows_for(a.nx, a.ny, kMixCols, resident);
     const long long tiles = (long long)((a.nx + kMixCols - 1) / kMixCols) * ((a.ny + a.tile_rows - 1) / a.tile_rows);
     const long long grid = tiles < resident ? tiles : resident;
-    k<<<(unsigned)grid, kMixCols, smem, st>>>(a, lo_row);
+    k<<<(unsigned)grid, kMixCols, smem, st>>>(a, maps, lo_row);
     return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
 }
 
 template <bool KODIS>
-static int launch_pulse_mixed_n(const PulseArgs &a, float *lo_row, cudaStream_t st) {
-    if (a.nout == 1) return launch_pulse_mixed<1, KODIS>(a, lo_row, st);
-    if (a.nout == 2) return launch_pulse_mixed<2, KODIS>(a, lo_row, st);
-    return launch_pulse_mixed<4, KODIS>(a, lo_row, st);
+static int launch_pulse_mixed_n(const PulseArgs &a, const MixMaps &maps, float *lo_row, cudaStream_t st) {
+    if (a.nout == 1) return launch_pulse_mixed<1, KODIS>(a, maps, lo_row, st);
+    if (a.nout == 2) return launch_pulse_mixed<2, KODIS>(a, maps, lo_row, st);
+    return launch_pulse_mixed<4, KODIS>(a, maps, lo_row, st);
+}
+
+// Tensor-map encoder of the driver, resolved once through the runtime (no link to libcuda).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// One map of a [depth][ny][nx] tensor of 4-byte elements with planes `plane` bytes apart
+// and boxes of one row of kMixCols columns times `depth` planes (depth 1: two-dimensional).
+static bool encode_rows_map(CUtensorMap &m, const void *base, CUtensorMapDataType type, int nx, int ny, int depth,
+                            unsigned long long plane) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint32_t rank = depth > 1 ? 3 : 2;
+    const cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)depth};
+    const cuuint64_t strides[2] = {(cuuint64_t)nx * 4, (cuuint64_t)plane};
+    const cuuint32_t box[3] = {(cuuint32_t)kMixCols, 1, (cuuint32_t)depth};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return enc(&m, type, rank, const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Tensor maps of a pulse descriptor for the split-range kernel; false when its inputs do not
+// allow them (fields not equally spaced in one allocation, misaligned bases, or nx not a
+// multiple of 4).
+static bool fill_mix_maps(const ocs_pulse_desc *d, MixMaps &m) {
+    memset(&m, 0, sizeof(m));
+    if (d->nx % 4 != 0 || d->nx < 4) return false;
+    const int nf = d->do_kodis ? 8 : 5;
+    const char *f[8] = {(const char *)d->dx_d, (const char *)d->dy_d, (const char *)d->dz_d,
+                        (const char *)d->diffx_d, (const char *)d->diffy_d, (const char *)d->diffxx_d,
+                        (const char *)d->diffyy_d, (const char *)d->diffxy_d};
+    const long long plane = (long long)(f[1] - f[0]);
+    const long long need = (long long)d->nx * d->ny * 4;
+    if (plane < need || plane % 16 != 0 || ((uintptr_t)f[0] & 15)) return false;
+    for (int k = 1; k < nf; ++k)
+        if (!f[k] || f[k] - f[0] != k * plane) return false;
+    m.nf = nf;
+    if (!encode_rows_map(m.fields, f[0], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, d->nx, d->ny, nf, (unsigned long long)plane))
+        return false;
+    if (d->do_bragg) {
+        if ((((uintptr_t)d->ind0_m_d) | ((uintptr_t)d->ind0_p_d) | ((uintptr_t)d->scat_d)) & 15) return false;
+        if (!encode_rows_map(m.indm, d->ind0_m_d, CU_TENSOR_MAP_DATA_TYPE_INT32, d->nx, d->ny, 1, 0) ||
+            !encode_rows_map(m.indp, d->ind0_p_d, CU_TENSOR_MAP_DATA_TYPE_INT32, d->nx, d->ny, 1, 0) ||
+            !encode_rows_map(m.scat, d->scat_d, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, d->nx, d->ny, 2 * d->npol,
+                             (unsigned long long)need))
+            return false;
+    }
+    return true;
 }
 
 }  // namespace ocs
@@ -1104,19 +1164,20 @@ extern "C" int64_t ocs_pulse_workspace_bytes(int32_t ny, int32_t nch) {
 static bool mixed_split_ok(const ocs_pulse_desc *d);
 namespace ocs {
 bool pulse_split_ok(const ocs_pulse_desc *d) { return mixed_split_ok(d); }
+size_t pulse_maps_bytes() { return sizeof(MixMaps); }
+int pulse_maps_fill(const ocs_pulse_desc *d, void *out) {
+    MixMaps m;
+    if (!fill_mix_maps(d, m)) return OCS_ERR_UNSUPPORTED;
+    memcpy(out, &m, sizeof(m));
+    return OCS_OK;
+}
 }  // namespace ocs
 static bool mixed_split_ok(const ocs_pulse_desc *d) {
     if (d->sca || d->skim || (d->do_kodis && d->spec_mode != 0) || !(d->do_kodis || d->do_bragg)) return false;
-    if (d->nx % 4 != 0) return false;
     if (d->do_bragg && (!d->s_m32_d || !d->s_p32_d)) return false;
-    if (!d->diffx_d || !d->diffy_d) return false;
-    const void *ptrs[] = {d->dx_d, d->dy_d, d->dz_d, d->diffx_d, d->diffy_d,
-                          d->do_kodis ? d->diffxx_d : nullptr, d->do_kodis ? d->diffyy_d : nullptr,
-                          d->do_kodis ? d->diffxy_d : nullptr, d->do_bragg ? d->ind0_m_d : nullptr,
-                          d->do_bragg ? d->ind0_p_d : nullptr, d->do_bragg ? d->scat_d : nullptr};
-    for (const void *p : ptrs)
-        if (((uintptr_t)p) & 15) return false;
-    return ((uintptr_t)d->rowtab_d & 15) == 0;
+    if (!d->diffx_d || !d->diffy_d || ((uintptr_t)d->rowtab_d & 15)) return false;
+    MixMaps m;
+    return fill_mix_maps(d, m);
 }
 
 // Compensation row of the mixed kernel (complex64 [npol*nch][nbins]) and the workspace
@@ -1180,6 +1241,8 @@ extern "C" int ocs_pulse(const ocs_pulse_desc *d, int precision, void *stream) {
         return OCS_OK;
     }
     if (precision == OCS_PREC_MIXED && mixed_split_ok(d)) {
+        MixMaps maps;
+        if (!fill_mix_maps(d, maps)) return OCS_ERR_CUDA;
         float *lo_row = (float *)d->raw_lo_d;
         const int rows = d->ny > nout * d->nbins ? d->ny : nout * d->nbins;
         long long blocks = (rows + 127) / 128;
@@ -1189,7 +1252,8 @@ extern "C" int ocs_pulse(const ocs_pulse_desc *d, int precision, void *stream) {
         for (int o = 0; o < nout; o += 4) {
             a.out0 = o;
             a.nout = nout - o < 4 ? nout - o : 4;
-            st = d->do_kodis ? launch_pulse_mixed_n<true>(a, lo_row, s) : launch_pulse_mixed_n<false>(a, lo_row, s);
+            st = d->do_kodis ? launch_pulse_mixed_n<true>(a, maps, lo_row, s)
+                             : launch_pulse_mixed_n<false>(a, maps, lo_row, s);
             if (st != OCS_OK) return st;
             a.refresh = 0;
         }

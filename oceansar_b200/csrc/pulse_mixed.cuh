@@ -24,19 +24,23 @@
 // float32 compensation row; the next pulse's row-table kernel (or ocs_pulse_flush) folds
 // that row into the raw row.
 //
-// Input staging: the facet inputs of a warp's 32 columns (fields, sqrt(RCS), scatterer
-// start indices) are moved into a four-row shared-memory ring by one-dimensional bulk
-// copies (cp.async.bulk, one per input array and row, issued by lane 0) that complete on
-// the slot's mbarrier; the warp reads a row once its barrier phase has completed, so warps
-// never wait on each other.  Every mbarrier wait is bounded: a wait that gives up sets the
-// launch's error flag, drains the warp's copies in flight and ends the warp's work.
+// Input staging: the facet inputs of a CTA row (the float32 fields, sqrt(RCS) and
+// scatterer start indices of 128 columns) are moved into a four-row shared-memory ring by
+// tiled tensor copies (cp.async.bulk.tensor: one three-dimensional box for all fields, one
+// per index map and one for the sqrt(RCS) planes) that complete on the slot's mbarrier.
+// The warp that finishes reading a row last refills its slot with the row four ahead, so no
+// warp ever waits for another, only for data.  Every mbarrier wait is bounded: a wait that
+// gives up sets the launch's error flag, lets the copies in flight land and ends the CTA's
+// work.
 #pragma once
+#include <cuda.h>
+
 #include "bulk.cuh"
 
 namespace ocs {
 
 constexpr int kMixCols = 128;       // columns (threads) per CTA, 32 per warp
-constexpr int kMixSlots = 4;        // ring rows per warp (three in flight)
+constexpr int kMixSlots = 4;        // ring rows (three in flight while one is read)
 constexpr int kMixArrays = 14;      // staged input arrays per row (see MixArr)
 constexpr int kMixRT = 8;           // float row-table entries before the channel factors
 constexpr int kMixS = 12;           // register-window slots
@@ -44,6 +48,15 @@ constexpr int kMixNbw = 160;        // CTA shared bin window
 
 // staged arrays: fields, Kodis curvatures, scatterer start indices, sqrt(RCS) [pol][line]
 enum MixArr { kAdx = 0, kAdy, kAdz, kAdiffx, kAdiffy, kAdxx, kAdyy, kAdxy, kAindm, kAindp, kAscat };
+
+// Tensor maps of one launch's inputs: the fields as one [nf][ny][nx] float32 tensor (the
+// surface keeps them in one block, Dx Dy Dz Diffx Diffy [Diffxx Diffyy Diffxy]), the two
+// int32 [ny][nx] scatterer index maps and the [2 npol][ny][nx] sqrt(RCS) planes; every box
+// is one row of kMixCols columns.
+struct alignas(64) MixMaps {
+    CUtensorMap fields, indm, indp, scat;
+    int nf;                         // fields in the fields map (5, or 8 with the curvatures)
+};
 
 // Per-pulse workspace after the float64 row table: float row table [ny][kMixRT + 2 nch]
 // (Bh, Bl, phi_y, sin_az, cos_azp, sin_azp, azp, -, then the channel factors), then the
@@ -169,15 +182,16 @@ template <int NOUT> struct MixSmem {
     float *rt;                      // float row table of the tile [rows][RT]
     double *raz;                    // float64 az, sin_az of the tile's rows [2][rows]
     double *sred;                   // block reduction scratch [32]
-    float *stage;                   // [4 warps][kMixSlots][kMixArrays][32]
-    unsigned long long *bar;        // [4 warps][kMixSlots]
+    float *stage;                   // [kMixSlots][kMixArrays][kMixCols]
+    unsigned long long *bar;        // [kMixSlots] full barriers
+    int *cnt;                       // [kMixSlots] warps done with the slot's row
     int rcap;                       // rows the row tables hold (the largest tile height)
 };
 
 template <int NOUT> OCS_HD size_t mix_smem_bytes(int nch, int rows_cap) {
     return (size_t)wtab_len<float, kMixS>(kSincTaps, kSincOvs) * 4 + (size_t)NOUT * kMixNbw * 2 * 2 * 4 +
            (size_t)rows_cap * (kMixRT + 2 * nch) * 4 + 2 * (size_t)rows_cap * 8 + 32 * 8 +
-           (size_t)4 * kMixSlots * kMixArrays * 32 * 4 + 4 * kMixSlots * 8 + 128;
+           (size_t)kMixSlots * kMixArrays * kMixCols * 4 + kMixSlots * 16 + 256;
 }
 
 template <int NOUT> OCS_D MixSmem<NOUT> mix_smem(unsigned char *smem, int nch, int rows_cap) {
@@ -189,8 +203,9 @@ template <int NOUT> OCS_D MixSmem<NOUT> mix_smem(unsigned char *smem, int nch, i
         off += bytes;
         return p;
     };
-    sm.bar = reinterpret_cast<unsigned long long *>(take(4 * kMixSlots * 8, 8));
-    sm.stage = reinterpret_cast<float *>(take((size_t)4 * kMixSlots * kMixArrays * 32 * 4, 128));
+    sm.bar = reinterpret_cast<unsigned long long *>(take(kMixSlots * 8, 8));
+    sm.cnt = reinterpret_cast<int *>(take(kMixSlots * 4, 4));
+    sm.stage = reinterpret_cast<float *>(take((size_t)kMixSlots * kMixArrays * kMixCols * 4, 128));
     sm.wtab = reinterpret_cast<float *>(take((size_t)wtab_len<float, kMixS>(kSincTaps, kSincOvs) * 4, 16));
     sm.bhi = reinterpret_cast<float *>(take((size_t)NOUT * kMixNbw * 2 * 4, 16));
     sm.blo = reinterpret_cast<float *>(take((size_t)NOUT * kMixNbw * 2 * 4, 16));
@@ -318,8 +333,8 @@ OCS_D double srs_f64(double sr_c, double cos_i, double sin_i, double az, double 
 // One tile of 128 columns x tile_rows rows.  `rseq` is the warp's running row count (ring
 // slot and barrier parity); `bad` becomes true when a bounded wait gave up.
 template <int NOUT, bool KODIS>
-OCS_D void mix_tile(const PulseArgs &a, float *lo_row, int tile, int tile_rows, const MixSmem<NOUT> &sm,
-                    unsigned &rseq, bool &bad, double &spec_sum, double (&bragg_sum)[2]) {
+OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int tile, int tile_rows,
+                    const MixSmem<NOUT> &sm, unsigned &rseq, bool &bad, double &spec_sum, double (&bragg_sum)[2]) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tiles_x = (a.nx + kMixCols - 1) / kMixCols;
     const int x0t = (tile % tiles_x) * kMixCols;
@@ -359,11 +374,11 @@ OCS_D void mix_tile(const PulseArgs &a, float *lo_row, int tile, int tile_rows, 
 
     MixWindow<NOUT> win;
     win.reset();
-    const int xw = x0t + 32 * warp;       // first column of this warp
-    if (xw < a.nx && !bad) {
-        const int ncw = min(32, a.nx - xw);
+    if (!bad) {
+        // every warp takes part in every row (the ring's slots are released per warp);
+        // lanes past the last column stage and wait but compute nothing
         const bool col_ok = x < a.nx;
-        const int xs = col_ok ? x : xw;    // a valid column for lanes past the edge
+        const int xs = col_ok ? x : a.nx - 1;
         // ---- per-column constants (float64 reference quantities, converted once) ----
         const double sr_c = a.sr_col[xs];
         float Ch, Cl;
@@ -392,63 +407,40 @@ OCS_D void mix_tile(const PulseArgs &a, float *lo_row, int tile, int tile_rows, 
             outs |= (unsigned)(c | (p << 3) | (xti ? 16 : 0)) << (5 * k);
             kxti[k] = k < a.nout ? (float)(-a.k0 * a.b_xti[c]) : 0.f;
         }
-        // ---- staging: arrays of this launch and bytes per row ----
-        unsigned amask = (1u << kAdx) | (1u << kAdy) | (1u << kAdz) | (1u << kAdiffx) | (1u << kAdiffy);
-        if (kodis) amask |= (1u << kAdxx) | (1u << kAdyy) | (1u << kAdxy);
-        if (a.do_bragg) amask |= (1u << kAindm) | (1u << kAindp);
-        if (load_scat) amask |= (a.npol == 2 ? 15u : 3u) << kAscat;
-        const unsigned row_bytes = (unsigned)__popc(amask) * (unsigned)ncw * 4u;
-        float *wst = sm.stage + (size_t)warp * kMixSlots * kMixArrays * 32;
-        unsigned long long *wbar = sm.bar + warp * kMixSlots;
+        // ---- staging: tensor copies of whole CTA rows into the ring ----
+        const int nf = maps->nf;
+        const unsigned row_bytes = (unsigned)(nf + (a.do_bragg ? 2 : 0) + (load_scat ? 2 * a.npol : 0)) * kMixCols * 4u;
         const unsigned first = rseq;      // ring position of this tile's row 0
-        unsigned issued = 0;              // rows of this tile issued (lane 0's count)
-        auto issue = [&](int r) {
-            if (lane == 0 && r < nrows) {
-                const unsigned q = first + (unsigned)r;
-                const int slot = (int)(q % kMixSlots);
-                float *dst = wst + (size_t)slot * kMixArrays * 32;
-                unsigned long long *bar = wbar + slot;
-                fence_proxy_async();
-                mbar_expect_tx(bar, row_bytes);
-                const long long idx = (long long)(y0 + r) * a.nx + xw;
-                const unsigned nb = (unsigned)ncw * 4u;
-                bulk_g2s(dst + kAdx * 32, a.dx_f + idx, nb, bar);
-                bulk_g2s(dst + kAdy * 32, a.dy_f + idx, nb, bar);
-                bulk_g2s(dst + kAdz * 32, a.dz_f + idx, nb, bar);
-                bulk_g2s(dst + kAdiffx * 32, a.diffx + idx, nb, bar);
-                bulk_g2s(dst + kAdiffy * 32, a.diffy + idx, nb, bar);
-                if (kodis) {
-                    bulk_g2s(dst + kAdxx * 32, a.diffxx + idx, nb, bar);
-                    bulk_g2s(dst + kAdyy * 32, a.diffyy + idx, nb, bar);
-                    bulk_g2s(dst + kAdxy * 32, a.diffxy + idx, nb, bar);
-                }
-                if (a.do_bragg) {
-                    bulk_g2s(dst + kAindm * 32, a.ind0_m + idx, nb, bar);
-                    bulk_g2s(dst + kAindp * 32, a.ind0_p + idx, nb, bar);
-                }
-                if (load_scat) {
-                    const int ns = 2 * a.npol;
-                    for (int k = 0; k < ns; ++k) bulk_g2s(dst + (kAscat + k) * 32, scat + k * npix + idx, nb, bar);
-                }
-                issued = (unsigned)r + 1;
+        auto slot_of = [&](int r) { return (int)((first + (unsigned)r) % kMixSlots); };
+        auto issue = [&](int r) {         // one thread; the slot of row r is free
+            const int slot = slot_of(r);
+            float *dst = sm.stage + (size_t)slot * kMixArrays * kMixCols;
+            unsigned long long *bar = sm.bar + slot;
+            fence_proxy_async();
+            mbar_expect_tx(bar, row_bytes);
+            const int yy = y0 + r;
+            tma_load_3d(dst + kAdx * kMixCols, &maps->fields, x0t, yy, 0, bar);
+            if (a.do_bragg) {
+                tma_load_2d(dst + kAindm * kMixCols, &maps->indm, x0t, yy, bar);
+                tma_load_2d(dst + kAindp * kMixCols, &maps->indp, x0t, yy, bar);
             }
+            if (load_scat) tma_load_3d(dst + kAscat * kMixCols, &maps->scat, x0t, yy, 0, bar);
         };
         auto wait_row = [&](int r) -> bool {
             const unsigned q = first + (unsigned)r;
-            return mbar_wait(wbar + (q % kMixSlots), (q / kMixSlots) & 1u);
+            return mbar_wait(sm.bar + (q % kMixSlots), (q / kMixSlots) & 1u);
         };
-        issue(0);
-        issue(1);
-        issue(2);
+        if (threadIdx.x == 0)
+            for (int r = 0; r < kMixSlots && r < nrows; ++r) issue(r);
         // gathers of the scatterer series, one row ahead
         float2 gm = {0.f, 0.f}, gp = {0.f, 0.f};
         const float2 *sm32 = reinterpret_cast<const float2 *>(a.s_m32);
         const float2 *sp32 = reinterpret_cast<const float2 *>(a.s_p32);
         auto gather = [&](int r, float2 &m, float2 &p) {
-            const float *src = wst + (size_t)((first + (unsigned)r) % kMixSlots) * kMixArrays * 32;
-            int i0 = __float_as_int(src[kAindm * 32 + lane]) + a.tmod_m;
+            const float *src = sm.stage + (size_t)slot_of(r) * kMixArrays * kMixCols;
+            int i0 = __float_as_int(src[kAindm * kMixCols + threadIdx.x]) + a.tmod_m;
             i0 = i0 >= a.n_m ? i0 - a.n_m : i0;
-            int i1 = __float_as_int(src[kAindp * 32 + lane]) + a.tmod_p;
+            int i1 = __float_as_int(src[kAindp * kMixCols + threadIdx.x]) + a.tmod_p;
             i1 = i1 >= a.n_p ? i1 - a.n_p : i1;
             if (col_ok) {
                 m = __ldg(sm32 + i0);
@@ -456,35 +448,48 @@ OCS_D void mix_tile(const PulseArgs &a, float *lo_row, int tile, int tile_rows, 
             }
         };
         // every lane waits (acquiring the copied data), the warp agrees on the outcome
-        unsigned waited = 0;              // rows 0 .. waited - 1 have completed
+        int fail_row = -1;
         bool ok = __all_sync(0xffffffffu, wait_row(0));
-        if (ok) waited = 1;
+        if (!ok) fail_row = 0;
         if (ok && a.do_bragg) gather(0, gm, gp);
         for (int i = 0; i < nrows && ok; ++i) {
-            // rows i and i + 1 have landed; the slot of row i - 1 is free again
+            // rows i and i + 1 have landed
             if (i + 1 < nrows) {
                 ok = __all_sync(0xffffffffu, wait_row(i + 1));
-                if (!ok) break;
-                waited = (unsigned)i + 2;
+                if (!ok) { fail_row = i + 1; break; }
             }
-            const float *src = wst + (size_t)((first + (unsigned)i) % kMixSlots) * kMixArrays * 32;
-            const float dx = src[kAdx * 32 + lane], dy = src[kAdy * 32 + lane], dz = src[kAdz * 32 + lane];
-            const float diffx = src[kAdiffx * 32 + lane], diffy = src[kAdiffy * 32 + lane];
+            const int slot = slot_of(i);
+            const float *src = sm.stage + (size_t)slot * kMixArrays * kMixCols;
+            const int t = threadIdx.x;
+            const float dx = src[kAdx * kMixCols + t], dy = src[kAdy * kMixCols + t], dz = src[kAdz * kMixCols + t];
+            const float diffx = src[kAdiffx * kMixCols + t], diffy = src[kAdiffy * kMixCols + t];
             float dxx = 0.f, dyy = 0.f, dxy = 0.f;
-            if (kodis) { dxx = src[kAdxx * 32 + lane]; dyy = src[kAdyy * 32 + lane]; dxy = src[kAdxy * 32 + lane]; }
+            if (kodis) {
+                dxx = src[kAdxx * kMixCols + t];
+                dyy = src[kAdyy * kMixCols + t];
+                dxy = src[kAdxy * kMixCols + t];
+            }
             float sc[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
             if (load_scat) {
-                sc[0][0] = src[kAscat * 32 + lane];
-                sc[0][1] = src[(kAscat + 1) * 32 + lane];
+                sc[0][0] = src[kAscat * kMixCols + t];
+                sc[0][1] = src[(kAscat + 1) * kMixCols + t];
                 if (a.npol == 2) {
-                    sc[1][0] = src[(kAscat + 2) * 32 + lane];
-                    sc[1][1] = src[(kAscat + 3) * 32 + lane];
+                    sc[1][0] = src[(kAscat + 2) * kMixCols + t];
+                    sc[1][1] = src[(kAscat + 3) * kMixCols + t];
                 }
             }
             const float2 cm = gm, cp = gp;
             if (a.do_bragg && i + 1 < nrows) gather(i + 1, gm, gp);
+            // release the slot of row i; the last of the four warps refills it with row i + 4
             __syncwarp();
-            issue(i + 3);                 // into the slot of row i - 1
+            if (lane == 0) {
+                __threadfence_block();
+                if (atomicAdd(sm.cnt + slot, 1) == 3) {
+                    sm.cnt[slot] = 0;
+                    __threadfence_block();
+                    if (i + kMixSlots < nrows) issue(i + kMixSlots);
+                }
+            }
             if (!col_ok) continue;
 
             const float *rt = sm.rt + i * RT;
@@ -636,13 +641,13 @@ OCS_D void mix_tile(const PulseArgs &a, float *lo_row, int tile, int tile_rows, 
             if (bin_d > -(1 << 29)) win.add(bin_d - kSincTaps / 2, lut, coef, sm.wtab, a.sinc, cb);
         }
         if (!ok) {
-            // a wait gave up: record it and let the copies this warp issued land before the
-            // shared memory can go away
+            // a wait gave up: record it, and let every copy that may be in flight (rows
+            // fail_row .. fail_row + 3, one per slot) land before the shared memory can go away
             bad = true;
             if (lane == 0) {
                 atomicOr(reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(a.rowtab) +
                                                  mix_hdr_offset(a.ny, a.nch)) + 1, 1);
-                for (unsigned r = waited; r < issued; ++r) wait_row((int)r);
+                for (int r = fail_row; r < fail_row + kMixSlots && r < nrows; ++r) wait_row(r);
             }
             __syncwarp();
         }
@@ -650,45 +655,70 @@ OCS_D void mix_tile(const PulseArgs &a, float *lo_row, int tile, int tile_rows, 
     }
     win.flush(cb);
     __syncthreads();
-    // CTA bins -> raw row (compensated; the rounding errors go to the compensation row)
-    for (int i = threadIdx.x; i < a.nout * kMixNbw; i += blockDim.x) {
-        const int o = i / kMixNbw, lb = i - o * kMixNbw;
-        const int b = cb.cta_base + lb;
-        if (b < 0 || b >= a.nbins) continue;
-        const float hr = sm.bhi[2 * i], lr = sm.blo[2 * i], hi_ = sm.bhi[2 * i + 1], li = sm.blo[2 * i + 1];
-        float *d = cb.out + (long long)o * cb.out_stride + 2 * b;
-        float *l = cb.lo_row ? cb.lo_row + (long long)o * 2 * a.nbins + 2 * b : nullptr;
-        if (hr != 0.f || lr != 0.f) {
-            const float v = __fadd_rn(hr, lr), e0 = two_sum_err(hr, lr, v);
-            const float old = atomicAdd(d, v);
-            const float e = two_sum_err(old, v, __fadd_rn(old, v)) + e0;
-            if (l && e != 0.f) atomicAdd(l, e);
+    // CTA bins -> raw row, compensated: first every returning add of this thread's bins (so
+    // that their round trips overlap), then the rounding errors, as plain reductions, into
+    // the compensation row
+    constexpr int kPer = (NOUT * kMixNbw + kMixCols - 1) / kMixCols;
+    float vr[kPer][2], orv[kPer][2], er[kPer][2];
+    long long off[kPer];
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        const int i = threadIdx.x + k * kMixCols;
+        off[k] = -1;
+        vr[k][0] = vr[k][1] = orv[k][0] = orv[k][1] = er[k][0] = er[k][1] = 0.f;
+        if (i < a.nout * kMixNbw) {
+            const int o = i / kMixNbw, lb = i - o * kMixNbw;
+            const int b = cb.cta_base + lb;
+            if (b >= 0 && b < a.nbins) {
+                off[k] = (long long)o * cb.out_stride + 2 * b;
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    const float h = sm.bhi[2 * i + c], l = sm.blo[2 * i + c];
+                    vr[k][c] = __fadd_rn(h, l);
+                    er[k][c] = two_sum_err(h, l, vr[k][c]);
+                    if (vr[k][c] != 0.f) orv[k][c] = atomicAdd(cb.out + off[k] + c, vr[k][c]);
+                }
+            }
         }
-        if (hi_ != 0.f || li != 0.f) {
-            const float v = __fadd_rn(hi_, li), e0 = two_sum_err(hi_, li, v);
-            const float old = atomicAdd(d + 1, v);
-            const float e = two_sum_err(old, v, __fadd_rn(old, v)) + e0;
-            if (l && e != 0.f) atomicAdd(l + 1, e);
+    }
+    if (cb.lo_row) {
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            if (off[k] < 0) continue;
+            const int i = threadIdx.x + k * kMixCols;
+            const int o = i / kMixNbw, b = cb.cta_base + (i - o * kMixNbw);
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                if (vr[k][c] == 0.f) continue;
+                const float e = two_sum_err(orv[k][c], vr[k][c], __fadd_rn(orv[k][c], vr[k][c])) + er[k][c];
+                if (e != 0.f) atomicAdd(cb.lo_row + (long long)o * 2 * a.nbins + 2 * b + c, e);
+            }
         }
     }
 }
 
+template <int NOUT> OCS_D void mix_init(const MixSmem<NOUT> &sm) {
+    if (threadIdx.x < kMixSlots) {
+        mbar_init(sm.bar + threadIdx.x, 1);
+        sm.cnt[threadIdx.x] = 0;
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    __syncthreads();
+}
+
 template <int NOUT, bool KODIS>
 __global__ void __launch_bounds__(kMixCols, NOUT < 4 ? 4 : 2)
-pulse_mixed_kernel(const __grid_constant__ PulseArgs a, float *lo_row) {
+pulse_mixed_kernel(const __grid_constant__ PulseArgs a, const __grid_constant__ MixMaps maps, float *lo_row) {
     extern __shared__ __align__(128) unsigned char smem[];
     const MixSmem<NOUT> sm = mix_smem<NOUT>(smem, a.nch, kPulseRows);
     build_wtab<float, kMixS>(sm.wtab, a.sinc, kSincTaps, kSincOvs);
-    if ((threadIdx.x & 31) == 0)
-        for (int s = 0; s < kMixSlots; ++s) mbar_init(sm.bar + (threadIdx.x >> 5) * kMixSlots + s, 1);
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    __syncthreads();
+    mix_init<NOUT>(sm);
     const int tiles = ((a.nx + kMixCols - 1) / kMixCols) * ((a.ny + a.tile_rows - 1) / a.tile_rows);
     double spec_sum = 0.0, bragg_sum[2] = {0.0, 0.0};
     unsigned rseq = 0;
     bool bad = false;
     for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x)
-        mix_tile<NOUT, KODIS>(a, lo_row, tile, a.tile_rows, sm, rseq, bad, spec_sum, bragg_sum);
+        mix_tile<NOUT, KODIS>(a, &maps, lo_row, tile, a.tile_rows, sm, rseq, bad, spec_sum, bragg_sum);
     if (a.out0 == 0) {
         if (KODIS) block_atomic_sum(spec_sum, &a.nrcs_spec[a.az_step], sm.sred);
         if (a.do_bragg && a.refresh)

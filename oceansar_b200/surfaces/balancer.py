@@ -40,7 +40,8 @@ class OceanSurfaceBalancer(object):
             self._sets = (surface._fields, surface._fields_b)
         self._lo = 0                            # which field set holds F(t_l)
         self._names = list(surface._fields)
-        self._fields = {n: _device.empty(shape, np.float32) for n in self._names}
+        block = _device.empty((max(1, len(self._names)),) + shape, np.float32)      # contiguous, in order
+        self._fields = {n: block[i] for i, n in enumerate(self._names)}
         self._dst = (ctypes.c_void_p * len(self._names))(*[self._fields[n].data_ptr() for n in self._names])
         self._host_cache = {}
         self.dt = dt

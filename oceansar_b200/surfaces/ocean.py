@@ -241,7 +241,10 @@ class OceanSurface(object):
                 names += GROUPS[g]
         self._out_names = names
         shape = (self.Ny, self.Nx)
-        self._fields = {n: _device.empty(shape, np.float32) for n in names}
+        # one contiguous block, fields in FIELD_NAMES order: the pulse kernel fetches a row
+        # of every field with a single tensor copy
+        block = _device.empty((max(1, len(names)),) + shape, np.float32)
+        self._fields = {n: block[i] for i, n in enumerate(names)}
         raw = []                      # (code, destination tensor, additive key, swell key)
         self._aux = {}
         chop = self.choppy_enable
@@ -434,7 +437,8 @@ class OceanSurface(object):
             raise NotImplementedError('choppy surfaces keep a single field buffer')
         if getattr(self, '_fields_b', None) is None:
             shape = (self.Ny, self.Nx)
-            self._fields_b = {n: _device.empty(shape, np.float32) for n in self._fields}
+            block = _device.empty((max(1, len(self._fields)),) + shape, np.float32)
+            self._fields_b = {n: block[i] for i, n in enumerate(self._fields)}
             self._dsts_b = (ctypes.c_void_p * len(self._raw))(*[self._fields_b[key].data_ptr()
                                                                   for _, _, key, _ in self._raw])
         return self._fields_b
