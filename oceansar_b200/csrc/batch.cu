@@ -37,9 +37,8 @@ struct ocs_batch {
     SlotState *d_slots = nullptr;
     char *d_sargs = nullptr;
     char *d_pargs = nullptr;
-    char *d_maps = nullptr;               // [max_slots] tensor maps (mixed form)
     char *h_stage = nullptr;              // pinned: [max_slots][stage_bytes]
-    size_t sbytes = 0, pbytes = 0, mbytes = 0, stage_bytes = 0;
+    size_t sbytes = 0, pbytes = 0, stage_bytes = 0;
     std::vector<cudaEvent_t> staged;      // per slot: its last staging copies
     std::vector<HostSlot> host;
 };
@@ -50,7 +49,6 @@ static void batch_free(ocs_batch *b) {
     cudaFree(b->d_slots);
     cudaFree(b->d_sargs);
     cudaFree(b->d_pargs);
-    cudaFree(b->d_maps);
     cudaFreeHost(b->h_stage);
     delete b;
 }
@@ -64,14 +62,12 @@ extern "C" int ocs_batch_create(int32_t max_slots, int32_t precision, ocs_batch 
     b->precision = precision;
     b->sbytes = (surface_args_bytes() + 255) & ~(size_t)255;
     b->pbytes = (pulse_args_bytes() + 255) & ~(size_t)255;
-    b->mbytes = (pulse_maps_bytes() + 255) & ~(size_t)255;
-    b->stage_bytes = ((sizeof(SlotState) + 255) & ~(size_t)255) + b->sbytes + b->pbytes + b->mbytes;
+    b->stage_bytes = ((sizeof(SlotState) + 255) & ~(size_t)255) + b->sbytes + b->pbytes;
     b->host.resize(max_slots);
     b->staged.assign(max_slots, nullptr);
     cudaError_t e = cudaMalloc(&b->d_slots, sizeof(SlotState) * max_slots);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_sargs, b->sbytes * max_slots);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_pargs, b->pbytes * max_slots);
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_maps, b->mbytes * max_slots);
     if (e == cudaSuccess) e = cudaMallocHost(&b->h_stage, b->stage_bytes * max_slots);
     for (int i = 0; i < max_slots && e == cudaSuccess; ++i)
         e = cudaEventCreateWithFlags(&b->staged[i], cudaEventDisableTiming);
@@ -124,13 +120,11 @@ extern "C" int ocs_batch_set(ocs_batch *b, int32_t slot, const ocs_scene_desc *s
     char *st_slot = stage;
     char *st_sargs = stage + ((sizeof(SlotState) + 255) & ~(size_t)255);
     char *st_pargs = st_sargs + b->sbytes;
-    char *st_maps = st_pargs + b->pbytes;
     memset(stage, 0, b->stage_bytes);
     int st = surface_args_fill(sd, st_sargs, &h.prog);
     if (st != OCS_OK) return st;
     st = pulse_args_fill(pd, st_pargs);
     if (st != OCS_OK) return st;
-    if (b->precision == OCS_PREC_MIXED && (st = pulse_maps_fill(pd, st_maps)) != OCS_OK) return st;
 
     SlotState s;
     memset(&s, 0, sizeof(s));
@@ -154,14 +148,11 @@ extern "C" int ocs_batch_set(ocs_batch *b, int32_t slot, const ocs_scene_desc *s
     s.tmod_tab = sc->tmod_d;
     s.sargs = b->d_sargs + b->sbytes * slot;
     s.pargs = b->d_pargs + b->pbytes * slot;
-    s.maps = b->d_maps + b->mbytes * slot;
     memcpy(st_slot, &s, sizeof(s));
     cudaStream_t cs = (cudaStream_t)stream;
     cudaError_t e = cudaMemcpyAsync(b->d_sargs + b->sbytes * slot, st_sargs, b->sbytes, cudaMemcpyHostToDevice, cs);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(b->d_pargs + b->pbytes * slot, st_pargs, b->pbytes, cudaMemcpyHostToDevice, cs);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(b->d_maps + b->mbytes * slot, st_maps, b->mbytes, cudaMemcpyHostToDevice, cs);
     // the slot record last: kernels that run after it see complete arguments
     if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_slots + slot, st_slot, sizeof(s), cudaMemcpyHostToDevice, cs);
     if (e == cudaSuccess) e = cudaEventRecord(b->staged[slot], cs);

@@ -41,7 +41,6 @@ struct SlotState {
     const int *tmod_tab;            // [az_steps][2] int(t prf) mod N_m, mod N_p
     const void *sargs;              // SurfaceArgs of the scene (device memory)
     const void *pargs;              // PulseArgs of the scene (device memory)
-    const void *maps;               // tensor maps of the mixed form's inputs (device memory)
 };
 
 struct BatchRef {
@@ -102,9 +101,6 @@ int batch_launch_pulse_rows(const BatchRef &b, int precision, cudaStream_t st);
 // Whether a scene's pulse descriptor takes the split-range mixed kernel (required of every
 // scene of a mixed-precision batch).
 bool pulse_split_ok(const ocs_pulse_desc *d);
-// Tensor maps of the mixed form for a scene (pulse_maps_bytes() bytes, 64-byte aligned out).
-size_t pulse_maps_bytes();
-int pulse_maps_fill(const ocs_pulse_desc *d, void *out);
 int batch_launch_pulse(const BatchRef &b, int precision, int width, int grid, cudaStream_t st);
 // Pulse-kernel items (groups of a width class x facet tiles) of one scene.
 int batch_pulse_items(int nx, int ny, int tile_rows, int nout, int precision, int width);

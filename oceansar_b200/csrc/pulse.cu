@@ -826,8 +826,7 @@ batch_pulse_mixed_kernel(const __grid_constant__ BatchRef b) {
     double spec_sum = 0.0, bragg_sum[2] = {0.0, 0.0};
     unsigned rseq = 0;
     bool bad = false;
-    mix_tile<NOUT, true>(pa, static_cast<const MixMaps *>(g.maps), nullptr, tile, g.tile_rows, sm, rseq, bad,
-                         spec_sum, bragg_sum);
+    mix_tile<NOUT, true, false>(pa, nullptr, nullptr, tile, g.tile_rows, sm, rseq, bad, spec_sum, bragg_sum);
     if (pa.out0 == 0) {
         if (pa.do_kodis) block_atomic_sum(spec_sum, &pa.nrcs_spec[pa.az_step], sm.sred);
         if (pa.do_bragg && pa.refresh)
@@ -885,7 +884,7 @@ static int tile_rows_for(int nx, int ny, int cols, int resident) {
 template <int NOUT, bool KODIS>
 static int launch_pulse_mixed(PulseArgs a, const MixMaps &maps, float *lo_row, cudaStream_t st) {
     const size_t smem = mix_smem_bytes<NOUT>(a.nch, kPulseRows);
-    auto k = pulse_mixed_kernel<NOUT, KODIS>;
+    auto k = a.refresh ? pulse_mixed_kernel<NOUT, KODIS, 1> : pulse_mixed_kernel<NOUT, KODIS, 0>;
     if (ensure_smem((const void *)k, smem) != cudaSuccess) return OCS_ERR_CUDA;
     const int resident = resident_ctas((const void *)k, kMixCols, smem);
     if (resident <= 0) return OCS_ERR_CUDA;
@@ -1164,13 +1163,6 @@ extern "C" int64_t ocs_pulse_workspace_bytes(int32_t ny, int32_t nch) {
 static bool mixed_split_ok(const ocs_pulse_desc *d);
 namespace ocs {
 bool pulse_split_ok(const ocs_pulse_desc *d) { return mixed_split_ok(d); }
-size_t pulse_maps_bytes() { return sizeof(MixMaps); }
-int pulse_maps_fill(const ocs_pulse_desc *d, void *out) {
-    MixMaps m;
-    if (!fill_mix_maps(d, m)) return OCS_ERR_UNSUPPORTED;
-    memcpy(out, &m, sizeof(m));
-    return OCS_OK;
-}
 }  // namespace ocs
 static bool mixed_split_ok(const ocs_pulse_desc *d) {
     if (d->sca || d->skim || (d->do_kodis && d->spec_mode != 0) || !(d->do_kodis || d->do_bragg)) return false;

@@ -332,7 +332,11 @@ OCS_D double srs_f64(double sr_c, double cos_i, double sin_i, double az, double 
 // ---------------------------------------------------------------------------------------
 // One tile of 128 columns x tile_rows rows.  `rseq` is the warp's running row count (ring
 // slot and barrier parity); `bad` becomes true when a bounded wait gave up.
-template <int NOUT, bool KODIS>
+// TMA = false: every thread loads its own column's inputs of a row from global memory at
+// the top of the row (the scene batch, whose slots keep no tensor maps).  REFRESH: 0 = a
+// pulse that reads the stored sqrt(RCS), 1 = a Bragg-refresh pulse (the Romeiser model is
+// compiled only into these), 2 = decided at run time from a.refresh (the scene batch).
+template <int NOUT, bool KODIS, bool TMA = true, int REFRESH = 2>
 OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int tile, int tile_rows,
                     const MixSmem<NOUT> &sm, unsigned &rseq, bool &bad, double &spec_sum, double (&bragg_sum)[2]) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -395,7 +399,8 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
         const float hdx = (float)a.kodis.hdx, hdy = (float)a.kodis.hdy, inv_sr0 = (float)(1.0 / a.sr0);
         const long long npix = (long long)a.nx * a.ny;
         float *scat = reinterpret_cast<float *>(a.scat);
-        const bool load_scat = a.do_bragg && !a.refresh;
+        const bool refresh = REFRESH == 2 ? a.refresh != 0 : REFRESH == 1;
+        const bool load_scat = a.do_bragg && !refresh;
         // outputs of this pass (5 bits each: channel, polarisation, XTI flag)
         unsigned outs = 0;
         float kxti[NOUT];                 // -k0 b_xti of each output's channel
@@ -408,11 +413,12 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
             kxti[k] = k < a.nout ? (float)(-a.k0 * a.b_xti[c]) : 0.f;
         }
         // ---- staging: tensor copies of whole CTA rows into the ring ----
-        const int nf = maps->nf;
+        const int nf = TMA ? maps->nf : 0;
         const unsigned row_bytes = (unsigned)(nf + (a.do_bragg ? 2 : 0) + (load_scat ? 2 * a.npol : 0)) * kMixCols * 4u;
         const unsigned first = rseq;      // ring position of this tile's row 0
         auto slot_of = [&](int r) { return (int)((first + (unsigned)r) % kMixSlots); };
         auto issue = [&](int r) {         // one thread; the slot of row r is free
+            if constexpr (!TMA) return;
             const int slot = slot_of(r);
             float *dst = sm.stage + (size_t)slot * kMixArrays * kMixCols;
             unsigned long long *bar = sm.bar + slot;
@@ -427,20 +433,30 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
             if (load_scat) tma_load_3d(dst + kAscat * kMixCols, &maps->scat, x0t, yy, 0, bar);
         };
         auto wait_row = [&](int r) -> bool {
+            if constexpr (!TMA) return true;
             const unsigned q = first + (unsigned)r;
             return mbar_wait(sm.bar + (q % kMixSlots), (q / kMixSlots) & 1u);
         };
-        if (threadIdx.x == 0)
+        if (TMA && threadIdx.x == 0)
             for (int r = 0; r < kMixSlots && r < nrows; ++r) issue(r);
         // gathers of the scatterer series, one row ahead
         float2 gm = {0.f, 0.f}, gp = {0.f, 0.f};
         const float2 *sm32 = reinterpret_cast<const float2 *>(a.s_m32);
         const float2 *sp32 = reinterpret_cast<const float2 *>(a.s_p32);
         auto gather = [&](int r, float2 &m, float2 &p) {
-            const float *src = sm.stage + (size_t)slot_of(r) * kMixArrays * kMixCols;
-            int i0 = __float_as_int(src[kAindm * kMixCols + threadIdx.x]) + a.tmod_m;
+            int i0, i1;
+            if constexpr (TMA) {
+                const float *src = sm.stage + (size_t)slot_of(r) * kMixArrays * kMixCols;
+                i0 = __float_as_int(src[kAindm * kMixCols + threadIdx.x]);
+                i1 = __float_as_int(src[kAindp * kMixCols + threadIdx.x]);
+            } else {
+                const long long g = (long long)(y0 + r) * a.nx + xs;
+                i0 = __ldg(a.ind0_m + g);
+                i1 = __ldg(a.ind0_p + g);
+            }
+            i0 += a.tmod_m;
             i0 = i0 >= a.n_m ? i0 - a.n_m : i0;
-            int i1 = __float_as_int(src[kAindp * kMixCols + threadIdx.x]) + a.tmod_p;
+            i1 += a.tmod_p;
             i1 = i1 >= a.n_p ? i1 - a.n_p : i1;
             if (col_ok) {
                 m = __ldg(sm32 + i0);
@@ -459,30 +475,45 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
                 if (!ok) { fail_row = i + 1; break; }
             }
             const int slot = slot_of(i);
-            const float *src = sm.stage + (size_t)slot * kMixArrays * kMixCols;
-            const int t = threadIdx.x;
-            const float dx = src[kAdx * kMixCols + t], dy = src[kAdy * kMixCols + t], dz = src[kAdz * kMixCols + t];
-            const float diffx = src[kAdiffx * kMixCols + t], diffy = src[kAdiffy * kMixCols + t];
-            float dxx = 0.f, dyy = 0.f, dxy = 0.f;
-            if (kodis) {
-                dxx = src[kAdxx * kMixCols + t];
-                dyy = src[kAdyy * kMixCols + t];
-                dxy = src[kAdxy * kMixCols + t];
-            }
+            float dx, dy, dz, diffx, diffy, dxx = 0.f, dyy = 0.f, dxy = 0.f;
             float sc[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
-            if (load_scat) {
-                sc[0][0] = src[kAscat * kMixCols + t];
-                sc[0][1] = src[(kAscat + 1) * kMixCols + t];
-                if (a.npol == 2) {
-                    sc[1][0] = src[(kAscat + 2) * kMixCols + t];
-                    sc[1][1] = src[(kAscat + 3) * kMixCols + t];
+            if constexpr (TMA) {
+                const float *src = sm.stage + (size_t)slot * kMixArrays * kMixCols;
+                const int t = threadIdx.x;
+                dx = src[kAdx * kMixCols + t]; dy = src[kAdy * kMixCols + t]; dz = src[kAdz * kMixCols + t];
+                diffx = src[kAdiffx * kMixCols + t]; diffy = src[kAdiffy * kMixCols + t];
+                if (kodis) {
+                    dxx = src[kAdxx * kMixCols + t];
+                    dyy = src[kAdyy * kMixCols + t];
+                    dxy = src[kAdxy * kMixCols + t];
+                }
+                if (load_scat) {
+                    sc[0][0] = src[kAscat * kMixCols + t];
+                    sc[0][1] = src[(kAscat + 1) * kMixCols + t];
+                    if (a.npol == 2) {
+                        sc[1][0] = src[(kAscat + 2) * kMixCols + t];
+                        sc[1][1] = src[(kAscat + 3) * kMixCols + t];
+                    }
+                }
+            } else {
+                const long long g = (long long)(y0 + i) * a.nx + xs;
+                dx = __ldg(a.dx_f + g); dy = __ldg(a.dy_f + g); dz = __ldg(a.dz_f + g);
+                diffx = __ldg(a.diffx + g); diffy = __ldg(a.diffy + g);
+                if (kodis) { dxx = __ldg(a.diffxx + g); dyy = __ldg(a.diffyy + g); dxy = __ldg(a.diffxy + g); }
+                if (load_scat) {
+                    sc[0][0] = __ldg(scat + g);
+                    sc[0][1] = __ldg(scat + npix + g);
+                    if (a.npol == 2) {
+                        sc[1][0] = __ldg(scat + 2 * npix + g);
+                        sc[1][1] = __ldg(scat + 3 * npix + g);
+                    }
                 }
             }
             const float2 cm = gm, cp = gp;
             if (a.do_bragg && i + 1 < nrows) gather(i + 1, gm, gp);
             // release the slot of row i; the last of the four warps refills it with row i + 4
             __syncwarp();
-            if (lane == 0) {
+            if (TMA && lane == 0) {
                 __threadfence_block();
                 if (atomicAdd(sm.cnt + slot, 1) == 3) {
                     sm.cnt[slot] = 0;
@@ -566,7 +597,7 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
                 }
             }
             if (a.do_bragg) {
-                if (a.refresh) {
+                if (REFRESH != 0 && refresh) {
                     float hh[2], vv[2];
                     const int y = y0 + i;
                     if (a.lut) {
@@ -706,7 +737,7 @@ template <int NOUT> OCS_D void mix_init(const MixSmem<NOUT> &sm) {
     __syncthreads();
 }
 
-template <int NOUT, bool KODIS>
+template <int NOUT, bool KODIS, int REFRESH>
 __global__ void __launch_bounds__(kMixCols, NOUT < 4 ? 4 : 2)
 pulse_mixed_kernel(const __grid_constant__ PulseArgs a, const __grid_constant__ MixMaps maps, float *lo_row) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -718,7 +749,7 @@ pulse_mixed_kernel(const __grid_constant__ PulseArgs a, const __grid_constant__ 
     unsigned rseq = 0;
     bool bad = false;
     for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x)
-        mix_tile<NOUT, KODIS>(a, &maps, lo_row, tile, a.tile_rows, sm, rseq, bad, spec_sum, bragg_sum);
+        mix_tile<NOUT, KODIS, true, REFRESH>(a, &maps, lo_row, tile, a.tile_rows, sm, rseq, bad, spec_sum, bragg_sum);
     if (a.out0 == 0) {
         if (KODIS) block_atomic_sum(spec_sum, &a.nrcs_spec[a.az_step], sm.sred);
         if (a.do_bragg && a.refresh)
