@@ -320,6 +320,47 @@ template <int NOUT> struct MixWindow {
     }
 };
 
+// Tile-end flush of a warp's 32 register windows without contention: every lane writes its
+// window (one output at a time) into the warp's scratch, then lane l sums bin lo + l (and
+// every 32nd after it) over the lanes whose windows cover it, in lane order, and makes one
+// compensated add into the CTA bins -- the lanes of a warp never add to the same bin.
+// scr: per-warp [32][kMixS][2] floats; sbase: per-warp [32] ints.  All 32 lanes call it.
+template <int NOUT>
+OCS_D void warp_flush(MixWindow<NOUT> &win, MixBins<NOUT> &cb, float *scr, int *sbase) {
+    const int lane = threadIdx.x & 31;
+    int lo = win.live ? win.base + win.lo : 0x3fffffff;
+    int hi = win.live ? win.base + win.hi : -0x3fffffff;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if (hi < lo) return;                  // no live window in the warp
+    sbase[lane] = win.live ? win.base : -0x3fffffff;
+#pragma unroll
+    for (int o = 0; o < NOUT; ++o) {
+#pragma unroll
+        for (int sl = 0; sl < kMixS; ++sl) {
+            scr[(lane * kMixS + sl) * 2] = win.re[o][sl];
+            scr[(lane * kMixS + sl) * 2 + 1] = win.im[o][sl];
+        }
+        __syncwarp();
+        for (int b = lo + lane; b <= hi; b += 32) {
+            float sr = 0.f, si = 0.f;
+            for (int j = 0; j < 32; ++j) {
+                const int off = b - sbase[j];
+                if (off >= 0 && off < kMixS) {
+                    sr += scr[(j * kMixS + off) * 2];
+                    si += scr[(j * kMixS + off) * 2 + 1];
+                }
+            }
+            cb.add(o, b, sr, si);
+        }
+        __syncwarp();
+    }
+    win.reset();
+}
+
 // Float64 slant range of one facet exactly as the drop-in computes it (no contraction).
 OCS_D double srs_f64(double sr_c, double cos_i, double sin_i, double az, double sin_az, float dx, float dy,
                      float dz) {
@@ -684,7 +725,14 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
         }
         rseq = first + (unsigned)nrows;
     }
-    win.flush(cb);
+    // every warp is past its last row: the ring holds no live data, its memory is the
+    // flush scratch
+    __syncthreads();
+    {
+        float *scr = sm.stage + (size_t)(threadIdx.x >> 5) * 32 * kMixS * 2;
+        int *sbase = reinterpret_cast<int *>(sm.stage + (size_t)4 * 32 * kMixS * 2) + 32 * (threadIdx.x >> 5);
+        warp_flush<NOUT>(win, cb, scr, sbase);
+    }
     __syncthreads();
     // CTA bins -> raw row, compensated: first every returning add of this thread's bins (so
     // that their round trips overlap), then the rounding errors, as plain reductions, into
