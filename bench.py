@@ -381,6 +381,38 @@ def accumulation_roofline(peak, peak_src, n=4096, nbins=2048, reps=10):
     return out
 
 
+def fma_rates(iters=4096, reps=5):
+    """FMA throughput of the device in float64, float32 and packed float32x2
+    (``ocs_fma_rate``: 8 independent chains per thread, 148 x 16 CTAs of 256 threads), as
+    TFLOP/s (2 flops per FMA), and the float64 : float32 ratio that bounds what moving
+    per-facet work from float64 to float32 can gain."""
+    import ctypes
+    import torch
+    from oceansar_b200 import _capi
+    lib = _capi.load()
+    props = torch.cuda.get_device_properties(torch.cuda.current_device())
+    blocks, threads = props.multi_processor_count * 16, 256
+    sink = torch.zeros(blocks, device="cuda", dtype=torch.float32)
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    out = {}
+    for kind, name, lanes in ((0, "f64", 1), (1, "f32", 1), (2, "f32x2", 2)):
+        for _ in range(2):
+            assert lib.ocs_fma_rate(kind, blocks, threads, iters, sink.data_ptr(), st) == 0
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            lib.ocs_fma_rate(kind, blocks, threads, iters, sink.data_ptr(), st)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        flops = 2.0 * blocks * threads * iters * 8 * lanes
+        out[name + "_tflops"] = round(flops / (ms * 1e-3) / 1e12, 2)
+    out["f32_over_f64"] = round(max(out["f32_tflops"], out["f32x2_tflops"]) / out["f64_tflops"], 2)
+    out["kernel"] = "fma_rate_kernel (8 independent FMA chains per thread)"
+    return out
+
+
 # ----------------------------------------------------------------------------------------
 # Batched and serving workloads (one GPU; replicas for N > 1 as for the default workload)
 def _workload_reference(specs, what):
@@ -632,7 +664,7 @@ def main():
     if args.accumulation_only:
         import torch
         torch.cuda.set_device(dist_info()[2])
-        print(json.dumps({"accumulation": accumulation_roofline(*peak_hbm())}), flush=True)
+        print(json.dumps({"accumulation": accumulation_roofline(*peak_hbm()), "fp_rates": fma_rates()}), flush=True)
         return
     c = C1 if args.small else SCENES[args.workload]
     tmpd = tempfile.mkdtemp(prefix="ocs_bench_")
@@ -774,10 +806,11 @@ def main():
                             "mixed_vs_f64": {"rel_l2": 1e-4, "max_phase_rad": 1e-3}})
 
     # ---- standalone accumulation, batched and serving workloads -----------------------------
-    accum = batched = serving = None
+    accum = batched = serving = rates = None
     if extras:
         from oceansar_b200.tune import Autotuner
         accum = accumulation_roofline(peak, peak_src)
+        rates = fma_rates()
         tuner = Autotuner()
         try:
             batched = batched_report(prep, tuner, args.precision)
@@ -798,7 +831,7 @@ def main():
                            "l2": "inputs larger than L2 (~0.5 GB working set)",
                            "graph": "whole scene replayed from one CUDA graph"},
                 "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
-                "cpu_baseline": cpu, "parity": parity or None, "fp64": fp64, "accumulation": accum,
+                "cpu_baseline": cpu, "parity": parity or None, "fp64": fp64, "fp_rates": rates, "accumulation": accum,
                 "batched": batched, "serving": serving}
         print(json.dumps(line), flush=True)
     if world > 1:

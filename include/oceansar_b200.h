@@ -276,6 +276,12 @@ typedef struct {
      * into the raw row by the next pulse's launch or by ocs_pulse_flush.  NULL: the raw row
      * is accumulated with plain float32 atomics. */
     void *raw_lo_d;
+    /* SKIM calibration target (oceansar/radarsim/skim_raw.py:151-164, 490-493, 608-615):
+     * pt_mode 0 none, 1 floating, 2 fixed.  The scene value of facet (pt_y, pt_x) becomes
+     * pt_amp exp(-2 i k0 r) of its phase range r (before the antenna pattern); a fixed
+     * target also takes that facet's displacements Dx, Dy, Dz as zero.  SKIM mode only. */
+    int32_t pt_mode, pt_x, pt_y;
+    double pt_amp;
 } ocs_pulse_desc;
 
 /* Workspace of ocs_pulse (per-pulse float64 and float32 tables of the row quantities and
@@ -317,6 +323,13 @@ int ocs_pulse_error(const ocs_pulse_desc *desc);
  * (complex128 [M][R]).  D_d: complex128 [M] scratch.  Float64 throughout. */
 int ocs_skim_upsample(const double *x_d, const double *dop_d, double *y_d, double *D_d, int32_t N, int32_t G,
                       int32_t R, int32_t n_up, double prf, void *stream);
+
+/* Arithmetic-rate probe (no reference counterpart; a diagnostic of the device the two
+ * precision forms run on): `blocks` x `threads` threads each run iters x 8 independent
+ * FMAs in float64 (kind 0), float32 (kind 1) or packed float32x2 (kind 2, two FMAs per
+ * instruction).  sink: >= blocks floats, not written in practice.  The caller times the
+ * launch on `stream`. */
+int ocs_fma_rate(int32_t kind, int32_t blocks, int32_t threads, int32_t iters, float *sink, void *stream);
 
 /* ------------------------------------------------------------------------------------
  * Standalone NRCS models (float64).

@@ -54,6 +54,7 @@ SIGNATURES = {
     "ocs_field_ka": [c_ptr, c_ptr],
     "ocs_skim_upsample": [c_ptr, c_ptr, c_ptr, c_ptr, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                           ctypes.c_int32, c_dbl, c_ptr],
+    "ocs_fma_rate": [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_ptr, c_ptr],
     "ocs_rd_rcmc": [c_ptr, c_i64, ctypes.c_int32, ctypes.c_int32, c_ptr, c_ptr, c_dbl, c_ptr],
     "ocs_rd_azfilter": [c_ptr, c_i64, ctypes.c_int32, ctypes.c_int32, c_ptr, c_ptr],
     "ocs_batch_create": [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(c_ptr)],

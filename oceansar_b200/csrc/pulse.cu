@@ -100,6 +100,8 @@ struct PulseArgs {
     int skim, ny_integ, s_int;              // SKIM mode: output row per ny_integ facet rows
     int skim_az2, skim_rcm;                 // SKIM: az/2 sin_az in the phase range / in the bins only
     double atx, arx;                        // SKIM: antenna lengths / wavelength (tx, rx)
+    int pt_mode, pt_x, pt_y;                // SKIM calibration target: 0 none, 1 floating, 2 fixed
+    double pt_amp;
 };
 
 // Kirchhoff specular term of one facet and polarisation code pc (0 = hh, 1 = vv),
@@ -465,6 +467,13 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
             }
             cur.read(a, st, slot_i, load_scat);
             slot_i = slot_n;
+            // SKIM calibration target: a fixed one sits at zero displacement (skim_raw.py:490-493)
+            const bool pt_here = (MODE & kModeSkim) && a.pt_mode != 0 && y0 + i == a.pt_y && x == a.pt_x;
+            if (pt_here && a.pt_mode == 2) {
+                cur.dx = 0.f;
+                cur.dy = 0.f;
+                cur.dz = 0.f;
+            }
             const double az = sm.r_az[i];
             // SKIM: sin_az = az / sr of this facet's column (skim_raw.py:486)
             const double sin_az = (MODE & kModeSkim) ? ddiv(az, sr_c) : sm.r_az[RCAP + i];
@@ -594,6 +603,13 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
                         scene[p] = cadd(scene[p], lb);
                     }
                 }
+            }
+            if (pt_here) {
+                // the target replaces the facet's scene value: pt_amp exp(-2 i k0 r)
+                // (skim_raw.py:608-615), float64 like the reference's complex128 scene
+                double ps, pc;
+                sincos((-two_k0) * srs, &ps, &pc);
+                for (int p = 0; p < a.npol; ++p) scene[p] = {(T)(a.pt_amp * pc), (T)(a.pt_amp * ps)};
             }
             // channels of this pass: antenna pattern x ATI phase (per row) x XTI phase
             cplx<T> coef[NOUT];
@@ -1047,6 +1063,11 @@ static int fill_pulse_args(const ocs_pulse_desc *d, PulseArgs &a) {
         a.s_int = d->ny / d->skim_ny_integ;
         a.skim_az2 = d->skim_az2 != 0;
         a.skim_rcm = d->skim_rcm != 0;
+        if (d->pt_mode < 0 || d->pt_mode > 2) return OCS_ERR_ARG;
+        a.pt_mode = d->pt_mode;
+        a.pt_x = d->pt_x;
+        a.pt_y = d->pt_y;
+        a.pt_amp = d->pt_amp;
         a.atx = a.ltx_over_l;
         a.arx = a.lrx_over_l;
         a.raw_out_stride = (long long)d->az_steps * a.s_int * d->nbins;

@@ -18,8 +18,9 @@ azimuth.  Compared with ``sar_raw`` its loop differs in these ways, all reproduc
 The device does the surface, the row table and one pulse-kernel launch per simulated step
 (the SKIM mode of ``ocs_pulse``, which writes the row-group profiles directly); the host
 does the set-up in the reference's order (same RNG stream), calibration and noise; the
-up-sampling and Doppler of the two-scale form run on the device (``ocs_skim_upsample``).  Not built: calibration targets
-(``sim.cal_targets``) and buoy-spectrum input, which raise ``NotImplementedError``.
+up-sampling and Doppler of the two-scale form run on the device (``ocs_skim_upsample``).  The
+calibration target (``sim.cal_targets``) is the pulse kernel's centre-facet substitution.
+Not built: buoy-spectrum input, which raises ``NotImplementedError``.
 """
 import ctypes
 
@@ -81,9 +82,10 @@ class SkimGenerator(object):
         if seed is not None:
             np.random.seed(seed)
         srg, radar, oc = cfg.srg, cfg.radar, cfg.ocean
-        if hasattr(cfg, 'sim') and getattr(cfg.sim, 'cal_targets', False) is not False \
-                and hasattr(cfg.sim, 'cal_targets'):
-            raise NotImplementedError('calibration targets are not built')
+        # calibration target at the scene centre (skim_raw.py:151-164): absent or False:
+        # none; 'floating' (any case): moves with the surface; any other string: fixed
+        cal = getattr(cfg.sim, 'cal_targets', False) if hasattr(cfg, 'sim') else False
+        self.pt_mode = 0 if cal is False else (1 if str(cal).lower() == 'floating' else 2)
         self.wh_tol, self.nesz = srg.wh_tol, srg.nesz
         self.use_hmtf = bool(srg.use_hmtf)
         self.scat_spec_enable = bool(srg.scat_spec_enable)
@@ -296,6 +298,8 @@ class SkimGenerator(object):
         d.skim, d.skim_ny_integ = 1, self.ny_integ
         d.skim_az2 = int(not self.two_scale)
         d.skim_rcm = int(self.rcm)
+        d.pt_mode = self.pt_mode
+        d.pt_x, d.pt_y, d.pt_amp = int(s.Nx / 2), int(s.Ny / 2), 1000.0
         nb = _capi.load().ocs_pulse_workspace_bytes(s.Ny, 1)
         self._rowtab = torch.empty(int(nb), dtype=torch.uint8, device=_device.device())
         d.rowtab_d = self._rowtab.data_ptr()

@@ -10,7 +10,8 @@ geometry and accumulation restatements:
   ``sr_prof`` and the reference Doppler, the two-scale Doppler decimation (``n_pulses_b``,
   ``ny_integ``, ``dop0``), Kodis or Kirchhoff specular, scatterer series at the PRF and
   the Romeiser model with its constructor defaults (LUT mode);
-* the loop ``:465-684`` and the post-processing ``:686-773`` (up-sampling, truncation,
+* the loop ``:465-684`` (with the calibration target of ``:151-164``, ``:490-493`` and
+  ``:608-615``) and the post-processing ``:686-773`` (up-sampling, truncation,
   calibration, noise).
 """
 import numpy as np
@@ -54,6 +55,11 @@ class SkimSim:
         if seed is not None:
             np.random.seed(seed)
         srg, radar, oc = cfg.srg, cfg.radar, cfg.ocean
+        # calibration target (skim_raw.py:151-164)
+        self.add_point_target, self.point_target_floats = False, True
+        if hasattr(cfg, 'sim') and hasattr(cfg.sim, 'cal_targets') and cfg.sim.cal_targets is not False:
+            self.add_point_target = True
+            self.point_target_floats = cfg.sim.cal_targets.lower() == 'floating'
         self.wh_tol, self.nesz = srg.wh_tol, srg.nesz
         self.use_hmtf = srg.use_hmtf
         self.scat_spec_enable, self.scat_spec_mode = srg.scat_spec_enable, srg.scat_spec_mode
@@ -179,6 +185,11 @@ class SkimSim:
         s.set_t(t_now)
         sin_az = az / self.sr
         az_proj_angle = np.arcsin(az / self.gr0)
+        pt_y, pt_x = int(s.Ny / 2), int(s.Nx / 2)
+        if not self.point_target_floats:                      # skim_raw.py:490-493
+            s.Dx[pt_y, pt_x] = 0
+            s.Dy[pt_y, pt_x] = 0
+            s.Dz[pt_y, pt_x] = 0
         if self.two_scale:
             sr_surface = self.sr - self.cos_inc * s.Dz + s.Dx * self.sin_inc + s.Dy * sin_az
             sr_surface4rcm = sr_surface + az / 2 * sin_az if self.rcm else sr_surface
@@ -239,6 +250,10 @@ class SkimSim:
                 scene_hh += np.sum(scat_bragg_hh * np.exp(1j * self.phase_bragg) * self.bragg_scats, axis=0)
             if self.do_vv:
                 scene_vv += np.sum(scat_bragg_vv * np.exp(1j * self.phase_bragg) * self.bragg_scats, axis=0)
+        if self.add_point_target:                             # skim_raw.py:608-615
+            pt = 1000 * np.exp(-1j * 2 * self.k0 * sr_surface[pt_y, pt_x])
+            scene_hh[pt_y, pt_x] = pt
+            scene_vv[pt_y, pt_x] = pt
         if self.L_total:
             beam_pattern = sinc_1tx_nrx(sin_az, self.ant_L * self.num_ch, self.f0, self.num_ch, field=True)
         else:

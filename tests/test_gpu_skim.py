@@ -33,10 +33,10 @@ def max_phase(a, b):
     return np.max(np.abs(np.angle(a[mask] * np.conj(b[mask]))))
 
 
-def stagewise(name, precision):
+def stagewise(name, precision, cfg=None):
     from oceansar_b200.radarsim.skim_raw import SkimGenerator
     from oracle.skim_raw import SkimSim
-    cfg = os.path.join(G, "cfg", name + ".cfg")
+    cfg = cfg or os.path.join(G, "cfg", name + ".cfg")
     osim = SkimSim(cfg, seed=0)
     gen = SkimGenerator(cfg, precision=precision, seed=0)
     assert (gen.steps, gen.rg_samp) == (osim.az_steps_, osim.rg_samp)
@@ -68,6 +68,24 @@ def test_stagewise_mixed(name):
     e, ph = rel_l2(prof, ref), max_phase(prof, ref)
     assert e < 1e-4 and ph < 1e-3, (e, ph)
     np.testing.assert_allclose(nrcs_avg, nref, rtol=1e-5)
+
+
+@pytest.mark.parametrize("name", ["skim1", "skim3"])
+@pytest.mark.parametrize("mode", ["floating", "fixed"])
+def test_calibration_target_stagewise(name, mode, tmp_path):
+    """sim.cal_targets (skim_raw.py:151-164, 490-493, 608-615): the centre facet's scene
+    value is replaced by 1000 exp(-2 i k0 r), and a fixed target is taken at zero
+    displacement.  Two-scale (skim1) and single-scale (skim3) forms, FP64 bar 1e-10; the
+    target must change the profiles (a kernel that ignored it would fail)."""
+    text = open(os.path.join(G, "cfg", name + ".cfg")).read()
+    cfg = tmp_path / (name + "_cal.cfg")
+    cfg.write_text(text.replace("[sim]\n", "[sim]\ncal_targets=%s\n" % mode, 1))
+    prof, ref, nrcs_avg, nref = stagewise(name, "f64", str(cfg))
+    assert prof.shape == ref.shape
+    assert rel_l2(prof, ref) < 1e-10, rel_l2(prof, ref)
+    np.testing.assert_allclose(nrcs_avg, nref, rtol=1e-9)
+    _, plain, _, _ = stagewise(name, "f64")
+    assert rel_l2(plain, ref) > 1e-3
 
 
 @pytest.mark.parametrize("name", CASES)
