@@ -254,7 +254,9 @@ typedef struct {
      * az_f32 = 1: the azimuth residual az_now is a float32 value and the row azimuth is the
      * float32 difference y - az_now (the reference's numpy promotion when the grid step is
      * float32 and the residual is not a float64 scalar).
-     * Requires nch = 1, Kodis (spec_mode 0), no LUT, no hMTF.  The scene batch rejects it. */
+     * Requires nch = 1, Kodis (spec_mode 0), no LUT; hMTF (use_hmtf) is read at the rolled
+     * row of the [ny][field_nx] surface and not clipped (the DopSCA generator's weighting,
+     * dopsca_raw.py:461-472).  The scene batch rejects it. */
     int32_t sca;
     int32_t field_nx, roll;
     double sr_bin_offset, cap_t;

@@ -115,11 +115,15 @@ constexpr int kC2Nbw = 256;
 // Register-batched form of the two-dimensional accumulation: persistent CTAs walk tiles
 // of kC2Cols columns x tile_rows rows; every thread loads the slant ranges and scene
 // values of its column for kRB rows at once (2 kRB independent coalesced loads in flight
-// per thread) and then runs them through its register window.
-constexpr int kRB = 8;
+// per thread) and then runs them through its register window.  The kernel is bound by
+// the latency of each facet's dependent chain (bin -> weight row -> multiply-adds), so
+// resident warps count most: single precision runs 4-row batches at 6 CTAs per SM
+// (within 80 registers), float64 8-row batches at 4 (its window takes twice the registers).
+template <typename T> __host__ __device__ constexpr int rows_per_batch() { return sizeof(T) == 4 ? 4 : 8; }
+template <typename T> __host__ __device__ constexpr int ctas_per_sm_2d() { return sizeof(T) == 4 ? 6 : 4; }
 
 template <typename T, int S>
-__global__ void __launch_bounds__(kC2Cols, 4)
+__global__ void __launch_bounds__(kC2Cols, ctas_per_sm_2d<T>())
 chan_profile_2d_regs_kernel(const double *__restrict__ srg, const cplx<T> *__restrict__ scene, int ny, int nx,
                             double binsize, double min_sr, const float *__restrict__ sinc, int taps, int ovs,
                             T *__restrict__ out, int nbins, int tile_rows) {
@@ -156,6 +160,7 @@ chan_profile_2d_regs_kernel(const double *__restrict__ srg, const cplx<T> *__res
         win.reset();
         if (x < nx) {
             const long long g0 = (long long)y0 * nx + x;
+            constexpr int kRB = rows_per_batch<T>();
             for (int i0 = 0; i0 < nrows; i0 += kRB) {
                 double sr[kRB];
                 cplx<T> c[kRB];

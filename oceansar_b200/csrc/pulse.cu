@@ -544,8 +544,18 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
                                           (T)sm.r_az[4 * RCAP + i], (T)cur.diffx, (T)cur.diffy, hh, vv);
                     }
                     if (a.use_hmtf) {
-                        float hm = a.hmtf[idx];
-                        hm = hm < -1.f ? -1.f : hm;
+                        float hm;
+                        if constexpr (MODE == kModeSca) {
+                            // the scatterometer generator weights by 1 + hMTF of the rolled
+                            // row, unclipped (its clipping writes land in the unrolled surface,
+                            // dopsca_raw.py:463-472)
+                            long long ridx_h, fidx_h;
+                            row_index(i, ridx_h, fidx_h);
+                            hm = a.hmtf[fidx_h];
+                        } else {
+                            hm = a.hmtf[idx];
+                            hm = hm < -1.f ? -1.f : hm;
+                        }
                         const T f = (T)(1.f + hm);
                         hh[0] *= f; hh[1] *= f; vv[0] *= f; vv[1] *= f;
                     }
@@ -900,7 +910,12 @@ static int tile_rows_for(int nx, int ny, int cols, int resident) {
 template <int NOUT, bool KODIS>
 static int launch_pulse_mixed(PulseArgs a, const MixMaps &maps, float *lo_row, cudaStream_t st) {
     const size_t smem = mix_smem_bytes<NOUT>(a.nch, kPulseRows);
-    auto k = a.refresh ? pulse_mixed_kernel<NOUT, KODIS, 1> : pulse_mixed_kernel<NOUT, KODIS, 0>;
+    // the common configuration (one polarisation, no XTI phase, every output in this pass,
+    // Kodis and direct Romeiser Bragg, no hMTF) runs an instantiation with those fixed
+    const bool fast = KODIS && a.do_kodis && a.do_bragg && a.npol == 1 && !a.any_xti && a.nout == NOUT && !a.lut &&
+                      !a.use_hmtf;
+    auto k = fast ? (a.refresh ? pulse_mixed_kernel<NOUT, KODIS, 1, KODIS> : pulse_mixed_kernel<NOUT, KODIS, 0, KODIS>)
+                  : (a.refresh ? pulse_mixed_kernel<NOUT, KODIS, 1> : pulse_mixed_kernel<NOUT, KODIS, 0>);
     if (ensure_smem((const void *)k, smem) != cudaSuccess) return OCS_ERR_CUDA;
     const int resident = resident_ctas((const void *)k, kMixCols, smem);
     if (resident <= 0) return OCS_ERR_CUDA;
@@ -1074,11 +1089,12 @@ static int fill_pulse_args(const ocs_pulse_desc *d, PulseArgs &a) {
         a.raw_row = (long long)d->az_step * a.s_int * d->nbins;
     }
     if (d->sca) {
-        // scatterometer mode: one channel, Kodis specular, direct Bragg model, no hMTF; the
-        // columns are whole range blocks of field_nx columns; the Bragg RCS is evaluated on
-        // every launch and not stored
+        // scatterometer mode: one channel, Kodis specular, direct Bragg model (hMTF, when on,
+        // read at the rolled row of the [ny][field_nx] surface, unclipped); the columns are
+        // whole range blocks of field_nx columns; the Bragg RCS is evaluated on every launch
+        // and not stored
         if (d->nch != 1 || d->field_nx < 1 || d->nx % d->field_nx != 0 || d->roll < 0 || d->roll >= d->ny ||
-            d->use_hmtf || a.spec_mode != 0 || d->lut_d)
+            a.spec_mode != 0 || d->lut_d)
             return OCS_ERR_ARG;
         if (!(d->sr_bin_offset >= 0.0) || !(d->cap_t >= 0.0)) return OCS_ERR_ARG;
         if (d->nrcs_rows < 1 || d->nrcs_row < 0 || d->nrcs_row >= d->nrcs_rows) return OCS_ERR_ARG;

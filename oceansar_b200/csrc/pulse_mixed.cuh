@@ -377,7 +377,7 @@ OCS_D double srs_f64(double sr_c, double cos_i, double sin_i, double az, double 
 // the top of the row (the scene batch, whose slots keep no tensor maps).  REFRESH: 0 = a
 // pulse that reads the stored sqrt(RCS), 1 = a Bragg-refresh pulse (the Romeiser model is
 // compiled only into these), 2 = decided at run time from a.refresh (the scene batch).
-template <int NOUT, bool KODIS, bool TMA = true, int REFRESH = 2>
+template <int NOUT, bool KODIS, bool TMA = true, int REFRESH = 2, bool FAST = false>
 OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int tile, int tile_rows,
                     const MixSmem<NOUT> &sm, unsigned &rseq, bool &bad, double &spec_sum, double (&bragg_sum)[2]) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -430,7 +430,9 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
         split_bins((sr_c - a.min_sr) * a.inv_binsize, Ch, Cl);
         const float phi_x = (float)reduce_2pi((-2.0 * a.k0) * sr_c);
         const float sin_i = (float)a.sin_inc[xs], cos_i = (float)a.cos_inc[xs];
-        const bool kodis = KODIS && a.do_kodis;
+        const bool kodis = FAST || (KODIS && a.do_kodis);
+        const bool bragg = FAST || a.do_bragg;
+        const int npol = FAST ? 1 : a.npol;
         const float tan_i = kodis ? (float)a.tan_inc[xs] : 0.f;
         const float dinc0 = (float)(a.inc[xs] - a.inc_angle);
         float cap_r = 0.f;
@@ -467,7 +469,7 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
             mbar_expect_tx(bar, row_bytes);
             const int yy = y0 + r;
             tma_load_3d(dst + kAdx * kMixCols, &maps->fields, x0t, yy, 0, bar);
-            if (a.do_bragg) {
+            if (bragg) {
                 tma_load_2d(dst + kAindm * kMixCols, &maps->indm, x0t, yy, bar);
                 tma_load_2d(dst + kAindp * kMixCols, &maps->indp, x0t, yy, bar);
             }
@@ -508,7 +510,7 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
         int fail_row = -1;
         bool ok = __all_sync(0xffffffffu, wait_row(0));
         if (!ok) fail_row = 0;
-        if (ok && a.do_bragg) gather(0, gm, gp);
+        if (ok && bragg) gather(0, gm, gp);
         for (int i = 0; i < nrows && ok; ++i) {
             // rows i and i + 1 have landed
             if (i + 1 < nrows) {
@@ -531,7 +533,7 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
                 if (load_scat) {
                     sc[0][0] = src[kAscat * kMixCols + t];
                     sc[0][1] = src[(kAscat + 1) * kMixCols + t];
-                    if (a.npol == 2) {
+                    if (npol == 2) {
                         sc[1][0] = src[(kAscat + 2) * kMixCols + t];
                         sc[1][1] = src[(kAscat + 3) * kMixCols + t];
                     }
@@ -544,14 +546,14 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
                 if (load_scat) {
                     sc[0][0] = __ldg(scat + g);
                     sc[0][1] = __ldg(scat + npix + g);
-                    if (a.npol == 2) {
+                    if (npol == 2) {
                         sc[1][0] = __ldg(scat + 2 * npix + g);
                         sc[1][1] = __ldg(scat + 3 * npix + g);
                     }
                 }
             }
             const float2 cm = gm, cp = gp;
-            if (a.do_bragg && i + 1 < nrows) gather(i + 1, gm, gp);
+            if (bragg && i + 1 < nrows) gather(i + 1, gm, gp);
             // release the slot of row i; the last of the four warps refills it with row i + 4
             __syncwarp();
             if (TMA && lane == 0) {
@@ -637,15 +639,15 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
                     }
                 }
             }
-            if (a.do_bragg) {
+            if (bragg) {
                 if (REFRESH != 0 && refresh) {
                     float hh[2], vv[2];
                     const int y = y0 + i;
-                    if (a.lut) {
+                    if (!FAST && a.lut) {
                         const int ai = lut_az_index(a, a.rowtab[2LL * a.ny + y]);
                         float r0[2], r1[2];
                         romeiser_lut<float>(a, ai, diffx, diffy, 0, r0);
-                        if (a.npol == 2) romeiser_lut<float>(a, ai, diffx, diffy, 1, r1);
+                        if (npol == 2) romeiser_lut<float>(a, ai, diffx, diffy, 1, r1);
                         else { r1[0] = r0[0]; r1[1] = r0[1]; }
                         const bool vv_first = a.rom.pol == POL_VV;
                         hh[0] = vv_first ? r1[0] : r0[0]; hh[1] = vv_first ? r1[1] : r0[1];
@@ -653,7 +655,7 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
                     } else {
                         romeiser_facet<float>(a.rom, (float)a.inc[x], rt[6], rt[4], rt[5], diffx, diffy, hh, vv);
                     }
-                    if (a.use_hmtf) {
+                    if (!FAST && a.use_hmtf) {
                         float hm = a.hmtf[(long long)y * a.nx + x];
                         hm = hm < -1.f ? -1.f : hm;
                         const float f = 1.f + hm;
@@ -662,7 +664,7 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
                     const long long idx = (long long)y * a.nx + x;
 #pragma unroll
                     for (int p = 0; p < 2; ++p) {
-                        if (p < a.npol) {
+                        if (p < npol) {
                             const bool use_vv = a.rom.pol == POL_VV || (a.rom.pol == POL_DP && p == 1);
                             const float r0 = use_vv ? vv[0] : hh[0], r1 = use_vv ? vv[1] : hh[1];
                             bragg_sum[p] += (double)r0 + (double)r1;
@@ -681,7 +683,7 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
                 __sincosf(th + cap_r, &s1, &c1);
 #pragma unroll
                 for (int p = 0; p < 2; ++p) {
-                    if (p < a.npol) {
+                    if (p < npol) {
                         const c64 l0 = cmul(c64{sc[p][0] * c0, sc[p][0] * s0}, c64{cm.x, cm.y});
                         const c64 l1 = cmul(c64{sc[p][1] * c1, sc[p][1] * s1}, c64{cp.x, cp.y});
                         scene[p] = cadd(scene[p], cadd(l0, l1));
@@ -691,15 +693,16 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
             // ---- channels: antenna pattern x ATI phase (row) x XTI phase (facet) ----
             c64 coef[NOUT];
             float wave_dinc = 0.f;
-            if (a.any_xti) wave_dinc = (dz * sin_i + dx * sin_i) * inv_sr0;
+            if (!FAST && a.any_xti) wave_dinc = (dz * sin_i + dx * sin_i) * inv_sr0;
 #pragma unroll
             for (int k = 0; k < NOUT; ++k) {
-                if (k < a.nout) {
-                    const unsigned okb = outs >> (5 * k);
+                if (FAST || k < a.nout) {
+                    // fast configuration: one polarisation, no XTI phase, output k is channel out0 + k
+                    const unsigned okb = FAST ? (unsigned)(a.out0 + k) : outs >> (5 * k);
                     const int c = okb & 7;
                     const c64 f = {rt[kMixRT + 2 * c], rt[kMixRT + 2 * c + 1]};
-                    c64 v = cmul((okb & 8) ? scene[1] : scene[0], f);
-                    if (okb & 16) {
+                    c64 v = cmul((!FAST && (okb & 8)) ? scene[1] : scene[0], f);
+                    if (!FAST && (okb & 16)) {
                         const float ph = wrap_pi(kxti[k] * (dinc0 + wave_dinc));
                         float s, cc;
                         __sincosf(ph, &s, &cc);
@@ -785,7 +788,7 @@ template <int NOUT> OCS_D void mix_init(const MixSmem<NOUT> &sm) {
     __syncthreads();
 }
 
-template <int NOUT, bool KODIS, int REFRESH>
+template <int NOUT, bool KODIS, int REFRESH, bool FAST = false>
 __global__ void __launch_bounds__(kMixCols, NOUT < 4 ? 4 : 2)
 pulse_mixed_kernel(const __grid_constant__ PulseArgs a, const __grid_constant__ MixMaps maps, float *lo_row) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -797,7 +800,8 @@ pulse_mixed_kernel(const __grid_constant__ PulseArgs a, const __grid_constant__ 
     unsigned rseq = 0;
     bool bad = false;
     for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x)
-        mix_tile<NOUT, KODIS, true, REFRESH>(a, &maps, lo_row, tile, a.tile_rows, sm, rseq, bad, spec_sum, bragg_sum);
+        mix_tile<NOUT, KODIS, true, REFRESH, FAST>(a, &maps, lo_row, tile, a.tile_rows, sm, rseq, bad, spec_sum,
+                                                   bragg_sum);
     if (a.out0 == 0) {
         if (KODIS) block_atomic_sum(spec_sum, &a.nrcs_spec[a.az_step], sm.sred);
         if (a.do_bragg && a.refresh)

@@ -17,10 +17,13 @@ surface and scatterer series for the same seed: surface (random phases, swell), 
 Bragg scatterer series ``rndscat_p`` and ``rndscat_m`` of shape (N_repeat_x, Ny, Nx) at the
 sub-pulse rate.
 
-Scope: Kodis specular and the direct Romeiser Bragg model.  The reference's Kirchhoff
-branch of this generator is marked FIXME there and its hMTF branch writes the rolled
-clipping mask into the unrolled surface; both raise ``NotImplementedError`` here, as do
-the LUT mode (the reference builds one table per range block) and buoy-spectrum input.
+Scope: Kodis specular, the direct Romeiser Bragg model and the hMTF modulation.  The
+reference's hMTF branch weights the Bragg RCS by 1 + hMTF of the rolled rows without
+clipping and writes its clipping mask (computed on the rolled rows) into the unrolled
+surface, where it persists while the ocean is frozen; both are reproduced.  The
+reference's Kirchhoff branch of this generator is marked FIXME there and raises
+``NotImplementedError`` here, as do the LUT mode (the reference builds one table per
+range block) and buoy-spectrum input.
 The reference adds no noise in this generator; neither does this one.
 """
 import ctypes
@@ -64,8 +67,6 @@ class DopscaGenerator(object):
         self.use_hmtf = bool(srg.use_hmtf)
         self.scat_spec_enable = bool(srg.scat_spec_enable)
         self.scat_bragg_enable = bool(srg.scat_bragg_enable)
-        if self.use_hmtf:
-            raise NotImplementedError('hMTF in the DopSCA generator is not built')
         if self.scat_spec_enable and srg.scat_spec_mode != 'kodis':
             raise NotImplementedError('specular mode %s in the DopSCA generator is not built' % srg.scat_spec_mode)
         if self.scat_bragg_enable and srg.scat_bragg_model != 'romeiser97':
@@ -94,6 +95,8 @@ class DopscaGenerator(object):
         compute = ['D', 'Diff']
         if self.scat_spec_enable:
             compute.append('Diff2')
+        if self.use_hmtf:
+            compute.append('hMTF')
         s = self.surface = OceanSurface()
         if reuse_ocean_file:
             try:
@@ -208,7 +211,10 @@ class DopscaGenerator(object):
         d.az_steps = self.az_steps
         d.ant_l_tx, d.ant_l_rx = float(self.ant_l_tx), float(self.ant_l_rx)
         d.b_ati, d.b_xti = self._b0, self._b0
-        d.do_kodis, d.do_bragg, d.use_hmtf = int(self.scat_spec_enable), int(self.scat_bragg_enable), 0
+        d.do_kodis, d.do_bragg = int(self.scat_spec_enable), int(self.scat_bragg_enable)
+        d.use_hmtf = int(self.use_hmtf and self.scat_bragg_enable)
+        if d.use_hmtf:
+            d.hmtf_d = f('hMTF').data_ptr()
         d.facet_dx, d.facet_dy = float(s.dx), float(s.dy)
         if self.scat_bragg_enable:
             self.rcs_bragg.fill(d)
@@ -263,6 +269,13 @@ class DopscaGenerator(object):
         if self.scat_bragg_enable:
             d.tind = self.rndscat_m.tind(t_now)
         _capi.call("ocs_pulse", ctypes.byref(d), PRECISIONS[self.precision], _device.stream_ptr(self.stream))
+        if d.use_hmtf and self.frozen:
+            # the reference's clipping of the rolled hMTF writes -1 into the unrolled
+            # surface where the rolled value is below -1 (dopsca_raw.py:463-466); a frozen
+            # surface keeps those writes for the following sub-pulses
+            with torch.cuda.stream(self.stream):          # None: the current stream
+                h = s.field('hMTF')
+                h.masked_fill_(torch.roll(h, -shift, dims=0) < -1, -1.0)
 
     def run(self, steps=None):
         for a in (range(self.az_steps) if steps is None else steps):

@@ -1,7 +1,7 @@
 """Oracle (test infrastructure only): the DopSCA scatterometer generator ``dopsca_raw``.
 
 Restates ``oceansar/dopscasim/dopsca_raw.py:34-632`` for the Kodis specular and direct
-Romeiser Bragg models with the oracle's own surface, NRCS, closure, geometry and
+Romeiser Bragg models (with the hMTF weighting of ``:461-472``) with the oracle's own surface, NRCS, closure, geometry and
 accumulation restatements:
 
 * set-up ``:66-360``: configuration (``[sca]``, ``[acquisition]``, ``ocean.N_repeat_x``),
@@ -36,8 +36,9 @@ class DopscaSim:
         self.wh_tol = srg.wh_tol
         self.scat_spec_enable = srg.scat_spec_enable
         self.scat_bragg_enable = srg.scat_bragg_enable
-        if srg.use_hmtf or (srg.scat_spec_enable and srg.scat_spec_mode != 'kodis'):
-            raise NotImplementedError('restated for Kodis + Romeiser without hMTF')
+        self.use_hmtf = bool(srg.use_hmtf)
+        if srg.scat_spec_enable and srg.scat_spec_mode != 'kodis':
+            raise NotImplementedError('restated for Kodis specular')
         self.inc_angle = np.deg2rad(sca.inc_angle)
         self.f0 = f0 = sca.f0
         pol = self.pol = sca.pol
@@ -58,7 +59,8 @@ class DopscaSim:
                np.deg2rad(oc.wind_dir), oc.wind_fetch, oc.wind_U, oc.current_mag,
                np.deg2rad(oc.current_dir), oc.dir_swell_dir, oc.freq_r, oc.sigf, oc.sigs, oc.Hs,
                oc.swell_dir_enable, oc.swell_enable, oc.swell_ampl, np.deg2rad(oc.swell_dir),
-               oc.swell_wl, ['D', 'Diff', 'Diff2'], oc.opt_res, oc.fft_max_prime,
+               oc.swell_wl, ['D', 'Diff', 'Diff2'] + (['hMTF'] if self.use_hmtf else []), oc.opt_res,
+               oc.fft_max_prime,
                choppy_enable=oc.choppy_enable, depth=oc.depth, dirspectrum_func=None,
                dir_swell_spec=spectra.ardhuin_swell_spec if oc.swell_dir_enable else None)
         n_rep = self.n_rep = int(oc.N_repeat_x)
@@ -167,6 +169,17 @@ class DopscaSim:
                     RCS_bragg_hh = r
                 else:
                     RCS_bragg_vv = r
+                if self.use_hmtf:                      # dopsca_raw.py:461-472
+                    if blk == 0:
+                        self.hmtf_in = s.hMTF.copy()       # the field this sub-pulse reads
+                        hmtf = np.roll(s.hMTF.copy(), -az_now_int_smp, axis=0)
+                        s.hMTF[np.where(hmtf < -1)] = -1
+                    if self.do_hh:
+                        RCS_bragg_hh[0] *= (1 + hmtf)
+                        RCS_bragg_hh[1] *= (1 + hmtf)
+                    if self.do_vv:
+                        RCS_bragg_vv[0] *= (1 + hmtf)
+                        RCS_bragg_vv[1] *= (1 + hmtf)
                 if self.do_hh:
                     scat_bragg_hh = np.sqrt(RCS_bragg_hh)
                     self.NRCS_avg_hh[az_step] += np.sum(RCS_bragg_hh) / self.surface_area

@@ -132,11 +132,12 @@ def test_single_precision_kernel():
 
 
 @pytest.mark.parametrize("shape", [(64, 64, 32), (97, 300, 90), (1024, 2048, 512), (5, 7, 16), (97, 301, 90),
-                                   (4096, 4096, 2048)])
+                                   (203, 390, 120), (3, 2, 8), (4096, 4096, 2048)])
 def test_two_dimensional_layout(shape):
     """The [ny, nx] column-walking kernel gives the flattened sum (edges: ragged tiles,
-    bins outside [0, nbins), a non-finite facet); at 4096 x 4096 the persistent CTAs walk
-    several tiles each."""
+    bins outside [0, nbins), a non-finite facet; 203 x 390: a ragged last column tile and
+    a last row batch of fewer rows); at 4096 x 4096 the persistent CTAs walk several
+    tiles each."""
     from oceansar_b200.radarsim import range_profile as rp
     ny, nx, nbins = shape
     srg, scene = _synthetic(ny, nx, nbins, 5)
@@ -152,7 +153,10 @@ def test_two_dimensional_layout(shape):
     assert rel(out[fin], ref[fin]) < 1e-10
 
 
-def test_two_dimensional_c64():
+@pytest.mark.parametrize("misaligned", [False, True], ids=["aligned", "misaligned"])
+def test_two_dimensional_c64(misaligned):
+    """Single precision in the [ny, nx] layout, also with inputs that start 8 bytes past
+    a 16-byte boundary (views into larger buffers)."""
     import ctypes
     from oceansar_b200 import _capi
     from oceansar_b200.radarsim import range_profile as rp
@@ -161,8 +165,11 @@ def test_two_dimensional_c64():
     sinc = rp.calc_sinc_vec(8, 20, Fs=1.1)
     ref = np.zeros(nbins, complex)
     orp.chan_profile(srg, scene, 2.725, 0.0, sinc, 8, 20, ref)
-    s_d = torch.tensor(srg, dtype=torch.float64, device="cuda")
-    c_d = torch.tensor(np.stack([scene.real, scene.imag], -1), dtype=torch.float32, device="cuda")
+    k = 1 if misaligned else 0
+    s_d = torch.tensor(np.concatenate([np.zeros(k), srg]), dtype=torch.float64, device="cuda")[k:]
+    c_d = torch.tensor(np.stack([np.concatenate([np.zeros(k), scene.real]), np.concatenate([np.zeros(k), scene.imag])],
+                                -1), dtype=torch.float32, device="cuda")[k:]
+    assert (s_d.data_ptr() % 16 == 8) == misaligned and (c_d.data_ptr() % 16 == 8) == misaligned
     w_d = torch.tensor(sinc, dtype=torch.float32, device="cuda")
     o_d = torch.zeros(nbins, 2, dtype=torch.float32, device="cuda")
     st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)

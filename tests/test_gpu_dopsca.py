@@ -27,18 +27,22 @@ def max_phase(a, b):
     return np.max(np.abs(np.angle(a[mask] * np.conj(b[mask]))))
 
 
-def stagewise(name, precision):
+def stagewise(name, precision, cfg=None, copy=lambda a, sub: True):
+    """copy(a, sub): whether the oracle's fields are written into the device buffers
+    before that sub-pulse (hMTF as the sub-pulse read it, before its clipping writes)."""
     from oceansar_b200.dopscasim import DopscaGenerator
     from oracle.dopsca_raw import DopscaSim
-    cfg = os.path.join(G, "cfg", name + ".cfg")
+    cfg = cfg or os.path.join(G, "cfg", name + ".cfg")
     osim = DopscaSim(cfg, seed=0)
     gen = DopscaGenerator(cfg, precision=precision, seed=0)
     assert (gen.az_steps, gen.rg_samp) == (osim.az_steps, osim.rg_samp)
     for a in range(gen.az_steps):
         for sub in range(gen.n_sub):
             osim.sub_pulse(a, sub)
-            for fld in gen.surface._fields:
-                gen.surface.field(fld).copy_(torch.from_numpy(np.ascontiguousarray(getattr(osim.surface, fld))))
+            if copy(a, sub):
+                for fld in gen.surface._fields:
+                    src = osim.hmtf_in if fld == 'hMTF' else getattr(osim.surface, fld)
+                    gen.surface.field(fld).copy_(torch.from_numpy(np.ascontiguousarray(src)))
             gen.sub_pulse(a, sub, update_surface=False)
     raw, nrcs_avg = gen.finish()
     ref, nref = osim.finish()
@@ -58,6 +62,46 @@ def test_stagewise_mixed(name):
     e, ph = rel_l2(raw, ref), max_phase(raw, ref)
     assert e < 1e-4 and ph < 1e-3, (e, ph)
     np.testing.assert_allclose(nrcs_avg, nref, rtol=1e-5)
+
+
+def _hmtf_cfg(tmp_path, name, frozen, wind=None):
+    import re
+    text = open(os.path.join(G, "cfg", name + ".cfg")).read()
+    text = text.replace("use_hmtf=False", "use_hmtf=True").replace("frozen_ocean=False", "frozen_ocean=%s" % frozen)
+    if wind is not None:
+        text = re.sub(r"wind_U\s*=\s*[0-9.]+", "wind_U=%s" % wind, text)
+    p = tmp_path / ("%s_hmtf.cfg" % name)
+    p.write_text(text)
+    return str(p)
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_hmtf_stagewise(precision, tmp_path):
+    """hMTF weighting of the Bragg RCS (dopsca_raw.py:461-472): 1 + hMTF of the rolled
+    rows, unclipped, on an evolving surface."""
+    raw, nrcs_avg, ref, nref = stagewise("dsc1", precision, _hmtf_cfg(tmp_path, "dsc1", False))
+    if precision == "f64":
+        assert rel_l2(raw, ref) < 1e-10, rel_l2(raw, ref)
+        np.testing.assert_allclose(nrcs_avg, nref, rtol=1e-9)
+    else:
+        e, ph = rel_l2(raw, ref), max_phase(raw, ref)
+        assert e < 1e-4 and ph < 1e-3, (e, ph)
+        np.testing.assert_allclose(nrcs_avg, nref, rtol=1e-5)
+
+
+def test_hmtf_frozen_clipping_writes(tmp_path):
+    """Frozen ocean at 16 m/s, where the rolled hMTF drops below -1: the reference leaves
+    those facets' RCS negative (NaN scatterer amplitudes, kept here) and writes -1 into the
+    unrolled surface at the rolled positions, which later sub-pulses read.  The device
+    fields are written from the oracle only while the surface still evolves (the first
+    azimuth step); afterwards both sides carry their own clipping writes."""
+    cfg = _hmtf_cfg(tmp_path, "dsc2", True, wind=16.)
+    raw, nrcs_avg, ref, nref = stagewise("dsc2", "f64", cfg, copy=lambda a, sub: a == 0)
+    fin = np.isfinite(ref)
+    assert 0 < (~fin).sum() < fin.sum() // 10
+    assert np.array_equal(np.isfinite(raw), fin)
+    assert rel_l2(raw[fin], ref[fin]) < 1e-10, rel_l2(raw[fin], ref[fin])
+    np.testing.assert_allclose(nrcs_avg, nref, rtol=1e-9)
 
 
 @pytest.mark.parametrize("name", ["dsc1", "dsc2"])
@@ -91,7 +135,7 @@ def test_invalid_scatterometer_descriptors():
     lib = _capi.load()
     d = gen.desc
     d.az_step, d.nrcs_row = 0, 0
-    for field, bad in (("field_nx", 7), ("roll", d.ny), ("nrcs_row", d.nrcs_rows), ("use_hmtf", 1)):
+    for field, bad in (("field_nx", 7), ("roll", d.ny), ("nrcs_row", d.nrcs_rows), ("lut_d", 256)):
         keep = getattr(d, field)
         setattr(d, field, bad)
         assert lib.ocs_pulse(ctypes.byref(d), 1, None) != 0, field
