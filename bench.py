@@ -814,7 +814,7 @@ def main():
         tuner = Autotuner()
         try:
             batched = batched_report(prep, tuner, args.precision)
-            serving = {"stable": serving_report(prep, tuner, args.precision, rate=2.0, duration=10.0),
+            serving = {"stable": serving_report(prep, tuner, args.precision, rate=1.2, duration=15.0),
                        "configured": serving_report(prep, tuner, args.precision, rate=20.0, duration=2.0)}
         finally:
             prep.close()

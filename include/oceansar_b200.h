@@ -254,7 +254,8 @@ typedef struct {
      * az_f32 = 1: the azimuth residual az_now is a float32 value and the row azimuth is the
      * float32 difference y - az_now (the reference's numpy promotion when the grid step is
      * float32 and the residual is not a float64 scalar).
-     * Requires nch = 1, Kodis (spec_mode 0), no LUT; hMTF (use_hmtf) is read at the rolled
+     * Requires nch = 1, Kodis (spec_mode 0); the LUT mode reads the table of the column's
+     * range block (lut_block); hMTF (use_hmtf) is read at the rolled
      * row of the [ny][field_nx] surface and not clipped (the DopSCA generator's weighting,
      * dopsca_raw.py:461-472).  The scene batch rejects it. */
     int32_t sca;
@@ -284,6 +285,10 @@ typedef struct {
      * target also takes that facet's displacements Dx, Dy, Dz as zero.  SKIM mode only. */
     int32_t pt_mode, pt_x, pt_y;
     double pt_amp;
+    /* Scatterometer mode with the Romeiser LUT: elements between the tables of consecutive
+     * range blocks in lut_d (the DopSCA generator builds one table per block at the block's
+     * mean incidence, dopsca_raw.py:329-356); 0: one table for every block. */
+    int64_t lut_block;
 } ocs_pulse_desc;
 
 /* Workspace of ocs_pulse (per-pulse float64 and float32 tables of the row quantities and

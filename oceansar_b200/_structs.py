@@ -40,7 +40,8 @@ class PulseDesc(ctypes.Structure):
                 ("s_m32_d", P), ("s_p32_d", P), ("sca", I32), ("field_nx", I32), ("roll", I32),
                 ("sr_bin_offset", F64), ("cap_t", F64), ("nrcs_row", I32), ("nrcs_rows", I32),
                 ("az_f32", I32), ("skim", I32), ("skim_ny_integ", I32), ("skim_az2", I32), ("skim_rcm", I32),
-                ("raw_lo_d", P), ("pt_mode", I32), ("pt_x", I32), ("pt_y", I32), ("pt_amp", F64)]
+                ("raw_lo_d", P), ("pt_mode", I32), ("pt_x", I32), ("pt_y", I32), ("pt_amp", F64),
+                ("lut_block", ctypes.c_int64)]
 
 
 class RcsDesc(ctypes.Structure):

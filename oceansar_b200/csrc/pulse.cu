@@ -102,6 +102,7 @@ struct PulseArgs {
     double atx, arx;                        // SKIM: antenna lengths / wavelength (tx, rx)
     int pt_mode, pt_x, pt_y;                // SKIM calibration target: 0 none, 1 floating, 2 fixed
     double pt_amp;
+    long long lut_block;                    // scatterometer LUT: elements between block tables
 };
 
 // Kirchhoff specular term of one facet and polarisation code pc (0 = hh, 1 = vv),
@@ -120,12 +121,13 @@ OCS_D c128 ka_specular(const KaParams &kp, int pc, double srs, double x, double 
 // polarisation p at (azimuth index of the row, clamped slope indices of the facet).
 // Indices round half to even from float64 differences and divisions, as numpy does.
 template <typename T>
-OCS_D void romeiser_lut(const PulseArgs &a, int az_ind, float diffx, float diffy, int p, T (&r)[2]) {
+OCS_D void romeiser_lut(const PulseArgs &a, int az_ind, float diffx, float diffy, int p, T (&r)[2],
+                        long long table = 0) {
     int iy = (int)rint(ddiv(dsub((double)diffy, a.lut_dy0), a.lut_ddy));
     int ix = (int)rint(ddiv(dsub((double)diffx, a.lut_dx0), a.lut_ddx));
     iy = iy > 0 ? (iy < a.lut_ndy ? iy : a.lut_ndy - 1) : 0;
     ix = ix > 0 ? (ix < a.lut_ndx ? ix : a.lut_ndx - 1) : 0;
-    const T *lut = static_cast<const T *>(a.lut);
+    const T *lut = static_cast<const T *>(a.lut) + table;
     const long long plane = (long long)a.lut_naz * a.lut_ndy * a.lut_ndx;
     const long long off = ((long long)az_ind * a.lut_ndy + iy) * a.lut_ndx + ix;
     r[0] = lut[(2LL * p) * plane + off];
@@ -532,9 +534,11 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
                     if (a.lut) {
                         // the table holds the model's output polarisation(s) in output order
                         const int ai = lut_az_index(a, sm.r_az[2 * RCAP + i]);
+                        // the scatterometer's range blocks each have their own table
+                        const long long tb = (MODE == kModeSca) ? (long long)(x / a.fnx) * a.lut_block : 0;
                         T r0[2], r1[2];
-                        romeiser_lut<T>(a, ai, cur.diffx, cur.diffy, 0, r0);
-                        if (a.npol == 2) romeiser_lut<T>(a, ai, cur.diffx, cur.diffy, 1, r1);
+                        romeiser_lut<T>(a, ai, cur.diffx, cur.diffy, 0, r0, tb);
+                        if (a.npol == 2) romeiser_lut<T>(a, ai, cur.diffx, cur.diffy, 1, r1, tb);
                         else { r1[0] = r0[0]; r1[1] = r0[1]; }
                         const bool vv_first = a.rom.pol == POL_VV;
                         hh[0] = vv_first ? r1[0] : r0[0]; hh[1] = vv_first ? r1[1] : r0[1];
@@ -1094,8 +1098,9 @@ static int fill_pulse_args(const ocs_pulse_desc *d, PulseArgs &a) {
         // whole range blocks of field_nx columns; the Bragg RCS is evaluated on every launch
         // and not stored
         if (d->nch != 1 || d->field_nx < 1 || d->nx % d->field_nx != 0 || d->roll < 0 || d->roll >= d->ny ||
-            a.spec_mode != 0 || d->lut_d)
+            a.spec_mode != 0 || d->lut_block < 0)
             return OCS_ERR_ARG;
+        a.lut_block = d->lut_d ? d->lut_block : 0;
         if (!(d->sr_bin_offset >= 0.0) || !(d->cap_t >= 0.0)) return OCS_ERR_ARG;
         if (d->nrcs_rows < 1 || d->nrcs_row < 0 || d->nrcs_row >= d->nrcs_rows) return OCS_ERR_ARG;
         a.sca = 1;

@@ -17,13 +17,14 @@ surface and scatterer series for the same seed: surface (random phases, swell), 
 Bragg scatterer series ``rndscat_p`` and ``rndscat_m`` of shape (N_repeat_x, Ny, Nx) at the
 sub-pulse rate.
 
-Scope: Kodis specular, the direct Romeiser Bragg model and the hMTF modulation.  The
+Scope: Kodis specular, the Romeiser Bragg model (direct or LUT) and the hMTF modulation.  The
 reference's hMTF branch weights the Bragg RCS by 1 + hMTF of the rolled rows without
 clipping and writes its clipping mask (computed on the rolled rows) into the unrolled
 surface, where it persists while the ocean is frozen; both are reproduced.  The
 reference's Kirchhoff branch of this generator is marked FIXME there and raises
-``NotImplementedError`` here, as do the LUT mode (the reference builds one table per
-range block) and buoy-spectrum input.
+``NotImplementedError`` here, as does buoy-spectrum input.  The Romeiser LUT mode keeps
+one table per range block (the reference builds one model per block), stacked on the
+device and selected by the column's block in the kernel.
 The reference adds no noise in this generator; neither does this one.
 """
 import ctypes
@@ -71,8 +72,7 @@ class DopscaGenerator(object):
             raise NotImplementedError('specular mode %s in the DopSCA generator is not built' % srg.scat_spec_mode)
         if self.scat_bragg_enable and srg.scat_bragg_model != 'romeiser97':
             raise NotImplementedError('RCS model %s for Bragg scattering not implemented' % srg.scat_bragg_model)
-        if self.scat_bragg_enable and bool(getattr(srg, 'use_lut', False)):
-            raise NotImplementedError('the Romeiser LUT mode in the DopSCA generator is not built')
+        self.use_lut = bool(getattr(srg, 'use_lut', False))
         self.inc_angle = np.deg2rad(sca.inc_angle)
         self.f0 = f0 = sca.f0
         self.pol = pol = sca.pol
@@ -173,6 +173,19 @@ class DopscaGenerator(object):
                                                 srg.scat_bragg_spec, srg.scat_bragg_spread,
                                                 srg.scat_bragg_d, rmss_x=s.rmss_x, rmss_y=s.rmss_y,
                                                 az_span=az_span, use_lut=False)
+            if self.use_lut:
+                # LUT mode: one table per range block at the block's mean incidence
+                # (dopsca_raw.py:329-356 builds one model per block); the lookup grids are
+                # the same for every block
+                self.rcs_lut_s = [nrcs.RCSRomeiser97(k0, inc_s[b], pol, s.dx, s.dy, linalg.norm(u_eff),
+                                                     np.arctan2(u_eff[1], u_eff[0]), s.wind_fetch,
+                                                     srg.scat_bragg_spec, srg.scat_bragg_spread,
+                                                     srg.scat_bragg_d, rmss_x=s.rmss_x, rmss_y=s.rmss_y,
+                                                     az_span=az_span, use_lut=True)
+                                  for b in range(n_rep)]
+                params = {m.lut_params() for m in self.rcs_lut_s}
+                if len(params) != 1:
+                    raise ValueError('the range blocks\' LUT grids differ')
         self._alloc()
 
     # ------------------------------------------------------------------------------------
@@ -234,6 +247,13 @@ class DopscaGenerator(object):
             if self.precision == 'mixed':
                 d.s_m32_d, d.s_p32_d = self.rndscat_m.device32().data_ptr(), self.rndscat_p.device32().data_ptr()
             d.ind0_m_d, d.ind0_p_d = self._ind_m.data_ptr(), self._ind_p.data_ptr()
+            if self.use_lut:
+                tabs = [m.lut_device(self.precision) for m in self.rcs_lut_s]
+                self._lut_d = torch.stack(tabs).contiguous()     # [block][npol][2][naz][ndy][ndx]
+                d.lut_d = self._lut_d.data_ptr()
+                d.lut_block = int(tabs[0].numel())
+                (d.lut_naz, d.lut_ndy, d.lut_ndx, d.lut_az0, d.lut_daz, d.lut_dy0, d.lut_ddy, d.lut_dx0,
+                 d.lut_ddx) = self.rcs_lut_s[0].lut_params()
         d.sinc_d = self._sinc_d.data_ptr()
         d.raw_d = self.raw_d.data_ptr()
         d.nbins = self.rg_samp

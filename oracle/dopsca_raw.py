@@ -119,7 +119,7 @@ class DopscaSim:
                                                    np.arctan2(u_eff[1], u_eff[0]), s.wind_fetch,
                                                    srg.scat_bragg_spec, srg.scat_bragg_spread, srg.scat_bragg_d,
                                                    rmss_x=s.rmss_x, rmss_y=s.rmss_y, az_span=az_span,
-                                                   use_lut=False)
+                                                   use_lut=bool(getattr(srg, 'use_lut', False)))
                                 for b in range(n_rep)]
             self.phase_bragg = np.zeros([2, s.Ny, s.Nx])
             self.bragg_scats = np.zeros([2, s.Ny, s.Nx], dtype=complex)

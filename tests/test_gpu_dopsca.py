@@ -89,6 +89,24 @@ def test_hmtf_stagewise(precision, tmp_path):
         np.testing.assert_allclose(nrcs_avg, nref, rtol=1e-5)
 
 
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_lut_mode_stagewise(precision, tmp_path):
+    """Romeiser LUT mode (srg.use_lut): one table per range block at the block's mean
+    incidence (dopsca_raw.py:329-356), selected by the column's block in the kernel."""
+    text = open(os.path.join(G, "cfg", "dsc1.cfg")).read()
+    assert "use_lut = False" in text
+    cfg = tmp_path / "dsc1_lut.cfg"
+    cfg.write_text(text.replace("use_lut = False", "use_lut = True", 1))
+    raw, nrcs_avg, ref, nref = stagewise("dsc1", precision, str(cfg))
+    if precision == "f64":
+        assert rel_l2(raw, ref) < 1e-10, rel_l2(raw, ref)
+        np.testing.assert_allclose(nrcs_avg, nref, rtol=1e-9)
+    else:
+        e, ph = rel_l2(raw, ref), max_phase(raw, ref)
+        assert e < 1e-4 and ph < 1e-3, (e, ph)
+        np.testing.assert_allclose(nrcs_avg, nref, rtol=1e-5)
+
+
 def test_hmtf_frozen_clipping_writes(tmp_path):
     """Frozen ocean at 16 m/s, where the rolled hMTF drops below -1: the reference leaves
     those facets' RCS negative (NaN scatterer amplitudes, kept here) and writes -1 into the
@@ -135,7 +153,7 @@ def test_invalid_scatterometer_descriptors():
     lib = _capi.load()
     d = gen.desc
     d.az_step, d.nrcs_row = 0, 0
-    for field, bad in (("field_nx", 7), ("roll", d.ny), ("nrcs_row", d.nrcs_rows), ("lut_d", 256)):
+    for field, bad in (("field_nx", 7), ("roll", d.ny), ("nrcs_row", d.nrcs_rows), ("lut_block", -1)):
         keep = getattr(d, field)
         setattr(d, field, bad)
         assert lib.ocs_pulse(ctypes.byref(d), 1, None) != 0, field
