@@ -254,7 +254,8 @@ typedef struct {
      * az_f32 = 1: the azimuth residual az_now is a float32 value and the row azimuth is the
      * float32 difference y - az_now (the reference's numpy promotion when the grid step is
      * float32 and the residual is not a float64 scalar).
-     * Requires nch = 1, Kodis (spec_mode 0); the LUT mode reads the table of the column's
+     * Requires nch = 1; Kodis or Kirchhoff specular (spec_mode 0 / 1 / 2, the Kirchhoff
+     * field at the field column's x, scaled like the Kodis one); the LUT mode reads the table of the column's
      * range block (lut_block); hMTF (use_hmtf) is read at the rolled
      * row of the [ny][field_nx] surface and not clipped (the DopSCA generator's weighting,
      * dopsca_raw.py:461-472).  The scene batch rejects it. */

@@ -385,7 +385,7 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
         const double tan_i = a.do_kodis ? a.tan_inc[x] : 0.0;
         double cap = 0.0;
         if (a.do_bragg) {
-            if constexpr (MODE == kModeSca) cap = dmul(dmul(2.0 * a.k0, a.c_b[x]), a.cap_t);
+            if constexpr ((MODE & kModeSca)) cap = dmul(dmul(2.0 * a.k0, a.c_b[x]), a.cap_t);
             else cap = ((2.0 * a.k0) * a.t_step) * a.c_b[x] * (double)(a.az_step + 1);
         }
         const float cap_r = (float)reduce_2pi(cap);
@@ -410,9 +410,9 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
         // indices of tile row r: per-facet arrays (ridx) and surface fields (fidx); the
         // scatterometer mode reads the fields of the rolled row and the column mod fnx
         int fx = x;
-        if constexpr (MODE == kModeSca) fx = x % a.fnx;
+        if constexpr ((MODE & kModeSca)) fx = x % a.fnx;
         auto row_index = [&](int r, long long &ridx, long long &fidx) {
-            if constexpr (MODE == kModeSca) {
+            if constexpr ((MODE & kModeSca)) {
                 int fr = y0 + r + a.roll;
                 fr = fr >= a.ny ? fr - a.ny : fr;
                 ridx = (long long)fr * a.nx + x;
@@ -490,14 +490,14 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
             {
                 // the scatterometer's sub-pulses arrive later by sr_bin_off; the SKIM
                 // two-scale form with rcm adds az/2*sin_az to the bins only
-                double srb = (MODE == kModeSca) ? dadd(srs, a.sr_bin_off) : srs;
+                double srb = ((MODE & kModeSca)) ? dadd(srs, a.sr_bin_off) : srs;
                 if ((MODE & kModeSkim) && a.skim_rcm) srb = dadd(srs, dmul(az * 0.5, sin_az));
                 if (sizeof(T) == 8) bin_and_lut(srb, a.min_sr, a.binsize, kSincOvs, bin_d, lut);
                 else bin_and_lut_fast(srb, a.min_sr, a.inv_binsize, kSincOvs, bin_d, lut);
             }
             // two-way spreading of the scatterometer scene, (sr0 / (sr0 + r))^2
             T rscale = (T)1;
-            if constexpr (MODE == kModeSca) {
+            if constexpr ((MODE & kModeSca)) {
                 const double q = ddiv(a.sr0, dadd(a.sr0, srs));
                 rscale = (T)dmul(q, q);
             }
@@ -507,10 +507,12 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
                 c128 last = {0.0, 0.0};
                 for (int p = 0; p < a.npol; ++p) {
                     const int pc = a.rom.pol == POL_DP ? p : (a.rom.pol == POL_HH ? 0 : 1);
-                    last = ka_specular(a.ka, pc, srs, (double)a.x_f[x], (double)a.y[y0 + i], sin_i, cos_i, tan_i,
+                    last = ka_specular(a.ka, pc, srs, (double)a.x_f[fx], (double)a.y[y0 + i], sin_i, cos_i, tan_i,
                                        sm.r_az[4 * RCAP + i], sm.r_az[3 * RCAP + i], cur.dz, cur.diffx, cur.diffy,
                                        cur.diffxx, cur.diffyy, cur.diffxy);
                     scene[p] = {(T)last.re, (T)last.im};
+                    // the scatterometer scales the field by the two-way spreading
+                    if constexpr ((MODE & kModeSca) != 0) scene[p] = {scene[p].re * rscale, scene[p].im * rscale};
                 }
                 spec_sum += last.re * last.re + last.im * last.im;
             } else if (a.do_kodis) {
@@ -519,7 +521,7 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
                 const T s4 = (T)3.5449077018110318;                 // sqrt(4 pi)
                 const cplx<T> es = {e.re * s4, e.im * s4};
                 spec_sum += (double)es.re * es.re + (double)es.im * es.im;
-                if constexpr (MODE == kModeSca) {
+                if constexpr ((MODE & kModeSca)) {
                     scene[0] = {es.re * rscale, es.im * rscale};
                     scene[1] = scene[0];
                 } else {
@@ -535,7 +537,7 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
                         // the table holds the model's output polarisation(s) in output order
                         const int ai = lut_az_index(a, sm.r_az[2 * RCAP + i]);
                         // the scatterometer's range blocks each have their own table
-                        const long long tb = (MODE == kModeSca) ? (long long)(x / a.fnx) * a.lut_block : 0;
+                        const long long tb = ((MODE & kModeSca)) ? (long long)(x / a.fnx) * a.lut_block : 0;
                         T r0[2], r1[2];
                         romeiser_lut<T>(a, ai, cur.diffx, cur.diffy, 0, r0, tb);
                         if (a.npol == 2) romeiser_lut<T>(a, ai, cur.diffx, cur.diffy, 1, r1, tb);
@@ -549,7 +551,7 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
                     }
                     if (a.use_hmtf) {
                         float hm;
-                        if constexpr (MODE == kModeSca) {
+                        if constexpr ((MODE & kModeSca)) {
                             // the scatterometer generator weights by 1 + hMTF of the rolled
                             // row, unclipped (its clipping writes land in the unrolled surface,
                             // dopsca_raw.py:463-472)
@@ -571,7 +573,7 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
                             bragg_sum[p] += (double)r0 + (double)r1;
                             sc[p][0] = tsqrt(r0);
                             sc[p][1] = tsqrt(r1);
-                            if (MODE != kModeSca && a.out0 == 0) {   // one output group stores the RCS
+                            if (!(MODE & kModeSca) && a.out0 == 0) {   // one output group stores the RCS
                                 scat[(2 * p) * npix + idx] = sc[p][0];
                                 scat[(2 * p + 1) * npix + idx] = sc[p][1];
                             }
@@ -613,7 +615,7 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
                         const cplx<T> l0 = cmul(cplx<T>{sc[p][0] * e0.re, sc[p][0] * e0.im}, sm);
                         const cplx<T> l1 = cmul(cplx<T>{sc[p][1] * e1.re, sc[p][1] * e1.im}, sp);
                         cplx<T> lb = cadd(l0, l1);
-                        if constexpr (MODE == kModeSca) lb = {lb.re * rscale, lb.im * rscale};
+                        if constexpr ((MODE & kModeSca)) lb = {lb.re * rscale, lb.im * rscale};
                         scene[p] = cadd(scene[p], lb);
                     }
                 }
@@ -670,7 +672,7 @@ OCS_D void pulse_tile(const PulseArgs &a, int tile, int tile_rows, const PulseSm
         }
         cp_async_wait<0>();
     }
-    if constexpr (MODE == kModeSca) {
+    if constexpr ((MODE & kModeSca)) {
         // the scatterometer's NRCS sums are kept per range block: each column adds its
         // tile's sums to its block
         if (x < a.nx) {
@@ -868,7 +870,8 @@ batch_pulse_mixed_kernel(const __grid_constant__ BatchRef b) {
 template <typename T, int NOUT, int S>
 static int launch_pulse(PulseArgs a, cudaStream_t st) {
     const size_t smem = pulse_smem_bytes<T, NOUT, S, kPulseRows>(a.nch);
-    auto k = a.sca ? pulse_kernel<T, NOUT, S, kModeSca>
+    auto k = a.sca ? (a.spec_mode != 0 ? pulse_kernel<T, NOUT, S, kModeSca | kModeKa>
+                                       : pulse_kernel<T, NOUT, S, kModeSca>)
            : a.skim ? (a.spec_mode != 0 ? pulse_kernel<T, NOUT, S, kModeSkim | kModeKa>
                                         : pulse_kernel<T, NOUT, S, kModeSkim>)
                     : (a.spec_mode != 0 ? pulse_kernel<T, NOUT, S, kModeKa> : pulse_kernel<T, NOUT, S, kModeStd>);
@@ -1093,12 +1096,13 @@ static int fill_pulse_args(const ocs_pulse_desc *d, PulseArgs &a) {
         a.raw_row = (long long)d->az_step * a.s_int * d->nbins;
     }
     if (d->sca) {
-        // scatterometer mode: one channel, Kodis specular, direct Bragg model (hMTF, when on,
+        // scatterometer mode: one channel, Kodis or Kirchhoff specular (the field scaled by
+        // the two-way spreading like the Kodis field), Bragg model (hMTF, when on,
         // read at the rolled row of the [ny][field_nx] surface, unclipped); the columns are
         // whole range blocks of field_nx columns; the Bragg RCS is evaluated on every launch
         // and not stored
         if (d->nch != 1 || d->field_nx < 1 || d->nx % d->field_nx != 0 || d->roll < 0 || d->roll >= d->ny ||
-            a.spec_mode != 0 || d->lut_block < 0)
+            d->lut_block < 0)
             return OCS_ERR_ARG;
         a.lut_block = d->lut_d ? d->lut_block : 0;
         if (!(d->sr_bin_offset >= 0.0) || !(d->cap_t >= 0.0)) return OCS_ERR_ARG;

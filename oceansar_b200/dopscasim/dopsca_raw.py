@@ -17,12 +17,15 @@ surface and scatterer series for the same seed: surface (random phases, swell), 
 Bragg scatterer series ``rndscat_p`` and ``rndscat_m`` of shape (N_repeat_x, Ny, Nx) at the
 sub-pulse rate.
 
-Scope: Kodis specular, the Romeiser Bragg model (direct or LUT) and the hMTF modulation.  The
+Scope: Kodis or Kirchhoff specular, the Romeiser Bragg model (direct or LUT) and the hMTF
+modulation.  The
 reference's hMTF branch weights the Bragg RCS by 1 + hMTF of the rolled rows without
 clipping and writes its clipping mask (computed on the rolled rows) into the unrolled
 surface, where it persists while the ocean is frozen; both are reproduced.  The
-reference's Kirchhoff branch of this generator is marked FIXME there and raises
-``NotImplementedError`` here, as does buoy-spectrum input.  The Romeiser LUT mode keeps
+reference's Kirchhoff branch (marked FIXME there) is reproduced as written: the
+tangent-plane field of every facet at the block's incidence, times exp(-2 i k0 r) and
+(4 pi)^1.5, scaled by the two-way spreading, after one unused phase screen per block from
+the global RNG.  Buoy-spectrum input raises ``NotImplementedError``.  The Romeiser LUT mode keeps
 one table per range block (the reference builds one model per block), stacked on the
 device and selected by the column's block in the kernel.
 The reference adds no noise in this generator; neither does this one.
@@ -68,8 +71,9 @@ class DopscaGenerator(object):
         self.use_hmtf = bool(srg.use_hmtf)
         self.scat_spec_enable = bool(srg.scat_spec_enable)
         self.scat_bragg_enable = bool(srg.scat_bragg_enable)
-        if self.scat_spec_enable and srg.scat_spec_mode != 'kodis':
-            raise NotImplementedError('specular mode %s in the DopSCA generator is not built' % srg.scat_spec_mode)
+        self.scat_spec_mode = srg.scat_spec_mode if self.scat_spec_enable else 'kodis'
+        if self.scat_spec_enable and self.scat_spec_mode not in ('kodis', 'fa', 'spa'):
+            raise NotImplementedError('RCS mode %s for specular scattering not implemented' % self.scat_spec_mode)
         if self.scat_bragg_enable and srg.scat_bragg_model != 'romeiser97':
             raise NotImplementedError('RCS model %s for Bragg scattering not implemented' % srg.scat_bragg_model)
         self.use_lut = bool(getattr(srg, 'use_lut', False))
@@ -155,7 +159,15 @@ class DopscaGenerator(object):
 
         # ---- scattering models (:297-360; global RNG draw 2: rndscat_p then rndscat_m) ---
         if self.scat_spec_enable:
-            self.rcs_spec = nrcs.RCSKodis(inc_s, k0, s.dx, s.dy)
+            if self.scat_spec_mode == 'kodis':
+                self.rcs_spec = nrcs.RCSKodis(inc_s, k0, s.dx, s.dy)
+            else:
+                # Kirchhoff (the reference's FIXME branch, dopsca_raw.py:302-308): one model
+                # per block after an unused phase screen per block, drawn to keep the RNG
+                # stream; the models differ in nothing the kernel reads
+                for _ in range(n_rep):
+                    np.random.uniform(0., 2. * np.pi, size=[s.Ny, s.Nx])
+                self.rcs_spec = nrcs.RCSKA(self.scat_spec_mode, k0, s.x, s.y, s.dx, s.dy)
         if self.scat_bragg_enable:
             tau_c = grid_coherence(oc.wind_U, s.dx, f0)
             self.rndscat_p = randomscat_ts(tau_c, (n_rep, s.Ny, s.Nx), 1 / self.sub_len)
@@ -213,7 +225,15 @@ class DopscaGenerator(object):
         if self.scat_spec_enable:
             d.diffxx_d, d.diffyy_d, d.diffxy_d = (f('Diffxx').data_ptr(), f('Diffyy').data_ptr(),
                                                   f('Diffxy').data_ptr())
-            d.kodis_R_re, d.kodis_R_im = float(self.rcs_spec.R.real), float(self.rcs_spec.R.imag)
+            if self.scat_spec_mode == 'kodis':
+                d.kodis_R_re, d.kodis_R_im = float(self.rcs_spec.R.real), float(self.rcs_spec.R.imag)
+            else:
+                d.spec_mode = 1 if self.scat_spec_mode == 'fa' else 2
+                self._x_d = _device.to_device(s.x, np.float32)
+                d.x_d = self._x_d.data_ptr()
+                d.ka_dx, d.ka_dy = float(s.dx), float(s.dy)
+                K = self.rcs_spec.constant(1, 1)
+                d.ka_K_re, d.ka_K_im = K.real, K.imag
         d.y_d = self._y_d.data_ptr()
         c = self._cols
         d.sr_col_d, d.sin_inc_d, d.cos_inc_d = c['sr'].data_ptr(), c['sin'].data_ptr(), c['cos'].data_ptr()

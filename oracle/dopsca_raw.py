@@ -1,7 +1,7 @@
 """Oracle (test infrastructure only): the DopSCA scatterometer generator ``dopsca_raw``.
 
-Restates ``oceansar/dopscasim/dopsca_raw.py:34-632`` for the Kodis specular and direct
-Romeiser Bragg models (with the hMTF weighting of ``:461-472``) with the oracle's own surface, NRCS, closure, geometry and
+Restates ``oceansar/dopscasim/dopsca_raw.py:34-632`` for the Kodis or Kirchhoff specular
+and the Romeiser Bragg models (with the hMTF weighting of ``:461-472``) with the oracle's own surface, NRCS, closure, geometry and
 accumulation restatements:
 
 * set-up ``:66-360``: configuration (``[sca]``, ``[acquisition]``, ``ocean.N_repeat_x``),
@@ -16,7 +16,7 @@ accumulation restatements:
 import numpy as np
 from scipy import linalg
 
-from . import closure, geometry as geo, nrcs, range_profile as rp, spectra
+from . import closure, geometry as geo, ka, nrcs, range_profile as rp, spectra
 from .cfg import ConfigFile
 from .sar_raw import C_LIGHT, sinc_bp
 from .surface import OceanSurface
@@ -37,8 +37,7 @@ class DopscaSim:
         self.scat_spec_enable = srg.scat_spec_enable
         self.scat_bragg_enable = srg.scat_bragg_enable
         self.use_hmtf = bool(srg.use_hmtf)
-        if srg.scat_spec_enable and srg.scat_spec_mode != 'kodis':
-            raise NotImplementedError('restated for Kodis specular')
+        self.scat_spec_mode = srg.scat_spec_mode
         self.inc_angle = np.deg2rad(sca.inc_angle)
         self.f0 = f0 = sca.f0
         pol = self.pol = sca.pol
@@ -103,8 +102,14 @@ class DopscaSim:
             self.proc_raw_vv = np.zeros([self.az_steps, self.rg_samp], dtype=complex)
         self.NRCS_avg_vv = np.zeros(self.az_steps, dtype=float)
         self.NRCS_avg_hh = np.zeros(self.az_steps, dtype=float)
-        if self.scat_spec_enable:
-            self.rcs_spec_s = [nrcs.RCSKodis(self.inc_s[b], k0, s.dx, s.dy) for b in range(n_rep)]
+        if self.scat_spec_enable:                          # dopsca_raw.py:297-309
+            self.rcs_spec_s = []
+            for b in range(n_rep):
+                if self.scat_spec_mode == 'kodis':
+                    self.rcs_spec_s.append(nrcs.RCSKodis(self.inc_s[b], k0, s.dx, s.dy))
+                else:
+                    np.random.uniform(0., 2. * np.pi, size=[s.Ny, s.Nx])     # spec_ph0, unused
+                    self.rcs_spec_s.append(ka.RCSKA(self.scat_spec_mode, k0, s.x, s.y, s.dx, s.dy))
         if self.scat_bragg_enable:
             tau_c = closure.grid_coherence(oc.wind_U, s.dx, f0)
             self.rndscat_p = closure.RandomScatTS(tau_c, (n_rep, s.Ny, s.Nx), 1 / self.sub_len)
@@ -153,12 +158,25 @@ class DopscaSim:
             scene_hh = np.zeros([s.Ny, s.Nx], dtype=complex)
             scene_vv = np.zeros([s.Ny, s.Nx], dtype=complex)
             if self.scat_spec_enable:
-                Esn_sp = np.sqrt(4. * np.pi) * self.rcs_spec_s[blk].field(az_proj_angle, sr_surface, Diffx, Diffy,
-                                                                          Diffxx, Diffyy, Diffxy)
-                if self.do_hh:
-                    scene_hh += Esn_sp * range_scaling
-                if self.do_vv:
-                    scene_vv += Esn_sp * range_scaling
+                if self.scat_spec_mode == 'kodis':
+                    Esn_sp = np.sqrt(4. * np.pi) * self.rcs_spec_s[blk].field(az_proj_angle, sr_surface, Diffx,
+                                                                              Diffy, Diffxx, Diffyy, Diffxy)
+                    if self.do_hh:
+                        scene_hh += Esn_sp * range_scaling
+                    if self.do_vv:
+                        scene_vv += Esn_sp * range_scaling
+                else:                                      # dopsca_raw.py:426-445
+                    for do, pol_tmp in ((self.do_hh, 'hh'), (self.do_vv, 'vv')):
+                        if not do:
+                            continue
+                        Esn_sp = (np.exp(-1j * (2. * self.k0 * sr_surface)) * (4. * np.pi) ** 1.5 *
+                                  self.rcs_spec_s[blk].field(1, 1, pol_tmp[0], pol_tmp[1], self.inc_s[blk],
+                                                             self.inc_s[blk], az_proj_angle, az_proj_angle + np.pi,
+                                                             Dz, Diffx, Diffy, Diffxx, Diffyy, Diffxy))
+                        if pol_tmp == 'hh':
+                            scene_hh += Esn_sp * range_scaling
+                        else:
+                            scene_vv += Esn_sp * range_scaling
                 self.NRCS_avg_hh[az_step] += (np.sum(np.abs(Esn_sp) ** 2) / self.surface_area)
                 self.NRCS_avg_vv[az_step] += self.NRCS_avg_hh[az_step]
             if self.scat_bragg_enable:

@@ -89,6 +89,28 @@ def test_hmtf_stagewise(precision, tmp_path):
         np.testing.assert_allclose(nrcs_avg, nref, rtol=1e-5)
 
 
+@pytest.mark.parametrize("name,mode", [("dsc1", "fa"), ("dsc1", "spa"), ("dsc2", "fa")])
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_kirchhoff_stagewise(name, mode, precision, tmp_path):
+    """Kirchhoff specular (scat_spec_mode fa / spa; the reference's FIXME branch,
+    dopsca_raw.py:302-308, 426-448): the tangent-plane field at the block's incidence,
+    times exp(-2 i k0 r) (4 pi)^1.5 and the two-way spreading; dsc2 with the specular term
+    switched on gives both polarisations on a choppy surface."""
+    text = open(os.path.join(G, "cfg", name + ".cfg")).read()
+    text = text.replace("scat_spec_enable=False", "scat_spec_enable=True")
+    assert "scat_spec_mode=kodis" in text
+    cfg = tmp_path / ("%s_%s.cfg" % (name, mode))
+    cfg.write_text(text.replace("scat_spec_mode=kodis", "scat_spec_mode=%s" % mode))
+    raw, nrcs_avg, ref, nref = stagewise(name, precision, str(cfg))
+    if precision == "f64":
+        assert rel_l2(raw, ref) < 1e-10, rel_l2(raw, ref)
+        np.testing.assert_allclose(nrcs_avg, nref, rtol=1e-9)
+    else:
+        e, ph = rel_l2(raw, ref), max_phase(raw, ref)
+        assert e < 1e-4 and ph < 1e-3, (e, ph)
+        np.testing.assert_allclose(nrcs_avg, nref, rtol=1e-5)
+
+
 @pytest.mark.parametrize("precision", ["f64", "mixed"])
 def test_lut_mode_stagewise(precision, tmp_path):
     """Romeiser LUT mode (srg.use_lut): one table per range block at the block's mean
