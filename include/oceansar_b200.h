@@ -332,6 +332,18 @@ int ocs_pulse_error(const ocs_pulse_desc *desc);
 int ocs_skim_upsample(const double *x_d, const double *dop_d, double *y_d, double *D_d, int32_t N, int32_t G,
                       int32_t R, int32_t n_up, double prf, void *stream);
 
+/* Complex128 power-of-two FFTs of the SAR processor (the transforms of sar_focus,
+ * oceansar/radarsim/sar_processor.py:170, 176, 217, whose sizes optimize_fftsize pads to
+ * powers of two).  ocs_fft64_rows: in-place transform of nrows contiguous rows of length
+ * n, forward (inverse = 0, exp(-2 pi i k m / n)) or inverse (inverse = 1, exp(+...) and
+ * 1/n), as numpy.fft; n <= 8192 needs no scratch, longer rows (four-step) need
+ * ocs_fft64_workspace_bytes(nrows, n) bytes of scratch (-1: n not a power of two).
+ * ocs_transpose_c128: dst[b][c][r] = src[b][r][c] for batch rows x cols matrices (the
+ * azimuth transforms of a [pol][az][rg] cube run as row transforms of its transpose). */
+int64_t ocs_fft64_workspace_bytes(int64_t nrows, int64_t n);
+int ocs_fft64_rows(double *data, int64_t nrows, int64_t n, int32_t inverse, double *scratch, void *stream);
+int ocs_transpose_c128(const double *src, double *dst, int64_t batch, int64_t rows, int64_t cols, void *stream);
+
 /* Arithmetic-rate probe (no reference counterpart; a diagnostic of the device the two
  * precision forms run on): `blocks` x `threads` threads each run iters x 8 independent
  * FMAs in float64 (kind 0), float32 (kind 1) or packed float32x2 (kind 2, two FMAs per

@@ -55,6 +55,9 @@ SIGNATURES = {
     "ocs_skim_upsample": [c_ptr, c_ptr, c_ptr, c_ptr, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                           ctypes.c_int32, c_dbl, c_ptr],
     "ocs_fma_rate": [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_ptr, c_ptr],
+    "ocs_fft64_workspace_bytes": [c_i64, c_i64],
+    "ocs_fft64_rows": [c_ptr, c_i64, c_i64, ctypes.c_int32, c_ptr, c_ptr],
+    "ocs_transpose_c128": [c_ptr, c_ptr, c_i64, c_i64, c_i64, c_ptr],
     "ocs_rd_rcmc": [c_ptr, c_i64, ctypes.c_int32, ctypes.c_int32, c_ptr, c_ptr, c_dbl, c_ptr],
     "ocs_rd_azfilter": [c_ptr, c_i64, ctypes.c_int32, ctypes.c_int32, c_ptr, c_ptr],
     "ocs_batch_create": [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(c_ptr)],
@@ -66,7 +69,7 @@ SIGNATURES = {
     "ocs_batch_counters": [c_ptr, c_ptr, c_ptr],
 }
 _RESTYPE = {"ocs_version": ctypes.c_char_p, "ocs_surface_workspace_bytes": ctypes.c_int64,
-            "ocs_pulse_workspace_bytes": ctypes.c_int64}
+            "ocs_pulse_workspace_bytes": ctypes.c_int64, "ocs_fft64_workspace_bytes": ctypes.c_int64}
 
 _lib = None
 

@@ -5,9 +5,10 @@ Per channel, as the reference: zero-pad to power-of-two sizes, 2-D FFT, range-ce
 migration correction by a range-frequency phase ramp per Doppler bin, range IFFT, azimuth
 compression (hyperbolic phase, amplitude weighting over the Doppler bandwidth, antenna-
 pattern compensation), azimuth IFFT, crop, and removal of the azimuth samples outside the
-valid aperture.  The transforms are complex128 library FFTs on the device (cuFFT through
-torch); the two phase multiplications between them are the fused kernels ``ocs_rd_rcmc``
-and ``ocs_rd_azfilter``, which form the phase of each sample on the fly.  The filter
+valid aperture.  The transforms are the library's own complex128 power-of-two FFTs
+(``ocs_fft64_rows``; the azimuth ones on the cube's transpose, ``ocs_transpose_c128``);
+the two phase multiplications between them are the fused kernels ``ocs_rd_rcmc`` and
+``ocs_rd_azfilter``, which form the phase of each sample on the fly.  The filter
 vectors are computed on the host exactly as the reference computes them.  The SLC file is
 a netCDF classic ``ProcFile``.  Plot options of the [processing] section are accepted and
 ignored (no plotting here).
@@ -31,6 +32,29 @@ def sinc_1tx_nrx(sin_angle, L, f0, num_chan, field=False, sin_squint=0):
     bp_tx = sinc_bp(sin_angle - sin_squint, L, f0)
     bp_rx = sinc_bp(sin_angle - sin_squint, L / num_chan, f0)
     return bp_tx * bp_rx
+
+
+def _fft_rows(t, inverse):
+    """In-place complex128 FFT along the last (contiguous) dimension of t (``ocs_fft64_rows``)."""
+    n = int(t.shape[-1])
+    nrows = t.numel() // n
+    ws = int(_capi.load().ocs_fft64_workspace_bytes(nrows, n))
+    if ws < 0:
+        raise ValueError('FFT length %d is not a power of two' % n)
+    scratch = torch.empty(ws // 16, dtype=torch.complex128, device=t.device) if ws else None
+    _capi.call("ocs_fft64_rows", t.data_ptr(), nrows, n, int(inverse),
+               scratch.data_ptr() if scratch is not None else None, _device.stream_ptr())
+
+
+def _fft_az(t, inverse):
+    """In-place complex128 FFT along dimension 1 of a contiguous [pol][az][rg] cube: row
+    transforms of its [pol][rg][az] transpose (``ocs_transpose_c128``)."""
+    p, a, r = (int(v) for v in t.shape)
+    tt = torch.empty((p, r, a), dtype=t.dtype, device=t.device)
+    sp = _device.stream_ptr()
+    _capi.call("ocs_transpose_c128", t.data_ptr(), tt.data_ptr(), p, a, r, sp)
+    _fft_rows(tt, inverse)
+    _capi.call("ocs_transpose_c128", tt.data_ptr(), t.data_ptr(), p, r, a, sp)
 
 
 def focus_cube(raw, cfg, sr0):
@@ -67,12 +91,13 @@ def focus_cube(raw, cfg, sr0):
             beam_pattern = (sinc_bp(sin_az, sar.ant_L_tx, f0, field=True) *
                             sinc_bp(sin_az, sar.ant_L_rx, f0, field=True))
         rcmc_fa = sr0 / np.sqrt(1 - (fa * (l0 / 2.) / v_ground) ** 2.) - sr0
-        data = torch.fft.fft(torch.fft.fft(data, dim=-1), dim=-2).contiguous()
+        _fft_rows(data, False)
+        _fft_az(data, False)
         rcmc_d = torch.from_numpy(np.ascontiguousarray(rcmc_fa, dtype=np.float64)).to(dev)
         fr_d = torch.from_numpy(np.ascontiguousarray(fr, dtype=np.float64)).to(dev)
         _capi.call("ocs_rd_rcmc", data.data_ptr(), data.shape[0], az_size, rg_size, rcmc_d.data_ptr(),
                    fr_d.data_ptr(), float(C_LIGHT), sp)
-        data = torch.fft.ifft(data, dim=2)
+        _fft_rows(data, True)
         # azimuth compression filter (sar_processor.py:180-215)
         n_samp = 2 * (int(pr.doppler_bw / (fa[1] - fa[0])) / 2)
         weighting = (pr.az_weighting -
@@ -88,9 +113,8 @@ def focus_cube(raw, cfg, sr0):
         ph_ac = 4. * np.pi / l0 * sr0 * (np.sqrt(1. - (fa * l0 / 2. / v_ground) ** 2.) - 1.)
         h = np.ascontiguousarray(np.exp(1j * ph_ac) * weighting, dtype=np.complex128)
         h_d = torch.from_numpy(h).to(dev)
-        data = data.contiguous()
         _capi.call("ocs_rd_azfilter", data.data_ptr(), data.shape[0], az_size, rg_size, h_d.data_ptr(), sp)
-        data = torch.fft.ifft(data, dim=1)
+        _fft_az(data, True)
         data = data[:, :int(az_size_orig), :int(rg_size_orig)]
         n_val_az_2 = np.floor(pr.doppler_bw / 2. / (2. * v_ground ** 2. / l0 / sr0) * prf / 2.) * 2.
         data = data[:, int(n_val_az_2):int(az_size_orig - n_val_az_2 - 1), :]

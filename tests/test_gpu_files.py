@@ -48,7 +48,7 @@ def test_surface_state_roundtrip(tmp_path):
 
 
 def test_sar_focus_against_reference(tmp_path):
-    """sar_focus on the GPU (library FFTs + fused phase kernels) against the reference's SLC
+    """sar_focus on the GPU (own complex128 FFTs + fused phase kernels) against the reference's SLC
     of the same raw cube, through the raw and SLC files."""
     from oceansar_b200.ocs_io import ProcFile, RawFile
     from oceansar_b200.radarsim.sar_processor import sar_focus
