@@ -590,7 +590,7 @@ def run_workload(args):
 
 
 # ----------------------------------------------------------------------------------------
-def kernel_roofline(gen, precision, peak, peak_src, ms_per_step, pulses):
+def kernel_roofline(gen, precision, peak, peak_src, ms_per_step, pulses, workload="c2"):
     """Per-kernel CUDA-event timing (each launch bracketed alone on its stream; 3 windows of
     128 pulses, median) and the dominant kernel's roofline; plus a consistency check of the
     per-kernel sum against the scene's step time."""
@@ -617,7 +617,8 @@ def kernel_roofline(gen, precision, peak, peak_src, ms_per_step, pulses):
     dom = max(kern, key=lambda k: kern[k]["ms"])
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
+    # the committed DRAM bytes were captured on the default two-channel 2048^2 scene
+    if workload == "c2" and os.path.exists(tpath):
         try:
             traffic = json.load(open(tpath)).get(precision, {}).get(dom)
         except (ValueError, OSError):
@@ -742,7 +743,8 @@ def main():
         parity[args.precision] = {"rel_l2": rel_l2(got_main, ref_rows), "max_phase_rad": max_phase(got_main, ref_rows)}
 
     peak, peak_src = peak_hbm()
-    roofline = kernel_roofline(gen, args.precision, peak, peak_src, ms, c["pulses"])
+    roofline = kernel_roofline(gen, args.precision, peak, peak_src, ms, c["pulses"],
+                               workload="c1" if args.small else args.workload)
 
     # ---- end to end through the public API with host buffers ---------------------------
     s = gen.surface
