@@ -129,6 +129,18 @@ scat_bragg_spec=elfouhaily
 scat_bragg_spread=cos2s
 scat_bragg_d=0.125
 use_lut=False
+
+[processing]
+az_weighting=0.75
+doppler_bw=1000.
+plot_format=png
+plot_tex=False
+plot_save=False
+plot_path=plots
+plot_raw=False
+plot_rcmc_dopp=False
+plot_rcmc_time=False
+plot_image_valid=False
 """
 
 
@@ -378,6 +390,51 @@ def accumulation_roofline(peak, peak_src, n=4096, nbins=2048, reps=10):
     out["c64"]["traffic"] = traffic
     out.update({"kernel": "chan_profile_2d_kernel", "grid": [n, n], "nbins": nbins, "peak": peak,
                 "peak_source": peak_src, "bound": "hbm"})
+    return out
+
+
+def sar_focus_report(gen, cfg_path, peak, peak_src, reps=3):
+    """The SAR processor (``sar_focus``, own complex128 FFTs) on the scene's raw cube: wall
+    time of ``focus_cube`` over all channels (host cube in, SLC out, as ``sar_focus`` runs
+    it), and the device time of its range (row) and azimuth (transpose, rows, transpose)
+    transforms on one channel's padded cube, with their HBM rooflines: a row transform
+    reads and writes the cube once (2 x 16 B per sample), an azimuth transform three times
+    (its two transposes and the rows)."""
+    import time
+    import torch
+    from oceansar_b200.ocs_io import ConfigFile
+    from oceansar_b200.radarsim.sar_processor import _fft_az, _fft_rows, focus_cube
+    from oceansar_b200.utils.misc import optimize_fftsize
+    cfg = ConfigFile(cfg_path)
+    raw = gen.raw()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    slc = focus_cube(raw, cfg, gen.sr_near)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    npol, nch, naz, nrg = raw.shape
+    a, r = (int(v) for v in optimize_fftsize((naz, nrg)))
+    g = torch.Generator(device="cuda").manual_seed(3)
+    cube = torch.randn(npol, a, r, dtype=torch.complex128, device="cuda", generator=g)
+    out = {"channels": int(nch), "cube": [int(npol), a, r], "focus_s": round(wall, 4),
+           "samples_per_s": float(npol * nch * a * r / wall), "slc_shape": list(slc.shape),
+           "kernel": "fft64_rows_kernel (+ transpose_c128_kernel)", "peak": peak, "peak_source": peak_src}
+    cube_bytes = cube.numel() * 16
+    for name, fn, passes in (("range_fft", lambda: _fft_rows(cube, False), 1),
+                             ("azimuth_fft", lambda: _fft_az(cube, False), 3)):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        gbs = 2 * passes * cube_bytes / (ms * 1e-3) / 1e9
+        out[name] = {"ms": round(ms, 4), "GBps": round(gbs, 1), "frac": round(gbs / peak, 4),
+                     "alg_bytes": 2 * passes * cube_bytes}
+    del cube
     return out
 
 
@@ -782,6 +839,9 @@ def main():
     e2e = {"value": echoes(c) * world / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms}
 
+    # ---- the SAR processor on this scene's raw cube ---------------------------------------
+    focus = sar_focus_report(gen, cfg_path, peak, peak_src) if extras else None
+
     # ---- FP64 drop-in form on the same workload (secondary figure) ---------------------
     fp64 = None
     if not args.no_fp64 and args.precision == "mixed":
@@ -833,7 +893,7 @@ def main():
                            "l2": "inputs larger than L2 (~0.5 GB working set)",
                            "graph": "whole scene replayed from one CUDA graph"},
                 "clocks": clk, "e2e": e2e, "gpu_launches": launches, "roofline": roofline,
-                "cpu_baseline": cpu, "parity": parity or None, "fp64": fp64, "fp_rates": rates, "accumulation": accum,
+                "cpu_baseline": cpu, "parity": parity or None, "fp64": fp64, "fp_rates": rates, "accumulation": accum, "sar_focus": focus,
                 "batched": batched, "serving": serving}
         print(json.dumps(line), flush=True)
     if world > 1:

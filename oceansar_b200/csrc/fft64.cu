@@ -29,12 +29,26 @@ fft64_rows_kernel(double2 *__restrict__ data, int n, int logn, int inverse, doub
     double2 *buf = fsm, *tw = fsm + n;
     double2 *x = data + (long long)blockIdx.x * n;
     const int T = blockDim.x;
-    // twiddles exp(-+2 pi i k / n), k < n/2 (2k/n is exact for a power-of-two n)
+    // twiddles exp(-+2 pi i k / n), k < n/2 (2k/n is exact for a power-of-two n): the first
+    // octant from sincospi, the rest by the exact symmetries of cos and sin about pi/4,
+    // pi/2 and pi (n >= 8)
     const double sg = inverse ? 1.0 : -1.0;
-    for (int k = threadIdx.x; k < n / 2; k += T) {
-        double s, c;
-        sincospi(2.0 * (double)k / (double)n, &s, &c);
-        tw[k] = make_double2(c, sg * s);
+    if (n < 8) {
+        for (int k = threadIdx.x; k < n / 2; k += T) {
+            double s, c;
+            sincospi(2.0 * (double)k / (double)n, &s, &c);
+            tw[k] = make_double2(c, sg * s);
+        }
+    } else {
+        const int q = n / 4;
+        for (int k = threadIdx.x; k <= n / 8; k += T) {
+            double s, c;
+            sincospi(2.0 * (double)k / (double)n, &s, &c);
+            tw[k] = make_double2(c, sg * s);                  // theta
+            tw[q - k] = make_double2(s, sg * c);              // pi/2 - theta
+            if (k > 0) tw[q + k] = make_double2(-s, sg * c);                 // pi/2 + theta
+            if (k > 0 && 8 * k < n) tw[2 * q - k] = make_double2(-c, sg * s);  // pi - theta
+        }
     }
     for (int j = threadIdx.x; j < n; j += T) buf[__brev((unsigned)j) >> (32 - logn)] = x[j];
     __syncthreads();

@@ -858,7 +858,14 @@ batch_pulse_mixed_kernel(const __grid_constant__ BatchRef b) {
     double spec_sum = 0.0, bragg_sum[2] = {0.0, 0.0};
     unsigned rseq = 0;
     bool bad = false;
-    mix_tile<NOUT, true, false>(pa, nullptr, nullptr, tile, g.tile_rows, sm, rseq, bad, spec_sum, bragg_sum);
+    // the fast configurations of the single-scene kernel, chosen per CTA from its slot
+    const bool fast = pa.do_kodis && pa.do_bragg && pa.npol == 1 && pa.nout == NOUT && !pa.lut && !pa.use_hmtf;
+    if (fast && !pa.any_xti)
+        mix_tile<NOUT, true, false, 2, 1>(pa, nullptr, nullptr, tile, g.tile_rows, sm, rseq, bad, spec_sum, bragg_sum);
+    else if (fast)
+        mix_tile<NOUT, true, false, 2, 2>(pa, nullptr, nullptr, tile, g.tile_rows, sm, rseq, bad, spec_sum, bragg_sum);
+    else
+        mix_tile<NOUT, true, false>(pa, nullptr, nullptr, tile, g.tile_rows, sm, rseq, bad, spec_sum, bragg_sum);
     if (pa.out0 == 0) {
         if (pa.do_kodis) block_atomic_sum(spec_sum, &pa.nrcs_spec[pa.az_step], sm.sred);
         if (pa.do_bragg && pa.refresh)
@@ -917,12 +924,14 @@ static int tile_rows_for(int nx, int ny, int cols, int resident) {
 template <int NOUT, bool KODIS>
 static int launch_pulse_mixed(PulseArgs a, const MixMaps &maps, float *lo_row, cudaStream_t st) {
     const size_t smem = mix_smem_bytes<NOUT>(a.nch, kPulseRows);
-    // the common configuration (one polarisation, no XTI phase, every output in this pass,
-    // Kodis and direct Romeiser Bragg, no hMTF) runs an instantiation with those fixed
-    const bool fast = KODIS && a.do_kodis && a.do_bragg && a.npol == 1 && !a.any_xti && a.nout == NOUT && !a.lut &&
-                      !a.use_hmtf;
-    auto k = fast ? (a.refresh ? pulse_mixed_kernel<NOUT, KODIS, 1, KODIS> : pulse_mixed_kernel<NOUT, KODIS, 0, KODIS>)
-                  : (a.refresh ? pulse_mixed_kernel<NOUT, KODIS, 1> : pulse_mixed_kernel<NOUT, KODIS, 0>);
+    // the common configurations (one polarisation, every output in this pass, Kodis and
+    // direct Romeiser Bragg, no hMTF; without (1) or with (2) XTI channels) run
+    // instantiations with those fixed
+    const bool fast = KODIS && a.do_kodis && a.do_bragg && a.npol == 1 && a.nout == NOUT && !a.lut && !a.use_hmtf;
+    constexpr int F1 = KODIS ? 1 : 0, F2 = KODIS ? 2 : 0;
+    auto k = !fast ? (a.refresh ? pulse_mixed_kernel<NOUT, KODIS, 1> : pulse_mixed_kernel<NOUT, KODIS, 0>)
+             : !a.any_xti ? (a.refresh ? pulse_mixed_kernel<NOUT, KODIS, 1, F1> : pulse_mixed_kernel<NOUT, KODIS, 0, F1>)
+                          : (a.refresh ? pulse_mixed_kernel<NOUT, KODIS, 1, F2> : pulse_mixed_kernel<NOUT, KODIS, 0, F2>);
     if (ensure_smem((const void *)k, smem) != cudaSuccess) return OCS_ERR_CUDA;
     const int resident = resident_ctas((const void *)k, kMixCols, smem);
     if (resident <= 0) return OCS_ERR_CUDA;

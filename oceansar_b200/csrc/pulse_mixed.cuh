@@ -377,7 +377,7 @@ OCS_D double srs_f64(double sr_c, double cos_i, double sin_i, double az, double 
 // the top of the row (the scene batch, whose slots keep no tensor maps).  REFRESH: 0 = a
 // pulse that reads the stored sqrt(RCS), 1 = a Bragg-refresh pulse (the Romeiser model is
 // compiled only into these), 2 = decided at run time from a.refresh (the scene batch).
-template <int NOUT, bool KODIS, bool TMA = true, int REFRESH = 2, bool FAST = false>
+template <int NOUT, bool KODIS, bool TMA = true, int REFRESH = 2, int FAST = 0>
 OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int tile, int tile_rows,
                     const MixSmem<NOUT> &sm, unsigned &rseq, bool &bad, double &spec_sum, double (&bragg_sum)[2]) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -693,16 +693,17 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
             // ---- channels: antenna pattern x ATI phase (row) x XTI phase (facet) ----
             c64 coef[NOUT];
             float wave_dinc = 0.f;
-            if (!FAST && a.any_xti) wave_dinc = (dz * sin_i + dx * sin_i) * inv_sr0;
+            if (FAST == 2 || (FAST == 0 && a.any_xti)) wave_dinc = (dz * sin_i + dx * sin_i) * inv_sr0;
 #pragma unroll
             for (int k = 0; k < NOUT; ++k) {
                 if (FAST || k < a.nout) {
-                    // fast configuration: one polarisation, no XTI phase, output k is channel out0 + k
-                    const unsigned okb = FAST ? (unsigned)(a.out0 + k) : outs >> (5 * k);
+                    // fast configurations: one polarisation, output k is channel out0 + k (mode 1:
+                    // no XTI phase; mode 2: the XTI flags of the tile's output word)
+                    const unsigned okb = FAST == 1 ? (unsigned)(a.out0 + k) : outs >> (5 * k);
                     const int c = okb & 7;
                     const c64 f = {rt[kMixRT + 2 * c], rt[kMixRT + 2 * c + 1]};
                     c64 v = cmul((!FAST && (okb & 8)) ? scene[1] : scene[0], f);
-                    if (!FAST && (okb & 16)) {
+                    if (FAST != 1 && (okb & 16)) {
                         const float ph = wrap_pi(kxti[k] * (dinc0 + wave_dinc));
                         float s, cc;
                         __sincosf(ph, &s, &cc);
@@ -788,7 +789,7 @@ template <int NOUT> OCS_D void mix_init(const MixSmem<NOUT> &sm) {
     __syncthreads();
 }
 
-template <int NOUT, bool KODIS, int REFRESH, bool FAST = false>
+template <int NOUT, bool KODIS, int REFRESH, int FAST = 0>
 __global__ void __launch_bounds__(kMixCols, NOUT < 4 ? 4 : 2)
 pulse_mixed_kernel(const __grid_constant__ PulseArgs a, const __grid_constant__ MixMaps maps, float *lo_row) {
     extern __shared__ __align__(128) unsigned char smem[];
