@@ -440,6 +440,7 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
         const float inv_bs = (float)a.inv_binsize;
         const float khi = (float)(2.0 * a.k0), klo = (float)(2.0 * a.k0 - (double)khi);
         const float hdx = (float)a.kodis.hdx, hdy = (float)a.kodis.hdy, inv_sr0 = (float)(1.0 / a.sr0);
+        const float hr = (float)(0.5 * a.kodis.R_re), hi_ = (float)(0.5 * a.kodis.R_im);   // R / 2
         const long long npix = (long long)a.nx * a.ny;
         float *scat = reinterpret_cast<float *>(a.scat);
         const bool refresh = REFRESH == 2 ? a.refresh != 0 : REFRESH == 1;
@@ -629,7 +630,6 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
                         const float sgn = J > 0.f ? (float)((dxx > 0.f) - (dxx < 0.f)) : 0.f;
                         const float fac = __fadd_rn(__fadd_rn(__fmul_rn(diffx, diffx), __fmul_rn(diffy, diffy)), 1.f);
                         const float amp = fac * 3.5449077018110318f / sqrtf(Ja);    // sqrt(4 pi)
-                        const float hr = (float)(0.5 * a.kodis.R_re), hi_ = (float)(0.5 * a.kodis.R_im);
                         // (R/2) eps fac e^{i ph} / sqrt|J|, eps = sign(Dxx) or 1j
                         const c64 re = J > 0.f ? c64{hr * sgn, hi_ * sgn} : c64{-hi_, hr};
                         const c64 e = cmul(re, c64{c * amp, s * amp});
