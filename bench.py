@@ -388,7 +388,7 @@ def accumulation_roofline(peak, peak_src, n=4096, nbins=2048, reps=10):
     except (OSError, ValueError, KeyError):
         traffic = None
     out["c64"]["traffic"] = traffic
-    out.update({"kernel": "chan_profile_2d_kernel", "grid": [n, n], "nbins": nbins, "peak": peak,
+    out.update({"kernel": "chan_profile_2d_hist_kernel", "grid": [n, n], "nbins": nbins, "peak": peak,
                 "peak_source": peak_src, "bound": "hbm"})
     return out
 

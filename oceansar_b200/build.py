@@ -6,6 +6,7 @@ shared library exporting the C ABI declared in ``include/oceansar_b200.h``.  Obj
 rebuilt when a source or header is newer than the library.  nvcc cross-compiles, so no GPU
 is needed to build.
 """
+import concurrent.futures
 import glob
 import os
 import shutil
@@ -42,19 +43,23 @@ def build(force=False, verbose=False, ptxas_info=False):
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     dep_t = _newest_dep()
     objs = []
-    rebuilt = False
+    cmds = []
     for src in srcs:
         obj = os.path.join(OBJDIR, os.path.basename(src)[:-3] + ".o")
         objs.append(obj)
         if (not force and os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(src)
                 and os.path.getmtime(obj) >= dep_t):
             continue
-        cmd = [nvcc()] + ARCH + NVCC_FLAGS + (["-Xptxas", "-v"] if ptxas_info else []) + \
-            ["-c", src, "-o", obj]
-        if verbose:
-            print(" ".join(cmd))
-        subprocess.check_call(cmd)
-        rebuilt = True
+        cmds.append([nvcc()] + ARCH + NVCC_FLAGS + (["-Xptxas", "-v"] if ptxas_info else []) +
+                    ["-c", src, "-o", obj])
+    # one nvcc per translation unit, run side by side
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for cmd in cmds:
+            if verbose:
+                print(" ".join(cmd))
+        for f in [ex.submit(subprocess.check_call, cmd) for cmd in cmds]:
+            f.result()
+    rebuilt = bool(cmds)
     if rebuilt or force or not os.path.exists(LIB) or \
             any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
         cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]

@@ -177,3 +177,39 @@ def test_two_dimensional_c64(misaligned):
                o_d.data_ptr(), nbins, st)
     out = o_d.cpu().numpy().astype(np.float64)
     assert rel(out[:, 0] + 1j * out[:, 1], ref) < 1e-5
+
+
+@pytest.mark.parametrize("spacing,jitter", [(3.0, 0.8), (10.0, 0.8), (0.57, 40.0), (1.4, 5.0)],
+                         ids=["1.1bins_per_col", "3.7bins_per_col", "scattered_40m", "0.5bins_per_col_5m"])
+@pytest.mark.parametrize("precision", ["f64", "c64"])
+def test_two_dimensional_steep_and_scattered(spacing, jitter, precision):
+    """The [ny, nx] kernel on layouts whose columns step more than a bin apart (the strips
+    are walked in narrower column groups) and whose ranges scatter far from their column
+    (many facets take the per-tap path): same sum as the flattened oracle."""
+    import ctypes
+    from oceansar_b200 import _capi
+    from oceansar_b200.radarsim import range_profile as rp
+    ny, nx = 301, 517
+    rs = np.random.RandomState(11)
+    col = np.arange(nx) * spacing + 40.0
+    row = ((np.arange(ny) - ny / 2) ** 2) / 4e4
+    srg = col[None, :] + row[:, None] + jitter * rs.randn(ny, nx)
+    scene = rs.randn(ny, nx) + 1j * rs.randn(ny, nx)
+    nbins = int((srg.max() + 60.0) / 2.725)
+    sinc = rp.calc_sinc_vec(8, 20, Fs=1.1)
+    ref = np.zeros(nbins, complex)
+    orp.chan_profile(srg.ravel(), scene.ravel(), 2.725, 0.0, sinc, 8, 20, ref)
+    if precision == "f64":
+        out = np.zeros(nbins, complex)
+        rp.chan_profile_numba(srg, scene, 2.725, 0.0, sinc, 8, 20, out)
+        assert rel(out, ref) < 1e-10
+        return
+    s_d = torch.tensor(srg, dtype=torch.float64, device="cuda")
+    c_d = torch.tensor(np.stack([scene.real, scene.imag], -1), dtype=torch.float32, device="cuda")
+    w_d = torch.tensor(sinc, dtype=torch.float32, device="cuda")
+    o_d = torch.zeros(nbins, 2, dtype=torch.float32, device="cuda")
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _capi.call("ocs_chan_profile_2d_c64", s_d.data_ptr(), c_d.data_ptr(), ny, nx, 2.725, 0.0, w_d.data_ptr(), 8, 20,
+               o_d.data_ptr(), nbins, st)
+    out = o_d.cpu().numpy().astype(np.float64)
+    assert rel(out[:, 0] + 1j * out[:, 1], ref) < 1e-5
