@@ -384,10 +384,11 @@ def accumulation_roofline(peak, peak_src, n=4096, nbins=2048, reps=10):
                      "frac": round(gbs / peak, 4), "alg_bytes_per_facet": bpf}
         del sc, o
     try:
-        traffic = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))["accumulation"]["c64"]
+        traffic = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))["accumulation"]
     except (OSError, ValueError, KeyError):
-        traffic = None
-    out["c64"]["traffic"] = traffic
+        traffic = {}
+    for name in ("c64", "f64"):
+        out[name]["traffic"] = traffic.get(name)
     out.update({"kernel": "chan_profile_2d_hist_kernel", "grid": [n, n], "nbins": nbins, "peak": peak,
                 "peak_source": peak_src, "bound": "hbm"})
     return out

@@ -225,10 +225,11 @@ static int launch_chan_profile_2d_regs(const double *srg, const void *scene, lon
 // whose bin is `bin` and whose LUT index is l,
 //     out[b] = sum over facets of sinc[lut + j ovs] c,  j = b - (bin - taps/2)
 //            = sum_{j < taps} sum_{l <= ovs} sinc[l + j ovs] H[b + taps/2 - j][l].
-// A CTA adds each facet's coefficient once into a shared-memory H that spans kHistBins<T>
-// bins around its tile of 128 columns x tile_rows rows (two shared atomic adds per facet
-// instead of a multiply-add per tap and window slot, and no register window, so eight CTAs
-// fit per SM), then convolves H with the oversampled pulse once per tile and adds the result
+// A CTA adds each facet's coefficient once into a shared-memory H that spans kHB bins
+// around its tile of 128 columns x tile_rows rows (two shared atomic adds per facet into
+// separate real and imaginary planes, instead of a multiply-add per tap and window slot; no
+// register window, so 8 to 12 CTAs fit per SM), then convolves H with the oversampled pulse
+// once per tile and adds the result
 // to the output with global atomics.  A tile whose first and last rows span more bins than H
 // holds is walked in narrower column groups (64 or 32 columns, two or four rows per step,
 // one H each); facets whose bin still falls outside H, and facets with non-finite
@@ -238,7 +239,9 @@ static int launch_chan_profile_2d_regs(const double *srg, const void *scene, lon
 constexpr int kHThreads = 128;
 constexpr int kHRB = 4;             // rows of loads in flight per thread
 constexpr int kHB = 64;             // bins held by H
-template <typename T> __host__ __device__ constexpr int hist_ctas_per_sm() { return 8; }
+// Resident CTAs per SM: single precision fits twelve within 40 registers; float64 keeps
+// eight (its division and 16-byte loads need the registers).
+template <typename T> __host__ __device__ constexpr int hist_ctas_per_sm() { return sizeof(T) == 4 ? 12 : 8; }
 
 // floor(bin_f) and round_half_even(ovs (1 - frac)) without conversion instructions: adding
 // M = 1.5 * 2^52 rounds a value below 2^51 in magnitude to an integer held in the low word
