@@ -559,7 +559,7 @@ def batched_report(prep, tuner, precision, n_scenes=64, seed=1):
     torch.cuda.empty_cache()
     return {"scenes": len(specs), "seed": seed, "echoes": ech, "device_s": dev_s, "value": ech / dev_s,
             "unit": UNIT, "steps": steps, "pulse_block": block,
-            "tile_rows": {"%dx%d/%d" % k: v for k, v in rows.items()}, "tune_s": t_tune,
+            "tile_rows": {"%dx%d/%d%s" % (k[0], k[1], k[2], "/ka" if k[3] else ""): v for k, v in rows.items()}, "tune_s": t_tune,
             "host_prep_s": host_prep, "launches_per_step_first": launches0, "gpu_launches": kernel_launches,
             "e2e": {"value": ech / e2e_s, "unit": UNIT, "h2d_bytes": int(h2d), "d2h_bytes": int(d2h),
                     "seconds": e2e_s}}

@@ -426,7 +426,9 @@ int ocs_rd_azfilter(double *data_d, int64_t npol, int32_t naz, int32_t nrg, cons
  * and leave the slots (as long as the set of grid sizes and output widths in use stays
  * the same).  No counterpart in the reference: its sar_raw
  * (oceansar/radarsim/sar_raw_nompi.py:32-641) runs the same per-pulse body for one scene
- * per call; a slot runs exactly that body (ocs_surface_update + ocs_pulse) at each pulse. */
+ * per call; a slot runs exactly that body (ocs_surface_update + ocs_pulse) at each pulse.
+ * SAR scenes with Kodis or Kirchhoff specular (spec_mode 0 / 1 / 2) and Bragg scattering;
+ * Kirchhoff scenes form launch classes of their own; DopSCA and SKIM pulses are rejected. */
 typedef struct {
     const ocs_surface_desc *surface;   /* as for ocs_surface_update; t, add and swell_rot are
                                           taken per pulse from the tables below           */

@@ -19,6 +19,7 @@ __global__ void batch_advance_kernel(const __grid_constant__ BatchRef b) {
 struct HostSlot {
     bool used = false;
     int rows_key = -1, cols_key = -1, prog = 0, nout = 0;
+    int kind = kSlotStd;                          // pulse-kernel class
     long long rows_items = 0, cols_items = 0;     // work items of the row / column pass
     long long pulse_items[5] = {0, 0, 0, 0, 0};   // pulse-kernel items per width class
     long long rows_smem = 0, cols_smem = 0;
@@ -96,8 +97,9 @@ extern "C" int ocs_batch_set(ocs_batch *b, int32_t slot, const ocs_scene_desc *s
     if (sd->nx != pd->nx || sd->ny != pd->ny) return OCS_ERR_ARG;
     const int tile_rows = sc->tile_rows == 0 ? 64 : sc->tile_rows;
     if (tile_rows < 1 || tile_rows > 128) return OCS_ERR_ARG;
-    if (b->precision == OCS_PREC_MIXED && !pulse_split_ok(pd)) return OCS_ERR_UNSUPPORTED;
     HostSlot h;
+    h.kind = pulse_kind(pd);
+    if (b->precision == OCS_PREC_MIXED && h.kind == kSlotStd && !pulse_split_ok(pd)) return OCS_ERR_UNSUPPORTED;
     h.rows_key = surface_key(sd->nx);
     h.cols_key = surface_key(sd->ny);
     if (h.rows_key < 0 || h.cols_key < 0) return OCS_ERR_UNSUPPORTED;
@@ -140,6 +142,7 @@ extern "C" int ocs_batch_set(ocs_batch *b, int32_t slot, const ocs_scene_desc *s
     s.nout = h.nout;
     s.tile_rows = tile_rows;
     s.prog = h.prog;
+    s.kind = h.kind;
     s.t_tab = sc->t_d;
     s.add_tab = sc->add_d;
     s.swrot_tab = reinterpret_cast<const float2 *>(sc->swell_rot_d);
@@ -175,7 +178,7 @@ extern "C" int ocs_batch_clear(ocs_batch *b, int32_t slot, void *stream) {
 }
 
 // Launch classes of the slots in use: row / column transform lengths (with the largest
-// shared memory each needs) and pulse-kernel widths.
+// shared memory each needs) and pulse-kernel (class, width) pairs.
 struct ClassLaunch {
     long long smem = 0;     // largest shared memory of the class's slots
     long long items = 0;    // items of all the class's slots (the grid)
@@ -184,13 +187,13 @@ struct ClassLaunch {
 struct BatchPlan {
     std::vector<std::pair<std::pair<int, int>, ClassLaunch>> rows;   // (length, program)
     std::vector<std::pair<int, ClassLaunch>> cols;
-    std::vector<std::pair<int, long long>> widths;    // (width class, items)
+    std::vector<std::pair<std::pair<int, int>, long long>> widths;    // ((kind, width class), items)
 };
 
 static BatchPlan batch_plan(const ocs_batch *b) {
     std::map<std::pair<int, int>, ClassLaunch> rows;
     std::map<int, ClassLaunch> cols;
-    std::map<int, long long> widths;
+    std::map<std::pair<int, int>, long long> widths;
     for (const HostSlot &h : b->host) {
         if (!h.used) continue;
         ClassLaunch &r = rows[std::make_pair(h.rows_key, h.prog)];
@@ -200,7 +203,7 @@ static BatchPlan batch_plan(const ocs_batch *b) {
         c.smem = std::max(c.smem, h.cols_smem);
         c.items += h.cols_items;
         for (int w : {1, 2, 4})
-            if (h.pulse_items[w] > 0) widths[w] += h.pulse_items[w];
+            if (h.pulse_items[w] > 0) widths[std::make_pair(h.kind, w)] += h.pulse_items[w];
     }
     BatchPlan p;
     p.rows.assign(rows.begin(), rows.end());
@@ -235,7 +238,9 @@ extern "C" int ocs_batch_step(ocs_batch *b, int32_t pulses, void *stream) {
                 return st;
         if ((st = batch_launch_pulse_rows(ref, b->precision, cs)) != OCS_OK) return st;
         for (const auto &w : p.widths)
-            if ((st = batch_launch_pulse(ref, b->precision, w.first, (int)w.second, cs)) != OCS_OK) return st;
+            if ((st = batch_launch_pulse(ref, b->precision, w.first.first, w.first.second, (int)w.second, cs)) !=
+                OCS_OK)
+                return st;
         batch_advance_kernel<<<1, 256, 0, cs>>>(ref);
         if (cudaGetLastError() != cudaSuccess) return OCS_ERR_CUDA;
     }

@@ -18,6 +18,11 @@ namespace ocs {
 
 constexpr int kMaxSlots = 256;
 
+// Pulse-kernel classes of a slot: Kodis / Bragg scenes, and scenes with the Kirchhoff
+// specular term (facet approach or stationary phase), which run their own instantiation.
+constexpr int kSlotStd = 0;
+constexpr int kSlotKa = 1;
+
 // Flags of the per-pulse table.
 constexpr int kFlagSurface = 1;     // synthesise the surface at this pulse
 constexpr int kFlagRefresh = 2;     // refresh the Bragg RCS at this pulse
@@ -33,6 +38,7 @@ struct SlotState {
     int nout;                       // npol * nch
     int tile_rows;                  // rows per pulse-kernel tile
     int prog;                       // field program of the row pass
+    int kind;                       // pulse-kernel class: kSlotStd or kSlotKa
     const float *t_tab;             // [az_steps] surface time (float32)
     const float *add_tab;           // [az_steps][nfields] additive field terms
     const float2 *swrot_tab;        // [az_steps] swell rotation exp(-i w_s t), or null
@@ -99,9 +105,11 @@ int batch_launch_rows(const BatchRef &b, int key, int prog, int grid, size_t sme
 int batch_launch_cols(const BatchRef &b, int key, int grid, size_t smem, cudaStream_t st);
 int batch_launch_pulse_rows(const BatchRef &b, int precision, cudaStream_t st);
 // Whether a scene's pulse descriptor takes the split-range mixed kernel (required of every
-// scene of a mixed-precision batch).
+// Kodis / Bragg scene of a mixed-precision batch).
 bool pulse_split_ok(const ocs_pulse_desc *d);
-int batch_launch_pulse(const BatchRef &b, int precision, int width, int grid, cudaStream_t st);
+// Pulse-kernel class of a scene (kSlotStd / kSlotKa).
+int pulse_kind(const ocs_pulse_desc *d);
+int batch_launch_pulse(const BatchRef &b, int precision, int kind, int width, int grid, cudaStream_t st);
 // Pulse-kernel items (groups of a width class x facet tiles) of one scene.
 int batch_pulse_items(int nx, int ny, int tile_rows, int nout, int precision, int width);
 // Row / column class key of a transform length (the length for compiled power-of-two

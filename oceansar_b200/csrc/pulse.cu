@@ -758,24 +758,27 @@ __global__ void batch_pulse_rows_kernel(const __grid_constant__ BatchRef b) {
         const PulseArgs &a = *static_cast<const PulseArgs *>(g.pargs);
         const int y = (item - pref[s]) * blockDim.x + threadIdx.x;
         if (y < a.ny) {
-            if (MIXED) mix_row(a, g.aznow_tab[g.counter], y);
+            // Kirchhoff slots run the float64-range kernel, which reads the float64 table only
+            if (MIXED && g.kind == kSlotStd) mix_row(a, g.aznow_tab[g.counter], y);
             else pulse_row(a, g.aznow_tab[g.counter], y);
         }
     }
 }
 
-// One launch covers every live slot's groups of width class NOUT; the host sizes the grid
-// for all slots in use and each CTA takes one (slot, group, tile) item.
-template <typename T, int NOUT, int S>
+// One launch covers every live slot's groups of width class NOUT among the slots of its
+// pulse-kernel class (MODE = kModeStd: Kodis / Bragg slots, kModeKa: Kirchhoff slots); the
+// host sizes the grid for all slots in use and each CTA takes one (slot, group, tile) item.
+template <typename T, int NOUT, int S, int MODE = kModeStd>
 __global__ void __launch_bounds__(kPulseCols, (sizeof(T) == 4 && NOUT < 4) ? 4 : 2)
 batch_pulse_kernel(const __grid_constant__ BatchRef b) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ PulseArgs pa;
     __shared__ int pref[kMaxSlots + 1];
     constexpr int G = sizeof(T) == 4 ? 4 : 2;
+    constexpr int kind = (MODE & kModeKa) ? kSlotKa : kSlotStd;
     const int total = scan_slots(b, pref, [](const SlotState &g) {
         int o, w;
-        return slot_live(g) ? groups_of_class(g.nout, G, NOUT, -1, o, w) * slot_pulse_tiles(g) : 0;
+        return (slot_live(g) && g.kind == kind) ? groups_of_class(g.nout, G, NOUT, -1, o, w) * slot_pulse_tiles(g) : 0;
     });
     const int item = blockIdx.x;
     if (item >= total) return;
@@ -807,7 +810,7 @@ batch_pulse_kernel(const __grid_constant__ BatchRef b) {
     const PulseSmem<T> sm = pulse_smem<T, NOUT, S, kPulseRowsMax>(smem, kMaxCh);
     build_wtab<T, S>(sm.wtab, pa.sinc, kSincTaps, kSincOvs);
     double spec_sum = 0.0, bragg_sum[2] = {0.0, 0.0};
-    pulse_tile<T, NOUT, S, kPulseRowsMax>(pa, tile, g.tile_rows, sm, spec_sum, bragg_sum);
+    pulse_tile<T, NOUT, S, kPulseRowsMax, MODE>(pa, tile, g.tile_rows, sm, spec_sum, bragg_sum);
     pulse_nrcs<T>(pa, sm, spec_sum, bragg_sum);
 }
 
@@ -823,7 +826,8 @@ batch_pulse_mixed_kernel(const __grid_constant__ BatchRef b) {
     constexpr int G = 4;
     const int total = scan_slots(b, pref, [](const SlotState &g) {
         int o, w;
-        return slot_live(g) ? groups_of_class(g.nout, G, NOUT, -1, o, w) * slot_pulse_tiles(g) : 0;
+        return (slot_live(g) && g.kind == kSlotStd) ? groups_of_class(g.nout, G, NOUT, -1, o, w) * slot_pulse_tiles(g)
+                                                    : 0;
     });
     const int item = blockIdx.x;
     if (item >= total) return;
@@ -1173,10 +1177,10 @@ static int batch_pulse_mixed_n(const BatchRef &b, int grid, cudaStream_t st) {
     return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
 }
 
-template <typename T, int NOUT, int S>
+template <typename T, int NOUT, int S, int MODE = kModeStd>
 static int batch_pulse_n(const BatchRef &b, int grid, cudaStream_t st) {
     const size_t smem = pulse_smem_bytes<T, NOUT, S, kPulseRowsMax>(kMaxCh);
-    auto k = batch_pulse_kernel<T, NOUT, S>;
+    auto k = batch_pulse_kernel<T, NOUT, S, MODE>;
     if (ensure_smem((const void *)k, smem) != cudaSuccess) return OCS_ERR_CUDA;
     k<<<grid, kPulseCols, smem, st>>>(b);
     return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
@@ -1189,8 +1193,26 @@ int batch_pulse_items(int nx, int ny, int tile_rows, int nout, int precision, in
     return groups * ((nx + kPulseCols - 1) / kPulseCols) * ((ny + tile_rows - 1) / tile_rows);
 }
 
-int batch_launch_pulse(const BatchRef &b, int precision, int width, int grid, cudaStream_t st) {
+int pulse_kind(const ocs_pulse_desc *d) { return (d->do_kodis && d->spec_mode != 0) ? kSlotKa : kSlotStd; }
+
+int batch_launch_pulse(const BatchRef &b, int precision, int kind, int width, int grid, cudaStream_t st) {
     if (grid < 1) return OCS_OK;
+    if (kind == kSlotKa) {
+        // Kirchhoff scenes: float64 ranges and phases in both precisions, as their single-scene
+        // pulses run (float32 for the rest in the mixed form)
+        if (precision == OCS_PREC_F64) {
+            if (width == 1) return batch_pulse_n<double, 1, 12, kModeKa>(b, grid, st);
+            if (width == 2) return batch_pulse_n<double, 2, 12, kModeKa>(b, grid, st);
+            return OCS_ERR_ARG;
+        }
+        if (precision == OCS_PREC_MIXED) {
+            if (width == 1) return batch_pulse_n<float, 1, 12, kModeKa>(b, grid, st);
+            if (width == 2) return batch_pulse_n<float, 2, 12, kModeKa>(b, grid, st);
+            if (width == 4) return batch_pulse_n<float, 4, 12, kModeKa>(b, grid, st);
+            return OCS_ERR_ARG;
+        }
+        return OCS_ERR_ARG;
+    }
     if (precision == OCS_PREC_F64) {
         if (width == 1) return batch_pulse_n<double, 1, 12>(b, grid, st);
         if (width == 2) return batch_pulse_n<double, 2, 12>(b, grid, st);

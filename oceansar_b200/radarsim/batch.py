@@ -84,8 +84,6 @@ class SceneBatch(object):
         """Place ``gen`` (a RawGenerator of this batch's precision) in a slot; returns it."""
         if gen.precision != self.precision:
             raise ValueError('scene precision %s differs from the batch (%s)' % (gen.precision, self.precision))
-        if gen.scat_spec_enable and gen.scat_spec_mode != 'kodis':
-            raise NotImplementedError('Kirchhoff specular scenes run through RawGenerator, not the scene batch')
         if gen.surface.choppy_enable:
             raise NotImplementedError('choppy surfaces run through RawGenerator, not the scene batch')
         if slot is None:
@@ -122,7 +120,7 @@ class SceneBatch(object):
         s.gen, s.tables, s.desc, s.sdesc, s.done = gen, dev, desc, sdesc, 0
         s.tile_rows = int(tile_rows) if tile_rows else 64
         s.key = (gen.surface.Nx, gen.surface.Ny, tuple(c for c, _, _, _ in gen.surface._raw),
-                 gen.npol * gen.num_ch, s.tile_rows)
+                 gen.npol * gen.num_ch, s.tile_rows, self._kirchhoff(gen))
         self._slots[slot] = s
         return slot
 
@@ -138,10 +136,15 @@ class SceneBatch(object):
     def tile_rows(self, slot):
         return self._slots[slot].tile_rows
 
+    @staticmethod
+    def _kirchhoff(gen):
+        """Whether the scene's specular term is a Kirchhoff model (its own pulse-kernel class)."""
+        return bool(gen.scat_spec_enable and gen.scat_spec_mode != 'kodis')
+
     def scene_class(self, slot):
-        """(Nx, Ny, outputs): scenes of one class share their launch shapes."""
+        """(Nx, Ny, outputs, Kirchhoff): scenes of one class share their launch shapes."""
         g = self._slots[slot].gen
-        return (g.surface.Nx, g.surface.Ny, g.npol * g.num_ch)
+        return (g.surface.Nx, g.surface.Ny, g.npol * g.num_ch, self._kirchhoff(g))
 
     def remove(self, slot):
         """Free a slot (the scene's buffers stay with its RawGenerator)."""

@@ -227,7 +227,7 @@ def run_batched(gens, precision='mixed', tuner=None, pulse_block=None, max_slots
     echoes = sum(scene_echoes(g) for g in gens)
     rep = dict(scenes=n, echoes=echoes, device_s=dev_s, wall_s=wall, echoes_per_s=echoes / dev_s,
                steps=batch.steps_run - steps0, pulse_block=pulse_block, tile_rows={
-                   '%dx%d/%d' % k: v for k, v in tuned_rows.items()}, tune_s=t_tune,
+                   '%dx%d/%d%s' % (k[0], k[1], k[2], '/ka' if k[3] else ''): v for k, v in tuned_rows.items()}, tune_s=t_tune,
                launches_first_step=launches, kernel_launches=kernel_launches[0])
     batch.close()
     return rep

@@ -7,7 +7,9 @@ raw cube 1e-5 (mixed: float32 accumulation) and 1e-12 (FP64), NRCS 1e-6 / 1e-12.
 
 The mix covers four transform-length classes (64 x 64, 64 x 32, 256 x 256 and the generic
 mixed-radix 48 x 54), one to four channels, dual polarisation, cross-track baselines,
-directional swell and pulse counts that differ, so scenes finish at different steps.
+directional swell, Kirchhoff specular scenes (facet approach and stationary phase, which
+form pulse-kernel classes of their own) and pulse counts that differ, so scenes finish at
+different steps.
 """
 import os
 import tempfile
@@ -39,6 +41,10 @@ def scene_cfgs(tmp):
     out.append((bench.write_cfg(c, os.path.join(tmp, "s256.cfg")), 3, bench.overrides(c)))
     c = dict(bench.C1, L=256, pulses=80, bins=256, wind_U=6.0, wind_dir=200.0)
     out.append((bench.write_cfg(c, os.path.join(tmp, "s256b.cfg")), 4, bench.overrides(c)))
+    # Kirchhoff specular scenes (their own pulse-kernel class): facet approach in dual
+    # polarisation, stationary phase in vv
+    out.append((os.path.join(G, "cfg", "c1fa.cfg"), 5, None))
+    out.append((os.path.join(G, "cfg", "c1spa.cfg"), 6, None))
     return out
 
 
