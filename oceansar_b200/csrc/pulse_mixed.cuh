@@ -373,8 +373,10 @@ OCS_D double srs_f64(double sr_c, double cos_i, double sin_i, double az, double 
 // ---------------------------------------------------------------------------------------
 // One tile of 128 columns x tile_rows rows.  `rseq` is the warp's running row count (ring
 // slot and barrier parity); `bad` becomes true when a bounded wait gave up.
-// TMA = false: every thread loads its own column's inputs of a row from global memory at
-// the top of the row (the scene batch, whose slots keep no tensor maps).  REFRESH: 0 = a
+// TMA = false (the scene batch, whose slots keep no tensor maps): every thread stages its
+// own column's inputs of each row into the same ring by per-thread asynchronous copies
+// (cp.async, one group per row, four rows ahead) and waits only for its own copies, since
+// it alone reads that column of a slot.  REFRESH: 0 = a
 // pulse that reads the stored sqrt(RCS), 1 = a Bragg-refresh pulse (the Romeiser model is
 // compiled only into these), 2 = decided at run time from a.refresh (the scene batch).
 template <int NOUT, bool KODIS, bool TMA = true, int REFRESH = 2, int FAST = 0>
@@ -461,8 +463,39 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
         const unsigned row_bytes = (unsigned)(nf + (a.do_bragg ? 2 : 0) + (load_scat ? 2 * a.npol : 0)) * kMixCols * 4u;
         const unsigned first = rseq;      // ring position of this tile's row 0
         auto slot_of = [&](int r) { return (int)((first + (unsigned)r) % kMixSlots); };
-        auto issue = [&](int r) {         // one thread; the slot of row r is free
-            if constexpr (!TMA) return;
+        auto issue = [&](int r) {         // TMA: one thread; the slot of row r is free
+            if constexpr (!TMA) {
+                // every thread: its column's words of row r, one copy group per row (empty
+                // past the tile, so that every thread counts the same groups)
+                if (r < nrows) {
+                    float *dst = sm.stage + (size_t)slot_of(r) * kMixArrays * kMixCols + threadIdx.x;
+                    const long long g = (long long)(y0 + r) * a.nx + xs;
+                    cp_async(dst + kAdx * kMixCols, a.dx_f + g, 4);
+                    cp_async(dst + kAdy * kMixCols, a.dy_f + g, 4);
+                    cp_async(dst + kAdz * kMixCols, a.dz_f + g, 4);
+                    cp_async(dst + kAdiffx * kMixCols, a.diffx + g, 4);
+                    cp_async(dst + kAdiffy * kMixCols, a.diffy + g, 4);
+                    if (kodis) {
+                        cp_async(dst + kAdxx * kMixCols, a.diffxx + g, 4);
+                        cp_async(dst + kAdyy * kMixCols, a.diffyy + g, 4);
+                        cp_async(dst + kAdxy * kMixCols, a.diffxy + g, 4);
+                    }
+                    if (bragg) {
+                        cp_async(dst + kAindm * kMixCols, a.ind0_m + g, 4);
+                        cp_async(dst + kAindp * kMixCols, a.ind0_p + g, 4);
+                    }
+                    if (load_scat) {
+                        cp_async(dst + kAscat * kMixCols, scat + g, 4);
+                        cp_async(dst + (kAscat + 1) * kMixCols, scat + npix + g, 4);
+                        if (npol == 2) {
+                            cp_async(dst + (kAscat + 2) * kMixCols, scat + 2 * npix + g, 4);
+                            cp_async(dst + (kAscat + 3) * kMixCols, scat + 3 * npix + g, 4);
+                        }
+                    }
+                }
+                cp_async_commit();
+                return;
+            }
             const int slot = slot_of(r);
             float *dst = sm.stage + (size_t)slot * kMixArrays * kMixCols;
             unsigned long long *bar = sm.bar + slot;
@@ -477,27 +510,28 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
             if (load_scat) tma_load_3d(dst + kAscat * kMixCols, &maps->scat, x0t, yy, 0, bar);
         };
         auto wait_row = [&](int r) -> bool {
-            if constexpr (!TMA) return true;
+            if constexpr (!TMA) {
+                // rows up to r + 3 are issued: row 0 waits with 3 groups pending, row r > 0
+                // (waited at the top of row r - 1, with rows r + 1 and r + 2 issued) with 2
+                if (r == 0) cp_async_wait<3>();
+                else cp_async_wait<2>();
+                return true;
+            }
             const unsigned q = first + (unsigned)r;
             return mbar_wait(sm.bar + (q % kMixSlots), (q / kMixSlots) & 1u);
         };
         if (TMA && threadIdx.x == 0)
             for (int r = 0; r < kMixSlots && r < nrows; ++r) issue(r);
+        if (!TMA)
+            for (int r = 0; r < kMixSlots; ++r) issue(r);
         // gathers of the scatterer series, one row ahead
         float2 gm = {0.f, 0.f}, gp = {0.f, 0.f};
         const float2 *sm32 = reinterpret_cast<const float2 *>(a.s_m32);
         const float2 *sp32 = reinterpret_cast<const float2 *>(a.s_p32);
         auto gather = [&](int r, float2 &m, float2 &p) {
-            int i0, i1;
-            if constexpr (TMA) {
-                const float *src = sm.stage + (size_t)slot_of(r) * kMixArrays * kMixCols;
-                i0 = __float_as_int(src[kAindm * kMixCols + threadIdx.x]);
-                i1 = __float_as_int(src[kAindp * kMixCols + threadIdx.x]);
-            } else {
-                const long long g = (long long)(y0 + r) * a.nx + xs;
-                i0 = __ldg(a.ind0_m + g);
-                i1 = __ldg(a.ind0_p + g);
-            }
+            const float *src = sm.stage + (size_t)slot_of(r) * kMixArrays * kMixCols;
+            int i0 = __float_as_int(src[kAindm * kMixCols + threadIdx.x]);
+            int i1 = __float_as_int(src[kAindp * kMixCols + threadIdx.x]);
             i0 += a.tmod_m;
             i0 = i0 >= a.n_m ? i0 - a.n_m : i0;
             i1 += a.tmod_p;
@@ -521,7 +555,7 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
             const int slot = slot_of(i);
             float dx, dy, dz, diffx, diffy, dxx = 0.f, dyy = 0.f, dxy = 0.f;
             float sc[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
-            if constexpr (TMA) {
+            {
                 const float *src = sm.stage + (size_t)slot * kMixArrays * kMixCols;
                 const int t = threadIdx.x;
                 dx = src[kAdx * kMixCols + t]; dy = src[kAdy * kMixCols + t]; dz = src[kAdz * kMixCols + t];
@@ -539,19 +573,6 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
                         sc[1][1] = src[(kAscat + 3) * kMixCols + t];
                     }
                 }
-            } else {
-                const long long g = (long long)(y0 + i) * a.nx + xs;
-                dx = __ldg(a.dx_f + g); dy = __ldg(a.dy_f + g); dz = __ldg(a.dz_f + g);
-                diffx = __ldg(a.diffx + g); diffy = __ldg(a.diffy + g);
-                if (kodis) { dxx = __ldg(a.diffxx + g); dyy = __ldg(a.diffyy + g); dxy = __ldg(a.diffxy + g); }
-                if (load_scat) {
-                    sc[0][0] = __ldg(scat + g);
-                    sc[0][1] = __ldg(scat + npix + g);
-                    if (npol == 2) {
-                        sc[1][0] = __ldg(scat + 2 * npix + g);
-                        sc[1][1] = __ldg(scat + 3 * npix + g);
-                    }
-                }
             }
             const float2 cm = gm, cp = gp;
             if (bragg && i + 1 < nrows) gather(i + 1, gm, gp);
@@ -565,6 +586,7 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
                     if (i + kMixSlots < nrows) issue(i + kMixSlots);
                 }
             }
+            if constexpr (!TMA) issue(i + kMixSlots);  // this thread's column of the slot is read
             if (!col_ok) continue;
 
             const float *rt = sm.rt + i * RT;
@@ -727,6 +749,7 @@ OCS_D void mix_tile(const PulseArgs &a, const MixMaps *maps, float *lo_row, int 
             }
             __syncwarp();
         }
+        if constexpr (!TMA) cp_async_wait<0>();  // no copy may land in the ring after the tile
         rseq = first + (unsigned)nrows;
     }
     // every warp is past its last row: the ring holds no live data, its memory is the
