@@ -21,7 +21,7 @@ import time
 
 import torch
 
-TILE_ROWS = (32, 64, 128)
+TILE_ROWS = (16, 32, 64, 128)
 PULSE_BLOCKS = (4, 16, 64)
 
 

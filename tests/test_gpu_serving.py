@@ -73,7 +73,7 @@ def test_serving_budget_limits_admission():
 
 def test_run_batched_with_autotuner(tmp_path):
     from oceansar_b200.serving import prepare_scene, run_batched
-    from oceansar_b200.tune import Autotuner
+    from oceansar_b200.tune import TILE_ROWS, Autotuner
     specs = [spec(128, 40, 31, 1, 0.0), spec(256, 24, 32, 2, 0.0), spec(128, 33, 33, 3, 0.0)]
     gens = [prepare_scene(s, 'mixed') for s in specs]
     tuner = Autotuner(path=str(tmp_path / 't.json'), steps=2, pulse_blocks=(2, 4))
@@ -81,7 +81,7 @@ def test_run_batched_with_autotuner(tmp_path):
     torch.cuda.synchronize()
     assert rep['scenes'] == 3 and rep['echoes_per_s'] > 0
     assert rep['pulse_block'] in (2, 4)
-    assert set(rep['tile_rows'].values()) <= {32, 64, 128}
+    assert set(rep['tile_rows'].values()) <= set(TILE_ROWS)
     for s, g in zip(specs, gens):
         raw0, _ = alone(s, 'mixed')
         assert rel_l2(g.raw(), raw0) <= 1e-5
