@@ -213,3 +213,31 @@ def test_two_dimensional_steep_and_scattered(spacing, jitter, precision):
                o_d.data_ptr(), nbins, st)
     out = o_d.cpu().numpy().astype(np.float64)
     assert rel(out[:, 0] + 1j * out[:, 1], ref) < 1e-5
+
+
+@pytest.mark.parametrize("precision", ["f64", "c64"])
+def test_two_dimensional_scene_off_pair_alignment(precision):
+    """The [ny, nx] kernel with a scene that starts one component past its element-pair
+    alignment (a view into a larger buffer: 4 bytes for complex64, 8 for complex128), which
+    takes the scalar-load path: same sum as the flattened oracle."""
+    import ctypes
+    from oceansar_b200 import _capi
+    from oceansar_b200.radarsim import range_profile as rp
+    ny, nx, nbins = 203, 390, 120
+    srg, scene = _synthetic(ny, nx, nbins, 8)
+    sinc = rp.calc_sinc_vec(8, 20, Fs=1.1)
+    ref = np.zeros(nbins, complex)
+    orp.chan_profile(srg, scene, 2.725, 0.0, sinc, 8, 20, ref)
+    dt = torch.float64 if precision == "f64" else torch.float32
+    inter = np.stack([scene.real, scene.imag], -1).ravel()
+    buf = torch.tensor(np.concatenate([[0.0], inter]), dtype=dt, device="cuda")
+    c_ptr = buf.data_ptr() + buf.element_size()
+    assert c_ptr % (2 * buf.element_size()) == buf.element_size()
+    s_d = torch.tensor(srg, dtype=torch.float64, device="cuda")
+    w_d = torch.tensor(sinc, dtype=torch.float32, device="cuda")
+    o_d = torch.zeros(nbins, 2, dtype=dt, device="cuda")
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    fn = "ocs_chan_profile_2d_f64" if precision == "f64" else "ocs_chan_profile_2d_c64"
+    _capi.call(fn, s_d.data_ptr(), c_ptr, ny, nx, 2.725, 0.0, w_d.data_ptr(), 8, 20, o_d.data_ptr(), nbins, st)
+    out = o_d.cpu().numpy().astype(np.float64)
+    assert rel(out[:, 0] + 1j * out[:, 1], ref) < (1e-10 if precision == "f64" else 1e-5)
