@@ -241,3 +241,31 @@ def test_two_dimensional_scene_off_pair_alignment(precision):
     _capi.call(fn, s_d.data_ptr(), c_ptr, ny, nx, 2.725, 0.0, w_d.data_ptr(), 8, 20, o_d.data_ptr(), nbins, st)
     out = o_d.cpu().numpy().astype(np.float64)
     assert rel(out[:, 0] + 1j * out[:, 1], ref) < (1e-10 if precision == "f64" else 1e-5)
+
+
+@pytest.mark.parametrize("precision", ["f64", "c64"])
+def test_two_dimensional_fine_oversampling(precision):
+    """A pulse oversampled 80 times (the fine-grid histogram would not fit its shared-memory
+    budget, so the register-window kernel runs): same sum as the flattened oracle."""
+    import ctypes
+    from oceansar_b200 import _capi
+    from oceansar_b200.radarsim import range_profile as rp
+    ny, nx, nbins = 150, 333, 110
+    srg, scene = _synthetic(ny, nx, nbins, 9)
+    sinc = rp.calc_sinc_vec(8, 80, Fs=1.1)
+    ref = np.zeros(nbins, complex)
+    orp.chan_profile(srg, scene, 2.725, 0.0, sinc, 8, 80, ref)
+    if precision == "f64":
+        out = np.zeros(nbins, complex)
+        rp.chan_profile_numba(srg.reshape(ny, nx), scene.reshape(ny, nx), 2.725, 0.0, sinc, 8, 80, out)
+        assert rel(out, ref) < 1e-10
+        return
+    s_d = torch.tensor(srg, dtype=torch.float64, device="cuda")
+    c_d = torch.tensor(np.stack([scene.real, scene.imag], -1), dtype=torch.float32, device="cuda")
+    w_d = torch.tensor(sinc, dtype=torch.float32, device="cuda")
+    o_d = torch.zeros(nbins, 2, dtype=torch.float32, device="cuda")
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _capi.call("ocs_chan_profile_2d_c64", s_d.data_ptr(), c_d.data_ptr(), ny, nx, 2.725, 0.0, w_d.data_ptr(), 8, 80,
+               o_d.data_ptr(), nbins, st)
+    out = o_d.cpu().numpy().astype(np.float64)
+    assert rel(out[:, 0] + 1j * out[:, 1], ref) < 1e-5
