@@ -269,3 +269,33 @@ def test_two_dimensional_fine_oversampling(precision):
                o_d.data_ptr(), nbins, st)
     out = o_d.cpu().numpy().astype(np.float64)
     assert rel(out[:, 0] + 1j * out[:, 1], ref) < 1e-5
+
+
+@pytest.mark.parametrize("taps,ovs", [(5, 10), (7, 3), (16, 4)], ids=["5taps_10x", "7taps_3x", "16taps_4x"])
+@pytest.mark.parametrize("precision", ["f64", "c64"])
+def test_two_dimensional_other_pulses(taps, ovs, precision):
+    """The [ny, nx] kernel with odd and long pulses and other oversampling factors (the
+    convolution splits the taps over four lanes unevenly): same sum as the flattened oracle."""
+    import ctypes
+    from oceansar_b200 import _capi
+    from oceansar_b200.radarsim import range_profile as rp
+    ny, nx, nbins = 131, 260, 100
+    srg, scene = _synthetic(ny, nx, nbins, 10)
+    srg = srg - 2.0
+    sinc = rp.calc_sinc_vec(taps, ovs, Fs=1.1)
+    ref = np.zeros(nbins, complex)
+    orp.chan_profile(srg, scene, 2.725, 0.0, sinc, taps, ovs, ref)
+    if precision == "f64":
+        out = np.zeros(nbins, complex)
+        rp.chan_profile_numba(srg.reshape(ny, nx), scene.reshape(ny, nx), 2.725, 0.0, sinc, taps, ovs, out)
+        assert rel(out, ref) < 1e-10
+        return
+    s_d = torch.tensor(srg, dtype=torch.float64, device="cuda")
+    c_d = torch.tensor(np.stack([scene.real, scene.imag], -1), dtype=torch.float32, device="cuda")
+    w_d = torch.tensor(sinc, dtype=torch.float32, device="cuda")
+    o_d = torch.zeros(nbins, 2, dtype=torch.float32, device="cuda")
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _capi.call("ocs_chan_profile_2d_c64", s_d.data_ptr(), c_d.data_ptr(), ny, nx, 2.725, 0.0, w_d.data_ptr(), taps,
+               ovs, o_d.data_ptr(), nbins, st)
+    out = o_d.cpu().numpy().astype(np.float64)
+    assert rel(out[:, 0] + 1j * out[:, 1], ref) < 1e-5
