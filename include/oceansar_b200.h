@@ -427,8 +427,9 @@ int ocs_rd_azfilter(double *data_d, int64_t npol, int32_t naz, int32_t nrg, cons
  * the same).  No counterpart in the reference: its sar_raw
  * (oceansar/radarsim/sar_raw_nompi.py:32-641) runs the same per-pulse body for one scene
  * per call; a slot runs exactly that body (ocs_surface_update + ocs_pulse) at each pulse.
- * SAR scenes with Kodis or Kirchhoff specular (spec_mode 0 / 1 / 2) and Bragg scattering;
- * Kirchhoff scenes form launch classes of their own; DopSCA and SKIM pulses are rejected. */
+ * SAR scenes with Kodis or Kirchhoff specular (spec_mode 0 / 1 / 2) and Bragg scattering,
+ * linear or choppy surfaces; Kirchhoff scenes form launch classes of their own, choppy
+ * scenes add one launch per step; DopSCA and SKIM pulses are rejected. */
 typedef struct {
     const ocs_surface_desc *surface;   /* as for ocs_surface_update; t, add and swell_rot are
                                           taken per pulse from the tables below           */
@@ -442,6 +443,10 @@ typedef struct {
     const int32_t *flags_d;            /* [az_steps] 1: synthesise the surface, 2: refresh
                                           the Bragg RCS at this pulse                       */
     const int32_t *tmod_d;             /* [az_steps][2] int(t prf) mod N_m, mod N_p         */
+    const ocs_choppy_desc *choppy;     /* choppy surfaces: the slope / curvature step run
+                                          after the column pass (ocs_surface_choppy; its
+                                          swell_rot is taken per pulse from swell_rot_d);
+                                          NULL for linear surfaces                          */
 } ocs_scene_desc;
 
 typedef struct ocs_batch ocs_batch;    /* opaque engine handle                              */

@@ -71,7 +71,8 @@ class SceneDesc(ctypes.Structure):
     """``ocs_scene_desc``: one scene of the scene batch."""
     _fields_ = [("surface", ctypes.c_void_p), ("pulse", ctypes.c_void_p), ("tile_rows", ctypes.c_int32),
                 ("t_d", ctypes.c_void_p), ("add_d", ctypes.c_void_p), ("swell_rot_d", ctypes.c_void_p),
-                ("az_now_d", ctypes.c_void_p), ("flags_d", ctypes.c_void_p), ("tmod_d", ctypes.c_void_p)]
+                ("az_now_d", ctypes.c_void_p), ("flags_d", ctypes.c_void_p), ("tmod_d", ctypes.c_void_p),
+                ("choppy", ctypes.c_void_p)]
 
 
 class KaDesc(ctypes.Structure):

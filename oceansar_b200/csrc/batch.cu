@@ -20,6 +20,7 @@ struct HostSlot {
     bool used = false;
     int rows_key = -1, cols_key = -1, prog = 0, nout = 0;
     int kind = kSlotStd;                          // pulse-kernel class
+    bool choppy = false;                          // runs the choppy step after the column pass
     long long rows_items = 0, cols_items = 0;     // work items of the row / column pass
     long long pulse_items[5] = {0, 0, 0, 0, 0};   // pulse-kernel items per width class
     long long rows_smem = 0, cols_smem = 0;
@@ -38,8 +39,9 @@ struct ocs_batch {
     SlotState *d_slots = nullptr;
     char *d_sargs = nullptr;
     char *d_pargs = nullptr;
+    char *d_cargs = nullptr;              // choppy-step arguments of choppy scenes
     char *h_stage = nullptr;              // pinned: [max_slots][stage_bytes]
-    size_t sbytes = 0, pbytes = 0, stage_bytes = 0;
+    size_t sbytes = 0, pbytes = 0, cbytes = 0, stage_bytes = 0;
     std::vector<cudaEvent_t> staged;      // per slot: its last staging copies
     std::vector<HostSlot> host;
 };
@@ -50,6 +52,7 @@ static void batch_free(ocs_batch *b) {
     cudaFree(b->d_slots);
     cudaFree(b->d_sargs);
     cudaFree(b->d_pargs);
+    cudaFree(b->d_cargs);
     cudaFreeHost(b->h_stage);
     delete b;
 }
@@ -63,12 +66,14 @@ extern "C" int ocs_batch_create(int32_t max_slots, int32_t precision, ocs_batch 
     b->precision = precision;
     b->sbytes = (surface_args_bytes() + 255) & ~(size_t)255;
     b->pbytes = (pulse_args_bytes() + 255) & ~(size_t)255;
-    b->stage_bytes = ((sizeof(SlotState) + 255) & ~(size_t)255) + b->sbytes + b->pbytes;
+    b->cbytes = (choppy_args_bytes() + 255) & ~(size_t)255;
+    b->stage_bytes = ((sizeof(SlotState) + 255) & ~(size_t)255) + b->sbytes + b->pbytes + b->cbytes;
     b->host.resize(max_slots);
     b->staged.assign(max_slots, nullptr);
     cudaError_t e = cudaMalloc(&b->d_slots, sizeof(SlotState) * max_slots);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_sargs, b->sbytes * max_slots);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_pargs, b->pbytes * max_slots);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_cargs, b->cbytes * max_slots);
     if (e == cudaSuccess) e = cudaMallocHost(&b->h_stage, b->stage_bytes * max_slots);
     for (int i = 0; i < max_slots && e == cudaSuccess; ++i)
         e = cudaEventCreateWithFlags(&b->staged[i], cudaEventDisableTiming);
@@ -122,11 +127,18 @@ extern "C" int ocs_batch_set(ocs_batch *b, int32_t slot, const ocs_scene_desc *s
     char *st_slot = stage;
     char *st_sargs = stage + ((sizeof(SlotState) + 255) & ~(size_t)255);
     char *st_pargs = st_sargs + b->sbytes;
+    char *st_cargs = st_pargs + b->pbytes;
     memset(stage, 0, b->stage_bytes);
     int st = surface_args_fill(sd, st_sargs, &h.prog);
     if (st != OCS_OK) return st;
     st = pulse_args_fill(pd, st_pargs);
     if (st != OCS_OK) return st;
+    if (sc->choppy) {
+        if (sc->choppy->n != (int64_t)sd->nx * sd->ny) return OCS_ERR_ARG;
+        st = choppy_args_fill(sc->choppy, st_cargs);
+        if (st != OCS_OK) return st;
+        h.choppy = true;
+    }
 
     SlotState s;
     memset(&s, 0, sizeof(s));
@@ -151,11 +163,14 @@ extern "C" int ocs_batch_set(ocs_batch *b, int32_t slot, const ocs_scene_desc *s
     s.tmod_tab = sc->tmod_d;
     s.sargs = b->d_sargs + b->sbytes * slot;
     s.pargs = b->d_pargs + b->pbytes * slot;
+    s.cargs = h.choppy ? b->d_cargs + b->cbytes * slot : nullptr;
     memcpy(st_slot, &s, sizeof(s));
     cudaStream_t cs = (cudaStream_t)stream;
     cudaError_t e = cudaMemcpyAsync(b->d_sargs + b->sbytes * slot, st_sargs, b->sbytes, cudaMemcpyHostToDevice, cs);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(b->d_pargs + b->pbytes * slot, st_pargs, b->pbytes, cudaMemcpyHostToDevice, cs);
+    if (e == cudaSuccess && h.choppy)
+        e = cudaMemcpyAsync(b->d_cargs + b->cbytes * slot, st_cargs, b->cbytes, cudaMemcpyHostToDevice, cs);
     // the slot record last: kernels that run after it see complete arguments
     if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_slots + slot, st_slot, sizeof(s), cudaMemcpyHostToDevice, cs);
     if (e == cudaSuccess) e = cudaEventRecord(b->staged[slot], cs);
@@ -188,6 +203,7 @@ struct BatchPlan {
     std::vector<std::pair<std::pair<int, int>, ClassLaunch>> rows;   // (length, program)
     std::vector<std::pair<int, ClassLaunch>> cols;
     std::vector<std::pair<std::pair<int, int>, long long>> widths;    // ((kind, width class), items)
+    bool choppy = false;                                              // some slot runs the choppy step
 };
 
 static BatchPlan batch_plan(const ocs_batch *b) {
@@ -206,6 +222,7 @@ static BatchPlan batch_plan(const ocs_batch *b) {
             if (h.pulse_items[w] > 0) widths[std::make_pair(h.kind, w)] += h.pulse_items[w];
     }
     BatchPlan p;
+    for (const HostSlot &h : b->host) p.choppy = p.choppy || (h.used && h.choppy);
     p.rows.assign(rows.begin(), rows.end());
     p.cols.assign(cols.begin(), cols.end());
     p.widths.assign(widths.begin(), widths.end());
@@ -215,7 +232,7 @@ static BatchPlan batch_plan(const ocs_batch *b) {
 extern "C" int ocs_batch_launches_per_step(const ocs_batch *b) {
     if (!b) return OCS_ERR_ARG;
     const BatchPlan p = batch_plan(b);
-    return (int)(p.rows.size() + p.cols.size() + p.widths.size()) + 2;
+    return (int)(p.rows.size() + p.cols.size() + p.widths.size()) + 2 + (p.choppy ? 1 : 0);
 }
 
 extern "C" int ocs_batch_step(ocs_batch *b, int32_t pulses, void *stream) {
@@ -236,6 +253,7 @@ extern "C" int ocs_batch_step(ocs_batch *b, int32_t pulses, void *stream) {
         for (const auto &c : p.cols)
             if ((st = batch_launch_cols(ref, c.first, (int)c.second.items, (size_t)c.second.smem, cs)) != OCS_OK)
                 return st;
+        if (p.choppy && (st = batch_launch_choppy(ref, cs)) != OCS_OK) return st;
         if ((st = batch_launch_pulse_rows(ref, b->precision, cs)) != OCS_OK) return st;
         for (const auto &w : p.widths)
             if ((st = batch_launch_pulse(ref, b->precision, w.first.first, w.first.second, (int)w.second, cs)) !=

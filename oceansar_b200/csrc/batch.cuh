@@ -47,6 +47,7 @@ struct SlotState {
     const int *tmod_tab;            // [az_steps][2] int(t prf) mod N_m, mod N_p
     const void *sargs;              // SurfaceArgs of the scene (device memory)
     const void *pargs;              // PulseArgs of the scene (device memory)
+    const void *cargs;              // ChoppyArgs of a choppy scene (device memory), or null
 };
 
 struct BatchRef {
@@ -103,6 +104,11 @@ int pulse_args_fill(const ocs_pulse_desc *d, void *out);
 // class, one item per CTA (finished slots leave CTAs that return at once).
 int batch_launch_rows(const BatchRef &b, int key, int prog, int grid, size_t smem, cudaStream_t st);
 int batch_launch_cols(const BatchRef &b, int key, int grid, size_t smem, cudaStream_t st);
+// Choppy surfaces: the slope / curvature step of every live choppy slot (after the column
+// pass), its swell rotation taken from the slot's per-pulse table.
+size_t choppy_args_bytes();
+int choppy_args_fill(const ocs_choppy_desc *d, void *out);
+int batch_launch_choppy(const BatchRef &b, cudaStream_t st);
 int batch_launch_pulse_rows(const BatchRef &b, int precision, cudaStream_t st);
 // Whether a scene's pulse descriptor takes the split-range mixed kernel (required of every
 // Kodis / Bragg scene of a mixed-precision batch).

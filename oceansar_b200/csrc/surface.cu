@@ -381,26 +381,30 @@ struct ChoppyArgs {
     float2 sw_dx, sw_dy, sw_dxx, sw_dyy, sw_dxy;
 };
 
+// One facet of the choppy step, with the swell rotation of the current time.
+OCS_D void choppy_px(const ChoppyArgs &c, long long i, float2 swell_rot) {
+    float2 s = make_float2(0.f, 0.f);
+    if (c.swell_exp) s = c_mul(c.swell_exp[i], swell_rot);
+    const float ax = c.ax[i], ay = c.ay[i], axx = c.axx[i], ayy = c.ayy[i];
+    if (c.diffx) {
+        c.diffx[i] = fadd(ax / (1.f + axx), fsub(fmul(c.sw_dx.x, s.x), fmul(c.sw_dx.y, s.y)));
+        c.diffy[i] = fadd(ay / (1.f + ayy), fsub(fmul(c.sw_dy.x, s.x), fmul(c.sw_dy.y, s.y)));
+    }
+    if (c.diffxx) {
+        const float px = 1.f + axx, py = 1.f + ayy;
+        float vxx = (px * c.fxx[i] - c.axxx[i] * ax) / powf(px, 3.f);
+        float vyy = (py * c.fyy[i] - c.ayyy[i] * ay) / powf(py, 3.f);
+        float vxy = (px * c.fxy[i] - c.axxy[i] * ax) / (powf(px, 2.f) * py);
+        c.diffxx[i] = fadd(vxx, fsub(fmul(c.sw_dxx.x, s.x), fmul(c.sw_dxx.y, s.y)));
+        c.diffyy[i] = fadd(vyy, fsub(fmul(c.sw_dyy.x, s.x), fmul(c.sw_dyy.y, s.y)));
+        c.diffxy[i] = fadd(vxy, fsub(fmul(c.sw_dxy.x, s.x), fmul(c.sw_dxy.y, s.y)));
+    }
+}
+
 __global__ void surface_choppy_kernel(ChoppyArgs c) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < c.n;
-         i += (long long)gridDim.x * blockDim.x) {
-        float2 s = make_float2(0.f, 0.f);
-        if (c.swell_exp) s = c_mul(c.swell_exp[i], c.swell_rot);
-        const float ax = c.ax[i], ay = c.ay[i], axx = c.axx[i], ayy = c.ayy[i];
-        if (c.diffx) {
-            c.diffx[i] = fadd(ax / (1.f + axx), fsub(fmul(c.sw_dx.x, s.x), fmul(c.sw_dx.y, s.y)));
-            c.diffy[i] = fadd(ay / (1.f + ayy), fsub(fmul(c.sw_dy.x, s.x), fmul(c.sw_dy.y, s.y)));
-        }
-        if (c.diffxx) {
-            const float px = 1.f + axx, py = 1.f + ayy;
-            float vxx = (px * c.fxx[i] - c.axxx[i] * ax) / powf(px, 3.f);
-            float vyy = (py * c.fyy[i] - c.ayyy[i] * ay) / powf(py, 3.f);
-            float vxy = (px * c.fxy[i] - c.axxy[i] * ax) / (powf(px, 2.f) * py);
-            c.diffxx[i] = fadd(vxx, fsub(fmul(c.sw_dxx.x, s.x), fmul(c.sw_dxx.y, s.y)));
-            c.diffyy[i] = fadd(vyy, fsub(fmul(c.sw_dyy.x, s.x), fmul(c.sw_dyy.y, s.y)));
-            c.diffxy[i] = fadd(vxy, fsub(fmul(c.sw_dxy.x, s.x), fmul(c.sw_dxy.y, s.y)));
-        }
-    }
+         i += (long long)gridDim.x * blockDim.x)
+        choppy_px(c, i, c.swell_rot);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -695,6 +699,34 @@ int batch_launch_cols(const BatchRef &b, int key, int grid, size_t smem, cudaStr
     }
 }
 
+// Choppy step of the batch: 256 facets of one live choppy slot per item.
+__global__ void batch_choppy_kernel(const __grid_constant__ BatchRef b) {
+    __shared__ int pref[kMaxSlots + 1];
+    const int total = scan_slots(b, pref, [](const SlotState &g) {
+        if (!slot_live(g) || !g.cargs) return 0;
+        return (int)((static_cast<const ChoppyArgs *>(g.cargs)->n + 255) / 256);
+    });
+    for (int item = blockIdx.x; item < total; item += gridDim.x) {
+        const int s = find_slot(pref, b.nslots, item);
+        const SlotState &g = b.slots[s];
+        const ChoppyArgs &c = *static_cast<const ChoppyArgs *>(g.cargs);
+        const long long i = (long long)(item - pref[s]) * 256 + threadIdx.x;
+        const float2 rot = g.swrot_tab ? g.swrot_tab[g.counter] : make_float2(0.f, 0.f);
+        if (i < c.n) choppy_px(c, i, rot);
+    }
+}
+
+size_t choppy_args_bytes() { return sizeof(ChoppyArgs); }
+
+int batch_launch_choppy(const BatchRef &b, cudaStream_t st) {
+    int sms = 0, dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return OCS_ERR_CUDA;
+    batch_choppy_kernel<<<sms * 16, 256, 0, st>>>(b);
+    return cudaGetLastError() == cudaSuccess ? OCS_OK : OCS_ERR_CUDA;
+}
+
 }  // namespace ocs
 
 using namespace ocs;
@@ -794,7 +826,7 @@ extern "C" int ocs_surface_update(const ocs_surface_desc *d, float t, void *stre
     return ocs_surface_update_passes(d, t, 3, stream);
 }
 
-extern "C" int ocs_surface_choppy(const ocs_choppy_desc *d, void *stream) {
+int ocs::choppy_args_fill(const ocs_choppy_desc *d, void *out) {
     if (!d || d->n <= 0 || !d->ax_d || !d->ay_d || !d->axx_d || !d->ayy_d) return OCS_ERR_ARG;
     ChoppyArgs c;
     memset(&c, 0, sizeof(c));
@@ -815,6 +847,14 @@ extern "C" int ocs_surface_choppy(const ocs_choppy_desc *d, void *stream) {
         c.sw_dxx = make_float2(m[4], m[5]); c.sw_dyy = make_float2(m[6], m[7]);
         c.sw_dxy = make_float2(m[8], m[9]);
     }
+    memcpy(out, &c, sizeof(c));
+    return OCS_OK;
+}
+
+extern "C" int ocs_surface_choppy(const ocs_choppy_desc *d, void *stream) {
+    ChoppyArgs c;
+    const int st = choppy_args_fill(d, &c);
+    if (st != OCS_OK) return st;
     long long blocks = (d->n + 255) / 256;
     if (blocks > 148 * 32) blocks = 148 * 32;
     surface_choppy_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(c);

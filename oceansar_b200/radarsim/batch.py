@@ -25,7 +25,7 @@ from .sar_raw_nompi import PRECISIONS
 
 
 class _Slot(object):
-    __slots__ = ("gen", "tables", "desc", "sdesc", "done", "tile_rows", "key")
+    __slots__ = ("gen", "tables", "desc", "sdesc", "cdesc", "done", "tile_rows", "key")
 
 
 class SceneBatch(object):
@@ -84,8 +84,6 @@ class SceneBatch(object):
         """Place ``gen`` (a RawGenerator of this batch's precision) in a slot; returns it."""
         if gen.precision != self.precision:
             raise ValueError('scene precision %s differs from the batch (%s)' % (gen.precision, self.precision))
-        if gen.surface.choppy_enable:
-            raise NotImplementedError('choppy surfaces run through RawGenerator, not the scene batch')
         if slot is None:
             free = self.free_slots()
             if not free:
@@ -112,12 +110,17 @@ class SceneBatch(object):
         d.az_step, d.az_now, d.refresh, d.tind = 0, 0.0, 0, 0
         sdesc = gen.surface.update_desc()
         p = lambda t: None if t is None else t.data_ptr()  # noqa: E731
+        # choppy surfaces: the slope / curvature step after the column pass (its swell
+        # rotation comes from the per-pulse table)
+        cdesc = gen.surface.choppy_desc() if gen.surface._aux else None
         desc = SceneDesc(ctypes.addressof(sdesc), ctypes.addressof(d), int(tile_rows), p(dev['t']),
-                         p(dev['add']), p(dev['swell_rot']), p(dev['az_now']), p(dev['flags']), p(dev['tmod']))
+                         p(dev['add']), p(dev['swell_rot']), p(dev['az_now']), p(dev['flags']), p(dev['tmod']),
+                         ctypes.addressof(cdesc) if cdesc is not None else None)
         _capi.call("ocs_batch_set", self._h, int(slot), ctypes.addressof(desc), self._sp())
         gen.t_last_rcs_bragg = t_last
         s = _Slot()
         s.gen, s.tables, s.desc, s.sdesc, s.done = gen, dev, desc, sdesc, 0
+        s.cdesc = cdesc
         s.tile_rows = int(tile_rows) if tile_rows else 64
         s.key = (gen.surface.Nx, gen.surface.Ny, tuple(c for c, _, _, _ in gen.surface._raw),
                  gen.npol * gen.num_ch, s.tile_rows, self._kirchhoff(gen))

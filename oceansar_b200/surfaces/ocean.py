@@ -457,7 +457,9 @@ class OceanSurface(object):
         desc._keep = add_c
         return desc
 
-    def _choppy(self, rot, sp):
+    def choppy_desc(self, rot=np.complex64(0)):
+        """``ocs_choppy_desc`` of a choppy surface (the caller keeps it alive while in use):
+        the slopes / curvatures from this surface's auxiliary fields, swell rotation ``rot``."""
         a, f = self._aux, self._fields
         p = lambda t: t.data_ptr() if t is not None else None  # noqa: E731
         m = (ctypes.c_float * 10)()
@@ -473,6 +475,11 @@ class OceanSurface(object):
                           p(f.get('Diffxy')) if d2 else None,
                           self._swell_d.data_ptr() if self._swell_d is not None else None,
                           float(np.real(rot)), float(np.imag(rot)), m)
+        desc._keep = m
+        return desc
+
+    def _choppy(self, rot, sp):
+        desc = self.choppy_desc(rot)
         _capi.call("ocs_surface_choppy", ctypes.addressof(desc), sp)
 
     # ------------------------------------------------------------------------------

@@ -8,8 +8,8 @@ raw cube 1e-5 (mixed: float32 accumulation) and 1e-12 (FP64), NRCS 1e-6 / 1e-12.
 The mix covers four transform-length classes (64 x 64, 64 x 32, 256 x 256 and the generic
 mixed-radix 48 x 54), one to four channels, dual polarisation, cross-track baselines,
 directional swell, Kirchhoff specular scenes (facet approach and stationary phase, which
-form pulse-kernel classes of their own) and pulse counts that differ, so scenes finish at
-different steps.
+form pulse-kernel classes of their own), a choppy surface and pulse counts that differ, so
+scenes finish at different steps.
 """
 import os
 import tempfile
@@ -31,8 +31,7 @@ def scene_cfgs(tmp):
     import bench
     out = [(os.path.join(G, "cfg", "c1small.cfg"), 0, None),
            (os.path.join(G, "cfg", "c3small.cfg"), 1, None)]
-    # the dual-polarisation two-channel case without choppy waves (choppy surfaces run
-    # through RawGenerator only)
+    # the dual-polarisation two-channel case without choppy waves
     txt = open(os.path.join(G, "cfg", "c2small.cfg")).read().replace("choppy_enable=True", "choppy_enable=False")
     p = os.path.join(tmp, "c2nochop.cfg")
     open(p, "w").write(txt)
@@ -45,6 +44,8 @@ def scene_cfgs(tmp):
     # polarisation, stationary phase in vv
     out.append((os.path.join(G, "cfg", "c1fa.cfg"), 5, None))
     out.append((os.path.join(G, "cfg", "c1spa.cfg"), 6, None))
+    # the choppy dual-polarisation case (slope / curvature step after the column pass)
+    out.append((os.path.join(G, "cfg", "c2small.cfg"), 7, None))
     return out
 
 
