@@ -229,13 +229,12 @@ static int launch_chan_profile_2d_regs(const double *srg, const void *scene, lon
 // around its tile of 128 columns x tile_rows rows (two shared atomic adds per facet into
 // separate real and imaginary planes, instead of a multiply-add per tap and window slot; no
 // register window, so 8 to 12 CTAs fit per SM), then convolves H with the oversampled pulse
-// once per tile and adds the result
-// to the output with global atomics.  A tile whose first and last rows span more bins than H
-// holds is walked in narrower column groups (64 or 32 columns, two or four rows per step,
-// one H each); facets whose bin still falls outside H, and facets with non-finite
-// coefficients (which must touch exactly their own taps, with the reference's complex
-// product), take the direct path of per-tap global atomics.  Bins outside [0, nbins) are
-// dropped, as the reference's edge branch does.
+// once per tile and adds the result to the output with global atomics.  A tile whose first
+// and last rows span more bins than H holds is walked in narrower column groups (64 or 32
+// columns, two or four rows per step, one H each); facets whose bin still falls outside H,
+// and facets with non-finite coefficients (which must touch exactly their own taps, with
+// the reference's complex product), take the direct path of per-tap global atomics.  Bins
+// outside [0, nbins) are dropped, as the reference's edge branch does.
 constexpr int kHThreads = 128;
 constexpr int kHRB = 4;             // rows of loads in flight per thread
 constexpr int kHB = 64;             // bins held by H
